@@ -1,0 +1,432 @@
+"""Benchmark: PatchMatch depth maps/s at 1600x1200 with 10 source views.
+
+Workload (one step): a seeded synthetic heightfield scene of 11 views at
+1600x1200 (f=1200, per-view gain, noise sigma=2). Every view is a reference
+view once: a photometric PatchMatch pass (random init, 6 iterations, window
+radius 5, step 1) against the other 10 views, then a geometric-consistency
+pass (initialised from its photometric maps, the 10 sources' photometric
+depth maps as the geometric term) — 11 depth maps per step.
+
+  value  device-resident: images already in HBM; engines read them there and
+         chain maps on the device; timed with CUDA events on the launching
+         stream, max over ranks.
+  e2e    the same step through the reference-facing API with host buffers:
+         pinned host images in, depth/normal maps back to host every pass.
+
+Under torchrun every rank runs its own scene replica (different seed): the
+reference views shard across GPUs with no data-path collective ("weak").
+``--impl reference`` times the CPU oracle (OpenMP transcription of the
+reference kernel logic; the reference itself has no CPU PatchMatch) on a
+bounded band of the same workload, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+W, H, NSRC, ITERS, RADIUS, STEP = 1600, 1200, 10, 6, 5, 1
+HYP_PER_PIXEL = 14          # 10 propagated + 4 refinement hypotheses per pixel per iteration
+FLOP_PER_TAP = 25           # incremental warp, 1/z, bilinear, 4 moment updates
+METRIC = "depth maps/s (1.6MP,10 src)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--storage", default="f32", choices=["u8", "f16", "f32"])
+    ap.add_argument("--views", type=int, default=NSRC + 1, help="views per scene (each is a reference once)")
+    ap.add_argument("--width", type=int, default=W)
+    ap.add_argument("--height", type=int, default=H)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+def dist_setup():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = tempfile.NamedTemporaryFile(mode="w+", suffix=".csv", delete=False)
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.file, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().strip().splitlines() if r.strip()]
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.file.name)
+        loaded = [s for s in sm if smax and s > 0.3 * max(smax)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+def make_options(scene, storage, geometric):
+    from sensemap_b200.patch_match import PatchMatchOptions
+    o = PatchMatchOptions(depth_min=scene.depth_min, depth_max=scene.depth_max, window_radius=RADIUS,
+                          window_step=STEP, sigma_spatial=RADIUS, num_iterations=ITERS,
+                          geom_consistency=geometric, init_depth_random=not geometric,
+                          geom_consistency_regularizer=0.1,  # config/mvs.yaml value
+                          image_storage=storage)
+    return o
+
+
+class Workload:
+    def __init__(self, scene, storage, device_images, host_images):
+        self.scene = scene
+        self.storage = storage
+        self.dev = device_images    # list of cuda float32 tensors (H x W)
+        self.host = host_images     # list of pinned float32 tensors
+        self.V = len(scene.views)
+
+    def views(self, images, depth=None, normal=None):
+        from sensemap_b200.patch_match import View
+        out = []
+        for i, v in enumerate(self.scene.views):
+            out.append(View(images[i], v.K, v.R, v.T,
+                            depth=None if depth is None else depth[i],
+                            normal=None if normal is None else normal[i]))
+        return out
+
+    def problem(self, ref, views):
+        from sensemap_b200.patch_match import Problem
+        return Problem(ref, [i for i in range(self.V) if i != ref], views)
+
+    def step_device(self, stream, keep):
+        """One scene step with device-resident inputs; engines are kept alive
+        (in `keep`) until the caller has synchronised."""
+        from sensemap_b200.patch_match import PatchMatchACMMCuda
+        sc = self.scene
+        views = self.views(self.dev)
+        opt_p = make_options(sc, self.storage, False)
+        photo = []
+        for r in range(self.V):
+            opt_p.random_seed = r
+            pm = PatchMatchACMMCuda(opt_p, self.problem(r, views), stream=stream)
+            pm.Run()
+            photo.append(pm)
+        maps = [pm.DeviceDepthNormal() for pm in photo]
+        gviews = self.views(self.dev, [m[0] for m in maps], [m[1] for m in maps])
+        opt_g = make_options(sc, self.storage, True)
+        geo = []
+        for r in range(self.V):
+            opt_g.random_seed = 1000 + r
+            pm = PatchMatchACMMCuda(opt_g, self.problem(r, gviews), stream=stream)
+            pm.Run()
+            geo.append(pm)
+        keep.extend(photo + geo)
+        return geo
+
+    def step_host(self):
+        """The same step through host buffers (reference-facing call pattern)."""
+        from sensemap_b200.patch_match import PatchMatchACMMCuda
+        sc = self.scene
+        views = self.views(self.host)
+        opt_p = make_options(sc, self.storage, False)
+        depth, normal = [], []
+        h2d = d2h = launches = 0
+        img_bytes = sum(int(t.numel()) * 4 for t in self.host)
+        for r in range(self.V):
+            opt_p.random_seed = r
+            with PatchMatchACMMCuda(opt_p, self.problem(r, views)) as pm:
+                pm.Run()
+                depth.append(pm.GetDepthMap())
+                normal.append(pm.GetNormalMap())
+                launches += pm.LaunchCount()
+            h2d += img_bytes
+            d2h += depth[-1].nbytes + normal[-1].nbytes
+        gviews = self.views(self.host, depth, normal)
+        opt_g = make_options(sc, self.storage, True)
+        out = []
+        for r in range(self.V):
+            opt_g.random_seed = 1000 + r
+            with PatchMatchACMMCuda(opt_g, self.problem(r, gviews)) as pm:
+                pm.Run()
+                out.append(pm.GetDepthMap())
+                launches += pm.LaunchCount()
+            h2d += img_bytes + sum(d.nbytes for d in depth) + normal[r].nbytes
+            d2h += out[-1].nbytes
+        return out, h2d, d2h, launches
+
+
+def storage_code(name):
+    from sensemap_b200 import STORE_F16, STORE_F32, STORE_U8
+    return {"u8": STORE_U8, "f16": STORE_F16, "f32": STORE_F32}[name]
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(scene, storage, seconds_target: float) -> dict:
+    """The oracle (OpenMP transcription of the reference kernel logic) on a
+    band of rows of one photometric pass of the bench workload, scaled to
+    depth maps/s (photometric + geometric pass of a full view)."""
+    import oracle.oracle as orc
+    from sensemap_b200.patch_match import Problem, View
+    V = len(scene.views)
+    views = [View(v.image, v.K, v.R, v.T) for v in scene.views]
+    prob = Problem(0, list(range(1, V)), views)
+    opt = make_options(scene, storage, False)
+    Hh = scene.views[0].image.shape[0]
+    r0 = Hh // 2
+    t = time.perf_counter()
+    orc.run(opt, prob, rows=(r0, r0 + 4))
+    t4 = time.perf_counter() - t
+    rows = int(max(4, min(Hh // 2, 4 * seconds_target / max(t4, 1e-3))))
+    t = time.perf_counter()
+    orc.run(opt, prob, rows=(r0, r0 + rows))
+    dt = time.perf_counter() - t
+    per_pass = dt * Hh / rows
+    value = 1.0 / (2.0 * per_pass)
+    return {"value": value, "unit": "depth maps/s", "cores": orc.num_threads(), "kind": "port",
+            "sample": (f"oracle photometric pass (6 iterations, N={V - 1}) over rows {r0}..{r0 + rows} of a "
+                       f"{scene.views[0].image.shape[1]}x{Hh} view in {dt:.1f} s; scaled by {Hh}/{rows} rows and x2 "
+                       f"for the geometric pass (extrapolated)")}
+
+
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+    from sensemap_b200 import synthetic as syn
+    from oracle import build as oracle_build
+    oracle_build.build()
+    scene = syn.heightfield_scene(seed=0, width=args.width, height=args.height, num_src=args.views - 1,
+                                  device="cuda" if torch.cuda.is_available() else "cpu")
+    storage = storage_code(args.storage)
+    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
+    samples = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(scene, storage, per_step / 2)
+        if i >= args.warmup:
+            samples.append(cb["value"])
+    value = statistics.median(samples)
+    line = {"metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * (args.views) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": f"heightfield scene, {args.views} views {args.width}x{args.height}, each view "
+                                   f"photometric + geometric PatchMatch (R={RADIUS}, S={STEP}, {ITERS} iterations)",
+                       "global_batch": args.views, "parallelism": "cpu-openmp"},
+            "cpu_baseline": {**cb, "value": value},
+            "e2e": {"value": value, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    world, rank, local = dist_setup()
+    from sensemap_b200 import build as engine_build
+    from sensemap_b200 import _native as N
+    from sensemap_b200 import synthetic as syn
+    engine_build.build()
+    N.lib()
+    storage = storage_code(args.storage)
+    t0 = time.perf_counter()
+    scene = syn.heightfield_scene(seed=rank, width=args.width, height=args.height, num_src=args.views - 1,
+                                  device="cuda")
+    log(f"[rank {rank}] scene rendered in {time.perf_counter() - t0:.1f} s; depth range "
+        f"{scene.depth_min:.2f}..{scene.depth_max:.2f}")
+    dev_imgs = [torch.from_numpy(v.image).cuda() for v in scene.views]
+    host_imgs = [torch.from_numpy(v.image).pin_memory() for v in scene.views]
+    wl = Workload(scene, storage, dev_imgs, host_imgs)
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def device_step(keep):
+        return wl.step_device(sptr, keep)
+
+    # Warm-up.
+    for _ in range(args.warmup):
+        keep = []
+        device_step(keep)
+        torch.cuda.synchronize()
+        del keep
+    # Timed region (device-resident inputs).
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    keep, launches = [], 0
+    ev0.record(stream)
+    last_geo = None
+    for _ in range(args.steps):
+        step_keep = []
+        last_geo = device_step(step_keep)
+        launches += sum(pm.LaunchCount() for pm in step_keep)
+        keep.append(step_keep)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    ms = max_over_ranks(ms, world)
+    depth_maps = args.steps * wl.V * world
+    value = depth_maps / (ms / 1000.0)
+    acc = [syn.depth_accuracy(pm.GetDepthMap(), scene.views[i].depth_gt) for i, pm in enumerate(last_geo)]
+    for k in keep:
+        for pm in k:
+            pm.close()
+    del keep
+
+    # Per-kernel device time (one profiled photometric + geometric pass of view 0).
+    from sensemap_b200.patch_match import PatchMatchACMMCuda
+    prof_keep = []
+    views = wl.views(dev_imgs)
+    pm = PatchMatchACMMCuda(make_options(scene, storage, False), wl.problem(0, views), stream=sptr)
+    pm.SetProfiling(True)
+    pm.Run()
+    prof = pm.Profile()
+    prof_keep.append(pm)
+    sweep_n, sweep_ms = prof.get("sweep", (0, 0.0))
+    T = (2 * RADIUS // STEP + 1) ** 2
+    taps_per_launch = (args.width * args.height / 2) * (args.views - 1) * HYP_PER_PIXEL * T
+    sweep_avg_s = sweep_ms / max(sweep_n, 1) / 1000.0
+    achieved_tflops = taps_per_launch * FLOP_PER_TAP / sweep_avg_s / 1e12
+    fp32 = ctypes_rate(N, 0)
+    tex = ctypes_rate(N, 1)
+    peak_taps = min(fp32 / FLOP_PER_TAP, tex)
+    roof = {"bound": "fp32-pipe/texture", "achieved": achieved_tflops, "peak": peak_taps * FLOP_PER_TAP / 1e12,
+            "unit": "TFLOP/s", "frac": (taps_per_launch / sweep_avg_s) / peak_taps, "traffic": None,
+            "kernel": "SweepKernel<5,1,16>", "taps_per_launch": taps_per_launch, "flop_per_tap": FLOP_PER_TAP,
+            "avg_launch_ms": sweep_avg_s * 1000.0,
+            "peak_source": (f"measured in this process: FP32 FMA {fp32 / 1e12:.1f} TFLOP/s, bilinear texture "
+                            f"{tex / 1e9:.0f} Gsample/s; peak = min(FP32/25, texture) taps/s x 25 flop"),
+            "kernel_share": {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}}
+    for p in prof_keep:
+        p.close()
+
+    e2e = None
+    if not args.no_e2e:
+        # End to end through host buffers (pinned inputs, host outputs).
+        wl.step_host()
+        torch.cuda.synchronize()
+        barrier(world)
+        t = time.perf_counter()
+        h2d = d2h = 0
+        for _ in range(args.steps):
+            _, h2d, d2h, _ = wl.step_host()
+        torch.cuda.synchronize()
+        el = max_over_ranks(time.perf_counter() - t, world)
+        e2e = {"value": depth_maps / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline(scene, storage, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"heightfield scene, {wl.V} views {args.width}x{args.height}, each view "
+                                       f"photometric + geometric PatchMatch (R={RADIUS}, S={STEP}, {ITERS} "
+                                       f"iterations), {args.storage} image storage",
+                           "global_batch": wl.V * world, "parallelism": f"views sharded, {world} replica(s)",
+                           "l2": "inputs larger than L2 (11 x 1600x1200 images + maps per step)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clock_info,
+                "accuracy": {"within_1pct_gt_mean": float(np.mean(acc)), "per_view": [round(a, 4) for a in acc]}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def ctypes_rate(N, kind):
+    import ctypes as C
+    r = C.c_double()
+    N.check(N.lib().smvs_test_calibrate(kind, 0.5, C.byref(r)))
+    return r.value
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,246 @@
+/*
+ * smvs.h — C ABI of the B200-native PatchMatch multi-view-stereo depth-map engine.
+ *
+ * This is the drop-in boundary for SenseMap's per-reference-view depth-map stage.
+ * Each entry point replaces one member of the reference's C++ operator
+ *   sensemap::mvs::PatchMatchACMMCuda (src/mvs/patch_match_cuda.h:154-203)
+ * and its option/problem types (src/controllers/patch_match_options.h:42-353),
+ * as cited beside each declaration. Conventions (all entry points):
+ *   - every function returns an int status (SMVS_OK == 0) and never exits the
+ *     process; smvs_last_error() gives a thread-local message for the last failure;
+ *   - caller-owned host buffers, library-owned device memory;
+ *   - no global per-thread constant slots: every engine carries its own
+ *     parameter block, so any number of engines may share a GPU;
+ *   - plain C types only (no CUDA or torch types); a CUDA stream is passed as
+ *     an opaque void* (cudaStream_t), NULL meaning an engine-owned stream.
+ */
+#ifndef SMVS_H_
+#define SMVS_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SMVS_ABI_VERSION 1
+/* Hard cap on source views per reference view. The reference caps at 8
+ * (MAX_NUM_SRC_IMAGE, src/mvs/kernel_functions.h:28); the view-selection
+ * bitmask is a uint32 (kernel_functions.cu:2205), which bounds it at 32. */
+#define SMVS_MAX_SRC 32
+/* Number of floats in one source-view pose record:
+ * [fx cx fy cy | R_rel(9) | T_rel(3) | C(3) | P(3x4) | P^-1(3x4)]
+ * (K_NUM_TFORM_PARAMS, kernel_functions.h:31; layout patch_match_cuda.cu:516-559). */
+#define SMVS_POSE_FLOATS 43
+
+typedef enum smvs_status {
+  SMVS_OK = 0,
+  SMVS_EINVAL = 1,    /* bad argument or unsupported option combination */
+  SMVS_ENOMEM = 2,    /* device or host allocation failed / budget exceeded */
+  SMVS_ECUDA = 3,     /* a CUDA runtime call failed */
+  SMVS_ESTATE = 4,    /* call out of order (e.g. get before run) */
+  SMVS_EIO = 5,       /* file read/write failed */
+  SMVS_ETIMEDOUT = 6, /* a bounded wait gave up */
+  SMVS_ECANCELED = 7  /* job cancelled */
+} smvs_status;
+
+/* Pixel type of caller images (host or device). Grey values are 0..255 in both. */
+typedef enum smvs_pixel_format {
+  SMVS_PIX_U8 = 0,
+  SMVS_PIX_F32 = 1
+} smvs_pixel_format;
+
+/* How source images are stored on the device and fetched by the cost kernels.
+ * All three use hardware bilinear filtering with border (zero) addressing, the
+ * sampling the reference uses (patch_match_cuda.cu:258-278). */
+typedef enum smvs_image_storage {
+  SMVS_STORE_U8 = 0,  /* 1 B/px, normalised read (the reference's own format) */
+  SMVS_STORE_F16 = 1, /* 2 B/px, precision form: FP16 storage, FP32 accumulation */
+  SMVS_STORE_F32 = 2  /* 4 B/px, plain FP32 path */
+} smvs_image_storage;
+
+typedef enum smvs_memory {
+  SMVS_MEM_HOST = 0,
+  SMVS_MEM_DEVICE = 1 /* pointers are device pointers on the engine's GPU */
+} smvs_memory;
+
+/* Mirrors the fields of PatchMatchOptions (patch_match_options.h:42-304) that the
+ * depth-map path reads, with the reference's defaults (smvs_options_default). */
+typedef struct smvs_options {
+  double depth_min;                        /* :74 */
+  double depth_max;                        /* :75 */
+  int window_radius;                       /* :78 */
+  int window_step;                         /* :85 */
+  double sigma_spatial;                    /* :89 (reference default = window_radius) */
+  double sigma_color;                      /* :90 */
+  int num_samples;                         /* :93 */
+  int num_iterations;                      /* :106 */
+  int geom_consistency;                    /* :110 */
+  double geom_consistency_regularizer;     /* :116 */
+  double geom_consistency_max_cost;        /* :120 */
+  int filter;                              /* :125 */
+  int filter_min_num_consistent;           /* :135 */
+  double filter_geom_consistency_max_cost; /* :139 */
+  int init_depth_random;                   /* :164 */
+  float random_depth_ratio;                /* :166 */
+  float random_angle1_range;               /* :167 (radians) */
+  float random_angle2_range;               /* :168 (radians) */
+  double init_ncc_matching_cost;           /* :180 */
+  double max_ncc_matching_cost;            /* :184 */
+  double alpha;                            /* :187 */
+  double beta;                             /* :190 */
+  int thk;                                 /* :192 (1..4) */
+  int num_good_hypothesis;                 /* :197 */
+  int num_bad_hypothesis;                  /* :198 */
+  int random_optimization;                 /* :68 */
+  int local_optimization;                  /* :69 */
+  int est_curvature;                       /* :71 */
+  int median_filter;                       /* :248 */
+  int conf_filter;                         /* :234 */
+  float depth_diff_threshold;              /* :231 */
+  float conf_threshold;                    /* :237 */
+  int has_prior_depth;                     /* :250 — prior paths not built: must be 0 */
+  int propagate_depth;                     /* :288 — prior paths not built: must be 0 */
+  /* ---- fields with no counterpart in the reference ---- */
+  uint64_t random_seed;  /* seed of the counter-based RNG (replaces cuRAND XORWOW,
+                            gpu_mat_prng.cu:10-37); results are a pure function of
+                            (inputs, options, seed) */
+  int image_storage;     /* smvs_image_storage */
+  int gpu_index;         /* CUDA device ordinal; -1 = current device */
+} smvs_options;
+
+/* One view: image + calibration. K, R, T follow the reference's Image
+ * accessors (src/mvs/image.h GetK/GetR/GetT): K row-major 3x3, (R, T) the
+ * world-to-camera transform, x_cam = R x_world + T. */
+typedef struct smvs_view {
+  int width;
+  int height;
+  int pixel_format;     /* smvs_pixel_format */
+  size_t row_stride;    /* bytes between rows of `pixels`; 0 = dense */
+  const void* pixels;   /* grey image, 0..255 */
+  float K[9];
+  float R[9];
+  float T[3];
+  float scale;          /* Problem::src_image_scales (patch_match_options.h:317); 0 or 1 = none.
+                           K is scaled by it (patch_match_cuda.cu:526-530); the caller
+                           passes the image already resampled to the scaled size. */
+  const float* depth;   /* optional W*H depth map of this view (geometric pass:
+                           source views' maps; ref view: initial map when
+                           init_depth_random == 0) */
+  const float* normal;  /* optional 3*W*H planar normal map (ref view initial map) */
+} smvs_view;
+
+/* Mirrors Problem (patch_match_options.h:306-353) with the non-owning pointers
+ * resolved to the views themselves. */
+typedef struct smvs_problem {
+  smvs_view ref;
+  const smvs_view* src;  /* num_src entries */
+  int num_src;           /* 1..SMVS_MAX_SRC */
+  const uint8_t* ref_mask; /* optional W*H mask; depth is zeroed where 0
+                              (MaskDepthMapKernel, kernel_functions.cu:3080-3093) */
+  int memory;            /* smvs_memory of pixels/depth/normal/ref_mask */
+} smvs_problem;
+
+typedef struct smvs_engine smvs_engine;
+
+/* Device pointers to an engine's maps (valid until smvs_destroy). Layouts are
+ * dense row-major; normal and cost are planar (slice-major), like GpuMat's
+ * slices (src/util/gpu_mat.h:194-198) without the pitch. */
+typedef struct smvs_device_maps {
+  int width, height, num_src;
+  float* depth;      /* W*H */
+  float* normal;     /* 3*W*H */
+  float* conf;       /* W*H */
+  float* cost;       /* N*W*H */
+  uint32_t* view_sel;/* W*H */
+} smvs_device_maps;
+
+/* Fill `opt` with the reference's defaults (PatchMatchOptions, patch_match_options.h:42-304). */
+int smvs_options_default(smvs_options* opt);
+
+/* Validate options like PatchMatchOptions::Check (patch_match_options.cc:75-101),
+ * plus this engine's limits (supported window radius/step pairs, thk <= 4). */
+int smvs_options_check(const smvs_options* opt);
+
+/* Replaces PatchMatchACMMCuda::PatchMatchACMMCuda(options, problem)
+ * (patch_match_cuda.cu:422-432): uploads the reference and source views,
+ * builds the 43-float pose records (InitTransforms :493-580) and the
+ * reference moments (InitRefImage :110-197). `stream` is a cudaStream_t or NULL. */
+int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
+                smvs_engine** out);
+
+/* Replaces PatchMatchACMMCuda::Run (patch_match_cuda.cu:748-1057): random or
+ * given initialisation, InitConfMapKernel, num_iterations checkerboard
+ * iterations with local optimisation, then the optional filters. Work is
+ * enqueued on the engine's stream; the call does not wait for it. */
+int smvs_run(smvs_engine* eng);
+
+/* Replaces PatchMatchACMMCuda::RunFilter(dedup) (patch_match_cuda.cu:1075-1108):
+ * the geometric-consistency filter of the reference view's depth map (the
+ * problem's ref.depth) against the source views' depth maps. */
+int smvs_run_filter(smvs_engine* eng, int deduplication);
+
+/* Replace GetDepthMap / GetNormalMap / GetConfMap (patch_match_cuda.cu:47-54,440-446).
+ * Copy to caller host buffers (synchronises the engine's stream). */
+int smvs_get_depth_map(smvs_engine* eng, float* out);        /* W*H */
+int smvs_get_normal_map(smvs_engine* eng, float* out);       /* 3*W*H planar */
+int smvs_get_conf_map(smvs_engine* eng, float* out);         /* W*H */
+int smvs_get_cost_map(smvs_engine* eng, float* out);         /* N*W*H planar */
+int smvs_get_view_sel_map(smvs_engine* eng, uint32_t* out);  /* W*H */
+/* Replaces GetCurvatureMap (patch_match_cuda.cu:444-446): 2*W*H planar uint16,
+ * available when est_curvature && geom_consistency (ComputeCurvatureMap,
+ * kernel_functions.cu:1603-1653). */
+int smvs_get_curvature_map(smvs_engine* eng, uint16_t* out);
+
+int smvs_get_size(const smvs_engine* eng, int* width, int* height, int* num_src);
+int smvs_get_device_maps(const smvs_engine* eng, smvs_device_maps* out);
+/* Block until the engine's queued work is done. */
+int smvs_synchronize(smvs_engine* eng);
+/* Number of kernel launches this engine has enqueued so far. */
+int64_t smvs_launch_count(const smvs_engine* eng);
+
+/* Kernel kinds for per-launch timing. No counterpart in the reference beyond
+ * its stdout CudaTimer per iteration (patch_match_cuda.cu:776, 908, 1055). */
+typedef enum smvs_kernel_kind {
+  SMVS_KERNEL_CONVERT = 0,
+  SMVS_KERNEL_PREP = 1,
+  SMVS_KERNEL_INIT = 2,
+  SMVS_KERNEL_INIT_CONF = 3,
+  SMVS_KERNEL_SWEEP = 4,
+  SMVS_KERNEL_LOCAL_OPT = 5,
+  SMVS_KERNEL_MASK = 6,
+  SMVS_KERNEL_FILTER = 7
+} smvs_kernel_kind;
+/* Record CUDA events around every subsequent launch of this engine. */
+int smvs_set_profiling(smvs_engine* eng, int enable);
+/* Number of timed launches of `kind` and their summed device time (ms); synchronises. */
+int smvs_get_profile(smvs_engine* eng, int kind, int* count, double* total_ms);
+void smvs_destroy(smvs_engine* eng);
+
+/* Thread-local message describing the last failure on this thread. */
+const char* smvs_last_error(void);
+
+/* ---- on-disk formats (host only) ---------------------------------------- */
+/* Mat<T>::Write / Read (src/util/mat.h:179-215): text header "W&H&D&" followed by
+ * the little-endian payload, slice-major then row-major. */
+int smvs_write_mat_f32(const char* path, const float* data, int width, int height, int depth);
+int smvs_write_mat_u32(const char* path, const uint32_t* data, int width, int height, int depth);
+int smvs_write_mat_u16(const char* path, const uint16_t* data, int width, int height, int depth);
+/* Reads the header; if `data` is NULL only the sizes are returned. `elem_size` is 2 or 4. */
+int smvs_read_mat(const char* path, void* data, size_t capacity_bytes, int elem_size,
+                  int* width, int* height, int* depth);
+/* NormalMap::Encode / Decode (src/mvs/normal_map.cc:109-181): one uint32 per pixel. */
+int smvs_encode_normal_map(const float* normal, int width, int height, uint32_t* code);
+int smvs_decode_normal_map(const uint32_t* code, int width, int height, float* normal);
+/* DepthMap::Write + NormalMap::Write + Mat<float>::Write of the conf map into
+ * <dir>/{depth_maps,normal_maps,conf_maps}/<image_name>.<type>.bin
+ * (base/common.h:16-33; patch_match_controller.cc:4369-4375, 4706, 4719). */
+int smvs_write_maps(smvs_engine* eng, const char* stereo_dir, const char* image_name,
+                    const char* output_type);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SMVS_H_ */

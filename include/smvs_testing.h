@@ -1,0 +1,33 @@
+/*
+ * smvs_testing.h — test hooks of the engine library (not part of the drop-in
+ * boundary; no counterpart in the reference).
+ */
+#ifndef SMVS_TESTING_H_
+#define SMVS_TESTING_H_
+
+#include <stddef.h>
+#include "smvs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Sample a w*h grey image (values as float, stored on the device in
+ * `storage` format: SMVS_STORE_U8 takes round(value) and reads it normalised,
+ * F16/F32 store value as is) through the same texture path the cost kernels
+ * use (linear filtering, border addressing, unnormalised coordinates) at n
+ * coordinates xy[2*i], xy[2*i+1]. Host buffers in and out; synchronous. */
+int smvs_test_sample_texture(const float* image, int w, int h, int storage, const float* xy, int n, float* out);
+
+/* Throughput calibration on the current device, used as roofline denominators
+ * for this path's bounds: kind 0 = FP32 FMA rate (flop/s, FMA = 2 flop),
+ * kind 1 = bilinear texture samples/s from an 8-bit texture with warp-coherent
+ * coordinates (the access pattern of the cost kernels). Runs for about
+ * `seconds`; synchronous. */
+int smvs_test_calibrate(int kind, double seconds, double* rate);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

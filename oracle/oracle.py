@@ -1,0 +1,143 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Mirrors sensemap_b200.patch_match's calling convention so tests can run the
+same Problem through the CUDA engine and through the oracle.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from sensemap_b200 import _native as N
+from sensemap_b200.patch_match import PatchMatchOptions, Problem
+
+from . import build as _build
+
+_LIB = None
+
+
+class orc_outputs(C.Structure):
+    _fields_ = [(n, C.c_void_p) for n in ("depth", "normal", "conf", "cost", "view_sel", "grad", "ref_sum",
+                                           "ref_sqsum", "poses")]
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = _build.build()
+        h = C.CDLL(str(path))
+        h.orc_run.restype = C.c_int
+        h.orc_run.argtypes = [C.POINTER(N.smvs_options), C.POINTER(N.smvs_problem), C.c_int, C.c_int,
+                              C.POINTER(orc_outputs)]
+        h.orc_run_filter.restype = C.c_int
+        h.orc_run_filter.argtypes = [C.POINTER(N.smvs_options), C.POINTER(N.smvs_problem), C.c_void_p]
+        h.orc_eval_costs.restype = C.c_int
+        h.orc_eval_costs.argtypes = [C.POINTER(N.smvs_options), C.POINTER(N.smvs_problem), C.c_int, C.c_void_p,
+                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_uniform.restype = C.c_float
+        h.orc_uniform.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
+        h.orc_tex_bilinear.restype = C.c_float
+        h.orc_tex_bilinear.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+        h.orc_num_threads.restype = C.c_int
+        _LIB = h
+    return _LIB
+
+
+def _problem_struct(problem: Problem):
+    keep = []
+
+    def fill(cv, v, scale):
+        img = np.asarray(v.image)
+        if img.dtype == np.uint8:
+            fmt = N.PIX_U8
+        else:
+            img = np.ascontiguousarray(img, dtype=np.float32)
+            fmt = N.PIX_F32
+        img = np.ascontiguousarray(img)
+        keep.append(img)
+        cv.width, cv.height, cv.pixel_format, cv.row_stride = img.shape[1], img.shape[0], fmt, 0
+        cv.pixels = img.ctypes.data
+        cv.K[:] = list(np.asarray(v.K, np.float64).reshape(9))
+        cv.R[:] = list(np.asarray(v.R, np.float64).reshape(9))
+        cv.T[:] = list(np.asarray(v.T, np.float64).reshape(3))
+        cv.scale = float(scale)
+        for name in ("depth", "normal"):
+            arr = getattr(v, name)
+            if arr is None:
+                setattr(cv, name, None)
+            else:
+                a = np.ascontiguousarray(arr, dtype=np.float32)
+                keep.append(a)
+                setattr(cv, name, a.ctypes.data)
+
+    prob = N.smvs_problem()
+    fill(prob.ref, problem.images[problem.ref_image_idx], 1.0)
+    srcs = (N.smvs_view * len(problem.src_image_idxs))()
+    scales = list(problem.src_image_scales) or [1.0] * len(problem.src_image_idxs)
+    for i, idx in enumerate(problem.src_image_idxs):
+        fill(srcs[i], problem.images[idx], scales[i])
+    keep.append(srcs)
+    prob.src = srcs
+    prob.num_src = len(problem.src_image_idxs)
+    if problem.mask is not None:
+        m = np.ascontiguousarray(problem.mask, dtype=np.uint8)
+        keep.append(m)
+        prob.ref_mask = m.ctypes.data
+    prob.memory = N.MEM_HOST
+    return prob, keep
+
+
+def run(options: PatchMatchOptions, problem: Problem, rows=None) -> dict:
+    """The oracle's PatchMatchACMMCuda(options, problem).Run(); returns all maps."""
+    prob, keep = _problem_struct(problem)
+    ref = problem.images[problem.ref_image_idx]
+    H, W, Nn = ref.height, ref.width, len(problem.src_image_idxs)
+    out = {"depth": np.zeros((H, W), np.float32), "normal": np.zeros((3, H, W), np.float32),
+           "conf": np.zeros((H, W), np.float32), "cost": np.zeros((Nn, H, W), np.float32),
+           "view_sel": np.zeros((H, W), np.uint32), "grad": np.zeros((H, W), np.float32),
+           "ref_sum": np.zeros((H, W), np.float32), "ref_sqsum": np.zeros((H, W), np.float32),
+           "poses": np.zeros((Nn, 43), np.float32)}
+    oo = orc_outputs(**{k: v.ctypes.data for k, v in out.items()})
+    r0, r1 = (0, 0) if rows is None else rows
+    st = lib().orc_run(C.byref(options.to_c()), C.byref(prob), r0, r1, C.byref(oo))
+    if st != 0:
+        raise N.SmvsError(st, "oracle run failed")
+    return out
+
+
+def run_filter(options: PatchMatchOptions, problem: Problem) -> np.ndarray:
+    prob, keep = _problem_struct(problem)
+    ref = problem.images[problem.ref_image_idx]
+    out = np.zeros((ref.height, ref.width), np.float32)
+    st = lib().orc_run_filter(C.byref(options.to_c()), C.byref(prob), out.ctypes.data)
+    if st != 0:
+        raise N.SmvsError(st, "oracle filter failed")
+    return out
+
+
+def eval_costs(options: PatchMatchOptions, problem: Problem, rows, cols, depths, normals):
+    """FP32 transcription and FP64 evaluation of the NCC cost of one hypothesis
+    per sampled pixel, for every source view: (n, N) float32, (n, N) float64."""
+    prob, keep = _problem_struct(problem)
+    rows = np.ascontiguousarray(rows, np.int32)
+    cols = np.ascontiguousarray(cols, np.int32)
+    depths = np.ascontiguousarray(depths, np.float32)
+    normals = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+    n = rows.shape[0]
+    Nn = len(problem.src_image_idxs)
+    c32 = np.zeros((n, Nn), np.float32)
+    c64 = np.zeros((n, Nn), np.float64)
+    st = lib().orc_eval_costs(C.byref(options.to_c()), C.byref(prob), n, rows.ctypes.data, cols.ctypes.data,
+                              depths.ctypes.data, normals.ctypes.data, c32.ctypes.data, c64.ctypes.data)
+    if st != 0:
+        raise N.SmvsError(st, "oracle eval failed")
+    return c32, c64
+
+
+def uniform(seed: int, stage: int, pixel: int, draw: int) -> float:
+    return float(lib().orc_uniform(seed, stage, pixel, draw))
+
+
+def num_threads() -> int:
+    return int(lib().orc_num_threads())

@@ -1,0 +1,73 @@
+/*
+ * smvs_oracle.h — CPU oracle for the PatchMatch depth-map path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is an OpenMP transcription of the reference
+ * kernel logic (SenseMap src/mvs/kernel_functions.cu, patch_match_cuda.cu,
+ * gpu_mat_ref_image.cu, utils.{h,cc}), labelled as such: the reference has no
+ * CPU PatchMatch of its own. It is the checker for the CUDA engine in
+ * sensemap_b200/csrc and the timed CPU baseline of bench.py; the product never
+ * links or calls it.
+ *
+ * Deliberate differences from the reference, each shared with the CUDA engine:
+ *   - cuRAND XORWOW is replaced by a counter-based generator (splitmix64 mixing,
+ *     Steele, Lea & Flood, OOPSLA 2014) keyed on (seed, stage, pixel, draw);
+ *   - the Marsaglia normal sampler gives up after 32 rejected trials.
+ * Parity against the reference's own kernels is checked by running them (built
+ * from the reference sources into oracle/_ref by oracle/ref_build.sh) on the
+ * same inputs: cost-level parity deterministically, full runs statistically.
+ */
+#ifndef SMVS_ORACLE_H_
+#define SMVS_ORACLE_H_
+
+#include <stdint.h>
+#include "../include/smvs.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Outputs of one oracle run (caller-owned, dense). Any pointer may be NULL. */
+typedef struct orc_outputs {
+  float* depth;      /* W*H */
+  float* normal;     /* 3*W*H planar */
+  float* conf;       /* W*H */
+  float* cost;       /* N*W*H planar */
+  uint32_t* view_sel;/* W*H */
+  float* grad;       /* W*H  (ComputeGradientMap) */
+  float* ref_sum;    /* W*H  (bilateral mean of the reference window) */
+  float* ref_sqsum;  /* W*H  (bilateral mean of squares) */
+  float* poses;      /* N*43 */
+} orc_outputs;
+
+/* PatchMatchACMMCuda(options, problem) + Run() on the CPU, rows [row_begin,
+ * row_end) of every half-sweep only when row_end > row_begin (a bounded band
+ * used for CPU timing), else the whole image. Host memory only. */
+int orc_run(const smvs_options* opt, const smvs_problem* prob, int row_begin, int row_end,
+            orc_outputs* out);
+
+/* PatchMatchACMMCuda::RunFilter(false): FilterDepthMapsKernel over the
+ * problem's ref.depth using the source views' depth maps. Writes W*H. */
+int orc_run_filter(const smvs_options* opt, const smvs_problem* prob, float* depth_out);
+
+/* Cost of one hypothesis at sampled pixels, FP32 transcription (same as the
+ * run) and FP64 evaluation (bilinear in double, exact exp/sqrt, unquantised
+ * texture weights). costs32/costs64 are n_pix*N. */
+int orc_eval_costs(const smvs_options* opt, const smvs_problem* prob, int n_pix,
+                   const int* rows, const int* cols, const float* depths,
+                   const float* normals /* n_pix*3 */, float* costs32, double* costs64);
+
+/* The generator shared with the engine: uniform in (0, 1]. */
+float orc_uniform(uint64_t seed, uint32_t stage, uint32_t pixel, uint32_t draw);
+
+/* Texture filtering model used by the oracle (CUDA linear filtering with
+ * 8-bit fixed-point weights): sample `img` (w*h floats) at unnormalised (x, y). */
+float orc_tex_bilinear(const float* img, int w, int h, float x, float y);
+
+/* Number of OpenMP threads the oracle uses. */
+int orc_num_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,158 @@
+"""ctypes binding of the engine's C ABI (include/smvs.h).
+
+Loads ``sensemap_b200/libsmvs.so`` (built in-tree by ``sensemap_b200.build``).
+There is no fallback: if the library is missing or does not load, every entry
+point raises ``NativeLibraryError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+SMVS_MAX_SRC = 32
+SMVS_POSE_FLOATS = 43
+
+SMVS_OK, SMVS_EINVAL, SMVS_ENOMEM, SMVS_ECUDA, SMVS_ESTATE, SMVS_EIO, SMVS_ETIMEDOUT, SMVS_ECANCELED = range(8)
+PIX_U8, PIX_F32 = 0, 1
+STORE_U8, STORE_F16, STORE_F32 = 0, 1, 2
+MEM_HOST, MEM_DEVICE = 0, 1
+(KERNEL_CONVERT, KERNEL_PREP, KERNEL_INIT, KERNEL_INIT_CONF, KERNEL_SWEEP, KERNEL_LOCAL_OPT, KERNEL_MASK,
+ KERNEL_FILTER) = range(8)
+KERNEL_NAMES = ["convert", "prep_ref", "init", "init_conf", "sweep", "local_opt", "mask", "filter"]
+
+STATUS_NAMES = {0: "SMVS_OK", 1: "SMVS_EINVAL", 2: "SMVS_ENOMEM", 3: "SMVS_ECUDA", 4: "SMVS_ESTATE",
+                5: "SMVS_EIO", 6: "SMVS_ETIMEDOUT", 7: "SMVS_ECANCELED"}
+
+
+class NativeLibraryError(RuntimeError):
+    pass
+
+
+class SmvsError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class smvs_options(C.Structure):
+    _fields_ = [
+        ("depth_min", C.c_double), ("depth_max", C.c_double),
+        ("window_radius", C.c_int), ("window_step", C.c_int),
+        ("sigma_spatial", C.c_double), ("sigma_color", C.c_double),
+        ("num_samples", C.c_int), ("num_iterations", C.c_int),
+        ("geom_consistency", C.c_int),
+        ("geom_consistency_regularizer", C.c_double), ("geom_consistency_max_cost", C.c_double),
+        ("filter", C.c_int), ("filter_min_num_consistent", C.c_int),
+        ("filter_geom_consistency_max_cost", C.c_double),
+        ("init_depth_random", C.c_int),
+        ("random_depth_ratio", C.c_float), ("random_angle1_range", C.c_float), ("random_angle2_range", C.c_float),
+        ("init_ncc_matching_cost", C.c_double), ("max_ncc_matching_cost", C.c_double),
+        ("alpha", C.c_double), ("beta", C.c_double),
+        ("thk", C.c_int), ("num_good_hypothesis", C.c_int), ("num_bad_hypothesis", C.c_int),
+        ("random_optimization", C.c_int), ("local_optimization", C.c_int),
+        ("est_curvature", C.c_int), ("median_filter", C.c_int), ("conf_filter", C.c_int),
+        ("depth_diff_threshold", C.c_float), ("conf_threshold", C.c_float),
+        ("has_prior_depth", C.c_int), ("propagate_depth", C.c_int),
+        ("random_seed", C.c_uint64), ("image_storage", C.c_int), ("gpu_index", C.c_int),
+    ]
+
+
+class smvs_view(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("pixel_format", C.c_int),
+        ("row_stride", C.c_size_t), ("pixels", C.c_void_p),
+        ("K", C.c_float * 9), ("R", C.c_float * 9), ("T", C.c_float * 3),
+        ("scale", C.c_float),
+        ("depth", C.c_void_p), ("normal", C.c_void_p),
+    ]
+
+
+class smvs_problem(C.Structure):
+    _fields_ = [
+        ("ref", smvs_view), ("src", C.POINTER(smvs_view)), ("num_src", C.c_int),
+        ("ref_mask", C.c_void_p), ("memory", C.c_int),
+    ]
+
+
+class smvs_device_maps(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int), ("num_src", C.c_int),
+        ("depth", C.c_void_p), ("normal", C.c_void_p), ("conf", C.c_void_p),
+        ("cost", C.c_void_p), ("view_sel", C.c_void_p),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "smvs_options_default": (C.c_int, [C.POINTER(smvs_options)]),
+    "smvs_options_check": (C.c_int, [C.POINTER(smvs_options)]),
+    "smvs_create": (C.c_int, [C.POINTER(smvs_options), C.POINTER(smvs_problem), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "smvs_run": (C.c_int, [C.c_void_p]),
+    "smvs_run_filter": (C.c_int, [C.c_void_p, C.c_int]),
+    "smvs_get_depth_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_normal_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_conf_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_cost_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_view_sel_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_curvature_map": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "smvs_get_size": (C.c_int, [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "smvs_get_device_maps": (C.c_int, [C.c_void_p, C.POINTER(smvs_device_maps)]),
+    "smvs_synchronize": (C.c_int, [C.c_void_p]),
+    "smvs_launch_count": (C.c_int64, [C.c_void_p]),
+    "smvs_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "smvs_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "smvs_destroy": (None, [C.c_void_p]),
+    "smvs_last_error": (C.c_char_p, []),
+    "smvs_write_mat_f32": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "smvs_write_mat_u32": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "smvs_write_mat_u16": (C.c_int, [C.c_char_p, C.c_void_p, C.c_int, C.c_int, C.c_int]),
+    "smvs_read_mat": (C.c_int, [C.c_char_p, C.c_void_p, C.c_size_t, C.c_int, C.POINTER(C.c_int),
+                                C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "smvs_encode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "smvs_decode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
+    "smvs_write_maps": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    # include/smvs_testing.h
+    "smvs_test_sample_texture": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
+                                           C.c_void_p]),
+    "smvs_test_calibrate": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_double)]),
+}
+
+_LIB = None
+
+
+def library_path() -> Path:
+    return Path(os.environ.get("SMVS_LIBRARY", Path(__file__).resolve().parent / "libsmvs.so"))
+
+
+def lib():
+    """The loaded engine library (raises NativeLibraryError if absent)."""
+    global _LIB
+    if _LIB is None:
+        path = library_path()
+        if not path.exists():
+            raise NativeLibraryError(f"{path} is missing: build it with sensemap_b200.build.build()")
+        try:
+            handle = C.CDLL(str(path))
+        except OSError as exc:
+            raise NativeLibraryError(f"cannot load {path}: {exc}") from exc
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = handle
+    return _LIB
+
+
+def last_error() -> str:
+    msg = lib().smvs_last_error()
+    return msg.decode() if msg else ""
+
+
+def check(status: int) -> None:
+    if status != SMVS_OK:
+        raise SmvsError(status, last_error())
+
+
+def exported_symbols() -> list[str]:
+    return list(_SIGNATURES)

@@ -1,0 +1,81 @@
+"""Build recipe for the engine's shared library (libsmvs.so, in-tree).
+
+Compiles sensemap_b200/csrc with nvcc for sm_100a only. The translation units
+are compiled in parallel and linked into ``sensemap_b200/libsmvs.so``; the
+result is reused when no source is newer than it.
+"""
+from __future__ import annotations
+
+import concurrent.futures as futures
+import os
+import shutil
+import subprocess
+from pathlib import Path
+
+PKG_DIR = Path(__file__).resolve().parent
+CSRC = PKG_DIR / "csrc"
+LIB_PATH = PKG_DIR / "libsmvs.so"
+BUILD_DIR = PKG_DIR / "_build"
+INCLUDE_DIR = PKG_DIR.parent / "include"
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ["-std=c++17", "-O3", "--use_fast_math", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+              "-Xptxas", "-v"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found: the engine needs the CUDA toolkit to build")
+
+
+def _sources() -> list[Path]:
+    return sorted(list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cpp")))
+
+
+def _deps() -> list[Path]:
+    return _sources() + sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE_DIR.glob("*.h")) \
+        + [Path(__file__)]
+
+
+def needs_build() -> bool:
+    if not LIB_PATH.exists():
+        return True
+    t = LIB_PATH.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in _deps())
+
+
+def _compile(src: Path, nvcc: str) -> tuple[Path, str]:
+    obj = BUILD_DIR / (src.name + ".o")
+    cmd = [nvcc, *NVCC_FLAGS, *ARCH_FLAGS, "-c", str(src), "-o", str(obj)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stderr}")
+    return obj, res.stderr
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile libsmvs.so for sm_100a (no GPU needed). Returns its path."""
+    if not force and not needs_build():
+        return LIB_PATH
+    nvcc = _nvcc()
+    BUILD_DIR.mkdir(exist_ok=True)
+    srcs = _sources()
+    with futures.ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 4)) as ex:
+        results = list(ex.map(lambda s: _compile(s, nvcc), srcs))
+    objs = [r[0] for r in results]
+    if verbose:
+        for _, log in results:
+            print(log)
+    tmp = LIB_PATH.with_suffix(".so.tmp")
+    cmd = [nvcc, *ARCH_FLAGS, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stderr}")
+    os.replace(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    print(build(force=True, verbose=True))

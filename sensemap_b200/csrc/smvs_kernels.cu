@@ -1,0 +1,211 @@
+// smvs_kernels.cu — per-pixel kernels (image conversion, reference moments,
+// initialisation, mask, geometric-consistency filter) and the dispatch over
+// the window-templated PatchMatch kernels of smvs_sweep.cuh.
+#include <cuda_fp16.h>
+
+#include "smvs_device.cuh"
+#include "smvs_kernels.h"
+
+namespace smvs {
+
+namespace detail {
+template <int R, int S>
+cudaError_t LaunchWindow(const JobParams& p, int op, int colour, cudaStream_t stream);
+}
+
+namespace {
+
+__device__ __forceinline__ float RefAt(const float* ref, int W, int H, int r, int c) {
+  return (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(ref + (size_t)r * W + c) : 0.0f;
+}
+
+// ---------------------------------------------------------------------------
+// Image conversion: caller pixels (u8 / f32 grey 0..255) into device storage.
+// normalise: values / 255 (u8 storage keeps the byte).
+// ---------------------------------------------------------------------------
+__global__ void ConvertImageKernel(const void* __restrict__ in, int in_format, size_t in_stride, int w, int h,
+                                   void* __restrict__ out, int out_storage, size_t out_pitch) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = blockIdx.y * blockDim.y + threadIdx.y;
+  if (x >= w || y >= h) return;
+  const char* irow = (const char*)in + in_stride * y;
+  const float g = (in_format == SMVS_PIX_U8) ? (float)((const uint8_t*)irow)[x] : ((const float*)irow)[x];
+  char* orow = (char*)out + out_pitch * y;
+  if (out_storage == SMVS_STORE_U8) {
+    const float q = fminf(255.f, fmaxf(0.f, rintf(g)));
+    ((uint8_t*)orow)[x] = (uint8_t)q;
+  } else if (out_storage == SMVS_STORE_F16) {
+    ((__half*)orow)[x] = __float2half_rn(g / 255.0f);
+  } else if (out_storage == SMVS_STORE_F32) {
+    ((float*)orow)[x] = g / 255.0f;
+  } else {  // reference image: uint8-quantised, normalised fp32
+    const float q = fminf(255.f, fmaxf(0.f, rintf(g)));
+    ((float*)orow)[x] = q / 255.0f;
+  }
+}
+
+// GpuMatRefImage::FilterKernel (gpu_mat_ref_image.cu:16-56) fused with
+// ComputeGradientMap (kernel_functions.cu:1655-1675).
+__global__ void PrepRefKernel(JobParams p, float* __restrict__ ref_sum, float* __restrict__ ref_sqsum,
+                              float* __restrict__ grad) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const float center = RefAt(p.ref, p.W, p.H, row, col);
+  float cs = 0.f, css = 0.f, ws = 0.f;
+  for (int wr = -p.R; wr <= p.R; wr += p.S)
+    for (int wc = -p.R; wc <= p.R; wc += p.S) {
+      const float color = RefAt(p.ref, p.W, p.H, row + wr, col + wc);
+      const float cd = center - color;
+      const float w = __expf(-(float)(wr * wr + wc * wc) * p.sn - cd * cd * p.cn);
+      cs += w * color;
+      css += w * color * color;
+      ws += w;
+    }
+  cs /= ws;
+  css /= ws;
+  const size_t pix = (size_t)row * p.W + col;
+  ref_sum[pix] = cs;
+  ref_sqsum[pix] = css;
+  const float kx[3][3] = {{-3, 0, 3}, {-10, 0, 10}, {-3, 0, 3}};
+  const float ky[3][3] = {{-3, -10, -3}, {0, 0, 0}, {3, 10, 3}};
+  float gx = 0.f, gy = 0.f;
+#pragma unroll
+  for (int dr = -1; dr <= 1; ++dr)
+#pragma unroll
+    for (int dc = -1; dc <= 1; ++dc) {
+      const float color = RefAt(p.ref, p.W, p.H, row + dr, col + dc);
+      gx += color * kx[dr + 1][dc + 1];
+      gy += color * ky[dr + 1][dc + 1];
+    }
+  grad[pix] = sqrtf(gx * gx + gy * gy);
+}
+
+// InitWorkspace: random branch (FillWithRandomNumbers, gpu_mat.h:114-130 +
+// InitNormalMap, kernel_functions.cu:689-701) or given-map branch (InitDepthMap,
+// kernel_functions.cu:703-737); also clears view_sel (patch_match_cuda.cu:677).
+__global__ void InitKernel(JobParams p, int random_init, float dmin, float dmax) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const size_t WH = (size_t)p.W * p.H;
+  const size_t pix = (size_t)row * p.W + col;
+  Rng r(p.stage_key, (uint32_t)pix);
+  const float vd[3] = {p.refiK[0] * col + p.refiK[1], p.refiK[2] * row + p.refiK[3], 1.0f};
+  float d, n[3];
+  if (random_init) {
+    d = r.Uniform() * (dmax - dmin) + dmin;
+    RandomNormal(r, vd, n);
+  } else {
+    d = p.depth[pix];
+    n[0] = p.normal[pix]; n[1] = p.normal[WH + pix]; n[2] = p.normal[2 * WH + pix];
+    if (d <= 0) {
+      d = r.Uniform() * (dmax - dmin) + dmin;
+      RandomNormal(r, vd, n);
+    }
+    if (Dot3(n, vd) >= 0) RandomNormal(r, vd, n);
+  }
+  p.depth[pix] = d;
+  p.normal[pix] = n[0]; p.normal[WH + pix] = n[1]; p.normal[2 * WH + pix] = n[2];
+  p.view_sel[pix] = 0u;
+}
+
+// MaskDepthMapKernel, kernel_functions.cu:3080-3093 ([quirk] last row and
+// column are left untouched).
+__global__ void MaskKernel(JobParams p, const uint8_t* __restrict__ mask) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (row >= p.H - 1 || col >= p.W - 1) return;
+  const size_t pix = (size_t)row * p.W + col;
+  if (mask[pix] == 0) p.depth[pix] = 0.0f;
+}
+
+// FilterDepthMapsKernel (kernel_functions.cu:3356-3410) and
+// DeduplicDepthMapsKernel (:3452-3487).
+__global__ void FilterDepthMapsKernel(JobParams p, const float* __restrict__ in_depth, float* __restrict__ out_depth,
+                                      int min_consistent, float filter_max_cost, int dedup) {
+  __shared__ float poses[SMVS_MAX_SRC * SMVS_POSE_FLOATS];
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += blockDim.x * blockDim.y) poses[i] = p.poses[i];
+  __syncthreads();
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const size_t pix = (size_t)row * p.W + col;
+  const float d = in_depth[pix];
+  if (d < 1e-6f) { out_depth[pix] = 0.0f; return; }
+  const float np[3] = {p.refiK[0] * col + p.refiK[1], p.refiK[2] * row + p.refiK[3], 1.0f};
+  int good = 0;
+  for (int v = 0; v < p.N; ++v) {
+    const bool ok = GeomCost(poses + v * SMVS_POSE_FLOATS, p.dep_tex[v], (float)row, (float)col, d, np, p.refK,
+                             p.geom_max) <= filter_max_cost;
+    if (ok && dedup) { out_depth[pix] = 0.0f; return; }
+    good += ok;
+  }
+  out_depth[pix] = (!dedup && good < min_consistent) ? 0.0f : d;
+}
+
+
+// Dispatch over the window sizes the reference supports
+// (kernel_functions.cu:1343-1400).
+cudaError_t LaunchWindowOp(const JobParams& p, int op, int colour, cudaStream_t stream) {
+  const int R = p.R, S = p.S;
+  if (R == 5 && S == 1) return detail::LaunchWindow<5, 1>(p, op, colour, stream);
+  if (R == 3 && S == 1) return detail::LaunchWindow<3, 1>(p, op, colour, stream);
+  if (R == 7 && S == 1) return detail::LaunchWindow<7, 1>(p, op, colour, stream);
+  if (R == 3 && S == 2) return detail::LaunchWindow<3, 2>(p, op, colour, stream);
+  if (R == 4 && S == 2) return detail::LaunchWindow<4, 2>(p, op, colour, stream);
+  if (R == 5 && S == 2) return detail::LaunchWindow<5, 2>(p, op, colour, stream);
+  if (R == 7 && S == 2) return detail::LaunchWindow<7, 2>(p, op, colour, stream);
+  return cudaErrorInvalidValue;
+}
+
+}  // namespace
+
+bool SupportedWindow(int R, int S) {
+  return (S == 1 && (R == 3 || R == 5 || R == 7)) || (S == 2 && (R == 3 || R == 4 || R == 5 || R == 7));
+}
+
+cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, int w, int h, void* out,
+                               int out_storage, size_t out_pitch, int /*normalise*/, cudaStream_t stream) {
+  dim3 block(32, 8), grid((w + 31) / 32, (h + 7) / 8);
+  ConvertImageKernel<<<grid, block, 0, stream>>>(in, in_format, in_stride, w, h, out, out_storage, out_pitch);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchPrepRef(const JobParams& p, float* ref_sum, float* ref_sqsum, float* grad, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  PrepRefKernel<<<grid, block, 0, stream>>>(p, ref_sum, ref_sqsum, grad);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchInit(const JobParams& p, int random_init, float opt_dmin, float opt_dmax, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  InitKernel<<<grid, block, 0, stream>>>(p, random_init, opt_dmin, opt_dmax);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchInitConf(const JobParams& p, cudaStream_t stream) { return LaunchWindowOp(p, 0, 0, stream); }
+
+cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream) {
+  return LaunchWindowOp(p, 1, colour, stream);
+}
+
+cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream) {
+  return LaunchWindowOp(p, 2, colour, stream);
+}
+
+cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  MaskKernel<<<grid, block, 0, stream>>>(p, mask);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchFilterDepthMaps(const JobParams& p, const float* in_depth, float* out_depth, int min_consistent,
+                                  float filter_max_cost, int dedup, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  FilterDepthMapsKernel<<<grid, block, 0, stream>>>(p, in_depth, out_depth, min_consistent, filter_max_cost, dedup);
+  return cudaGetLastError();
+}
+
+}  // namespace smvs

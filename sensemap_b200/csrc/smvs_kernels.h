@@ -1,0 +1,54 @@
+// smvs_kernels.h — host-side launchers of the PatchMatch kernels (internal).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/smvs.h"
+
+namespace smvs {
+
+// Per-job parameter block passed by value to every kernel. It replaces the
+// reference's __constant__ ref_K/ref_inv_K slots (kernel_functions.cu:18-20)
+// and its SweepOptions struct (kernel_functions.h:67-111).
+struct JobParams {
+  int W, H, N, R, S;
+  float sn, cn;                     // BilateralWeightComputer normalisations (utils.h:72-92)
+  float depth_min, depth_max;       // options' depth range (float)
+  float rand_depth_ratio, rand_a1, rand_a2;
+  float th_mc, max_mc, inv_beta2;
+  int num_samples, num_good, num_bad, random_opt, geom, thk;
+  float geom_reg, geom_max;
+  float refK[4], refiK[4];
+  uint64_t stage_key;
+  // State maps (dense row-major; normal and cost planar).
+  float* depth;
+  float* normal;
+  float* conf;
+  float* cost;
+  uint32_t* view_sel;
+  // Reference-view data.
+  const float* ref;        // W*H, [0,1]
+  const float* ref_sum;    // W*H
+  const float* ref_sqsum;  // W*H
+  const float* grad;       // W*H
+  const float* poses;      // N*43
+  cudaTextureObject_t src_tex[SMVS_MAX_SRC];
+  cudaTextureObject_t dep_tex[SMVS_MAX_SRC];
+};
+
+// All launchers enqueue on `stream` and return the launch status.
+cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, int w, int h, void* out,
+                               int out_storage, size_t out_pitch, int normalise, cudaStream_t stream);
+cudaError_t LaunchPrepRef(const JobParams& p, float* ref_sum, float* ref_sqsum, float* grad, cudaStream_t stream);
+cudaError_t LaunchInit(const JobParams& p, int random_init, float opt_dmin, float opt_dmax, cudaStream_t stream);
+cudaError_t LaunchInitConf(const JobParams& p, cudaStream_t stream);
+cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream);
+cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream);
+cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream);
+cudaError_t LaunchFilterDepthMaps(const JobParams& p, const float* in_depth, float* out_depth, int min_consistent,
+                                  float filter_max_cost, int dedup, cudaStream_t stream);
+
+bool SupportedWindow(int R, int S);
+
+}  // namespace smvs

@@ -1,0 +1,494 @@
+// smvs_sweep.cuh — window-templated PatchMatch kernels (internal).
+//
+// Thread-per-pixel checkerboard kernels. Per block: the reference-image tile
+// the window needs and the N pose records are staged in shared memory once;
+// source views are fetched through per-view texture objects over pitched HBM
+// (hardware bilinear, border = 0, the sampling the reference configures at
+// patch_match_cuda.cu:258-278). RNG draws come from a counter-based generator,
+// so there is no per-pixel state array. Each supported (radius, step) pair is
+// instantiated in its own translation unit (smvs_win_<R>_<S>.cu).
+#pragma once
+
+#include "smvs_device.cuh"
+#include "smvs_kernels.h"
+
+namespace smvs {
+namespace detail {
+namespace {  // internal linkage: every window translation unit gets its own copy
+
+constexpr int kBX = 32;  // threads per block in x
+constexpr int kBY = 8;   // threads per block in y
+
+__constant__ float kMWeights[5] = {0.f, 1.f, 2.01f, 3.03f, 4.06f};  // kernel_functions.cu:22
+__constant__ int kNeighborOffs[4][2] = {{0, -1}, {-1, 0}, {0, 1}, {1, 0}};  // :23-25 (first four)
+__constant__ int kDirSamples[8][20] = {  // :27-44 (row offset, col offset) pairs
+    {-1, -2, 1, -2, -2, -3, 2, -3, -3, -4, 3, -4, -4, -5, 4, -5, -5, -6, 5, -6},
+    {-1, 2, 1, 2, -2, 3, 2, 3, -3, 4, 3, 4, -4, 5, 4, 5, -5, 6, 5, 6},
+    {-2, -1, -2, 1, -3, -2, -3, 2, -4, -3, -4, 3, -5, -4, -5, 4, -6, -5, -6, 5},
+    {2, -1, 2, 1, 3, -2, 3, 2, 4, -3, 4, 3, 5, -4, 5, 4, 6, -5, 6, 5},
+    {0, -3, 0, -5, 0, -7, 0, -9, 0, -11, 0, -13, 0, -15, 0, -17, 0, -19, 0, -21},
+    {0, 3, 0, 5, 0, 7, 0, 9, 0, 11, 0, 13, 0, 15, 0, 17, 0, 19, 0, 21},
+    {-3, 0, -5, 0, -7, 0, -9, 0, -11, 0, -13, 0, -15, 0, -17, 0, -19, 0, -21, 0},
+    {3, 0, 5, 0, 7, 0, 9, 0, 11, 0, 13, 0, 15, 0, 17, 0, 19, 0, 21, 0}};
+
+__device__ __forceinline__ float RefAt(const float* ref, int W, int H, int r, int c) {
+  return (r >= 0 && r < H && c >= 0 && c < W) ? __ldg(ref + (size_t)r * W + c) : 0.0f;
+}
+
+// Stage the reference tile rows [row0, row0+th) x cols [col0, col0+tw) (border 0)
+// and the pose records in shared memory.
+__device__ __forceinline__ void StageShared(const JobParams& p, float* tile, int row0, int col0, int th, int tw,
+                                            float* poses) {
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nthr = blockDim.x * blockDim.y;
+  for (int i = tid; i < th * tw; i += nthr) {
+    const int r = i / tw, c = i - (i / tw) * tw;
+    tile[i] = RefAt(p.ref, p.W, p.H, row0 + r, col0 + c);
+  }
+  for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += nthr) poses[i] = __ldg(p.poses + i);
+}
+
+// ComputeNCCCost<R,S>, kernel_functions.cu:1245-1340. `win` points at the
+// window's top-left in the shared tile (row stride ws).
+template <int R, int S>
+__device__ __forceinline__ float NccCost(cudaTextureObject_t tex, const float* pose, int row, int col, float depth,
+                                         const float n[3], const float iK[4], int W, int H, float center,
+                                         float rsum, float rvar, const float* win, int ws, float sn, float cn) {
+  constexpr float kMaxCost = 2.0f;
+  float Hm[9];
+  ComposeHomography(pose, row, col, depth, n, iK, Hm);
+  const float inv_z0 = 1.0f / (Hm[6] * col + Hm[7] * row + Hm[8]);
+  const int u = (int)((Hm[0] * col + Hm[1] * row + Hm[2]) * inv_z0);
+  const int v = (int)((Hm[3] * col + Hm[4] * row + Hm[5]) * inv_z0);
+  // [quirk] bounds are the reference image's width/height (:1265-1270).
+  if (u < 0 || u >= W || v < 0 || v >= H) return kMaxCost;
+  const int row_start = row - R, col_start = col - R;
+  float col_src = Hm[0] * col_start + Hm[1] * row_start + Hm[2];
+  float row_src = Hm[3] * col_start + Hm[4] * row_start + Hm[5];
+  float z = Hm[6] * col_start + Hm[7] * row_start + Hm[8];
+  float bcol = col_src, brow = row_src, bz = z;
+  const float h0 = S * Hm[0], h1 = S * Hm[1], h3 = S * Hm[3], h4 = S * Hm[4], h6 = S * Hm[6], h7 = S * Hm[7];
+  float ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f;
+#pragma unroll
+  for (int dr = -R; dr <= R; dr += S) {
+#pragma unroll
+    for (int dc = -R; dc <= R; dc += S) {
+      const float iz = 1.0f / z;
+      const float fu = iz * col_src + 0.5f;
+      const float fv = iz * row_src + 0.5f;
+      const float rc = win[(dr + R) * ws + (dc + R)];
+      const float sc = tex2D<float>(tex, fu, fv);
+      const float cd = center - rc;
+      const float wgt = __expf(-(float)(dr * dr + dc * dc) * sn - cd * cd * cn);
+      const float wsc = wgt * sc;
+      ss += wsc;
+      sss += wsc * sc;
+      srs += wsc * rc;
+      sw += wgt;
+      col_src += h0;
+      row_src += h3;
+      z += h6;
+    }
+    bcol += h1; brow += h4; bz += h7;
+    col_src = bcol; row_src = brow; z = bz;
+  }
+  const float isw = 1.0f / sw;
+  ss *= isw; sss *= isw; srs *= isw;
+  const float svar = sss - ss * ss;
+  if (rvar < 1e-5f || svar < 1e-5f) return kMaxCost;
+  const float cov = srs - rsum * ss;
+  const float val = 1.0f - cov * rsqrtf(rvar * svar);
+  return fmaxf(0.0f, fminf(kMaxCost, val));
+}
+
+struct PixRef {
+  float center, rsum, rvar;
+  const float* win;
+  int ws;
+};
+
+template <int R, int S>
+__device__ __forceinline__ float ViewCost(const JobParams& p, const float* poses, int v, int row, int col,
+                                          float depth, const float n[3], const float np[3], const PixRef& pr) {
+  const float* pose = poses + v * SMVS_POSE_FLOATS;
+  float cost = NccCost<R, S>(p.src_tex[v], pose, row, col, depth, n, p.refiK, p.W, p.H, pr.center, pr.rsum,
+                             pr.rvar, pr.win, pr.ws, p.sn, p.cn);
+  if (p.geom)
+    cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, p.refK, p.geom_max);
+  return cost;
+}
+
+// InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior).
+template <int R, int S>
+__global__ void __launch_bounds__(kBX * kBY) InitConfKernel(JobParams p) {
+  extern __shared__ float smem[];
+  constexpr int tw = kBX + 2 * R, th = kBY + 2 * R;
+  float* tile = smem;
+  float* poses = smem + tw * th;
+  const int col0 = blockIdx.x * kBX, row0 = blockIdx.y * kBY;
+  StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
+  __syncthreads();
+  const int col = col0 + threadIdx.x, row = row0 + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const size_t WH = (size_t)p.W * p.H;
+  const size_t pix = (size_t)row * p.W + col;
+  PixRef pr;
+  pr.center = p.ref[pix];
+  pr.rsum = p.ref_sum[pix];
+  pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
+  pr.ws = tw;
+  pr.win = tile + threadIdx.y * tw + threadIdx.x;
+  const float np[3] = {p.refiK[0] * col + p.refiK[1], p.refiK[2] * row + p.refiK[3], 1.0f};
+  const float n[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const float depth = p.depth[pix];
+  float costs[SMVS_MAX_SRC];
+  int order[SMVS_MAX_SRC];
+  for (int v = 0; v < p.N; ++v) {
+    costs[v] = ViewCost<R, S>(p, poses, v, row, col, depth, n, np, pr);
+    order[v] = v;
+    p.cost[(size_t)v * WH + pix] = costs[v];
+  }
+  // Partial bubble sort: only the best thk positions are needed and the
+  // reference's full ascending bubble sort (utils.h:212-231) puts the same
+  // (stable) values there.
+  for (int i = 0; i < p.N - 1; ++i)
+    for (int j = 0; j < p.N - 1 - i; ++j)
+      if (costs[j] > costs[j + 1]) {
+        const float t = costs[j]; costs[j] = costs[j + 1]; costs[j + 1] = t;
+        const int o = order[j]; order[j] = order[j + 1]; order[j + 1] = o;
+      }
+  float conf = 0.f;
+  uint32_t sel = p.view_sel[pix];
+  for (int i = 0; i < p.thk; ++i) { conf += costs[i]; sel |= (1u << order[i]); }
+  conf /= kMWeights[p.thk];
+  p.conf[pix] = conf;
+  p.view_sel[pix] = sel;
+}
+
+// SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
+// propagate_depth): one checkerboard colour, one thread per pixel.
+template <int R, int S, int NB>
+__global__ void __launch_bounds__(kBX * kBY) SweepKernel(JobParams p, int colour) {
+  extern __shared__ float smem[];
+  constexpr int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
+  float* tile = smem;
+  float* poses = smem + tw * th;
+  const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
+  StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
+  __syncthreads();
+  const int row = row0 + threadIdx.y;
+  const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;
+  const int W = p.W, H = p.H, N = p.N;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  Rng r(p.stage_key, (uint32_t)pix);
+  float depth = p.depth[pix];
+  float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const float grad = p.grad[pix];
+  const float depth_min = p.depth_min;
+  const float depth_max = (float)(1.2 * (double)p.depth_max);  // [quirk] :2213
+  const float a1 = fminf(p.rand_a1, (float)(180.0 * 0.0174532925199432));
+  const float a2 = fminf(p.rand_a2, (float)(90.0 * 0.0174532925199432));
+  const float* iK = p.refiK;
+  const float vd[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
+  const float ivl = rsqrtf(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+
+  float hyp[kMaxHyp][4];
+  int ns = 0;
+  hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
+  ns = 1;
+  if (grad >= 1.0f) {  // :2237-2276
+    float nconf[4], O[4];
+    int nvalid = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      O[i] = (float)i;
+      const int u = kNeighborOffs[i][1] + col, v = kNeighborOffs[i][0] + row;
+      if (u < 0 || u >= W || v < 0 || v >= H) { nconf[i] = FLT_MAX; continue; }
+      nvalid++;
+      nconf[i] = p.conf[(size_t)v * W + u];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3 - i; ++j)
+        if (nconf[j] > nconf[j + 1]) {
+          float t = nconf[j]; nconf[j] = nconf[j + 1]; nconf[j + 1] = t;
+          t = O[j]; O[j] = O[j + 1]; O[j + 1] = t;
+        }
+    nvalid = min(nvalid, 2);
+    for (int i = 0; i < nvalid; ++i) {
+      const int idx = (int)O[i];
+      const int u = kNeighborOffs[idx][1] + col, v = kNeighborOffs[idx][0] + row;
+      const size_t q = (size_t)v * W + u;
+      float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
+      CorrectNormal(nn, vd, ivl);
+      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, v, u, vd);
+      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      ns++;
+    }
+  }
+  for (int k = 0; k < 8; ++k) {  // :2278-2327
+    int br = 0, bc = 0;
+    float best = FLT_MAX;
+#pragma unroll
+    for (int s = 0; s < 10; ++s) {
+      const int nr = row + kDirSamples[k][2 * s], nc = col + kDirSamples[k][2 * s + 1];
+      if (nr < 0 || nr >= H || nc < 0 || nc >= W) continue;
+      const float nconf = p.conf[(size_t)nr * W + nc];
+      if (best > nconf) { br = nr; bc = nc; best = nconf; }
+    }
+    if (best < FLT_MAX) {
+      const size_t q = (size_t)br * W + bc;
+      float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
+      CorrectNormal(nn, vd, ivl);
+      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, br, bc, vd);
+      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      ns++;
+    }
+  }
+
+  PixRef pr;
+  pr.center = p.ref[pix];
+  pr.rsum = p.ref_sum[pix];
+  pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
+  pr.ws = tw;
+  pr.win = tile + threadIdx.y * tw + (col - col0);
+  float M[kMaxHyp][NB];
+  for (int v = 0; v < N; ++v) M[0][v] = p.cost[(size_t)v * WH + pix];
+  for (int h = 1; h < ns; ++h)
+    for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr);
+
+  // ACMM view selection, :2364-2427.
+  uint32_t flags = 0;
+  float probs[NB];
+  for (int v = 0; v < N; ++v) {
+    unsigned n1 = 0, n2 = 0;
+    float pv = 0.f;
+    for (int h = 0; h < ns; ++h) {
+      const float cst = M[h][v];
+      pv += __expf(-cst * cst * p.inv_beta2);
+      n1 += (cst < p.th_mc);
+      n2 += (cst > p.max_mc);
+    }
+    probs[v] = pv;
+    if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
+  }
+  if (flags == 0) return;
+  for (int v = 0; v < N; ++v)
+    if (!((flags >> v) & 1u)) probs[v] = 0.f;
+  {
+    float sum = 0.f;
+    for (int v = 0; v < N; ++v) sum += probs[v];
+    const float inv = 1.0f / sum;
+    float cum = 0.f;
+    for (int v = 0; v < N; ++v) { cum += probs[v] * inv; probs[v] = cum; }
+  }
+  float vw[NB];
+  for (int v = 0; v < N; ++v) vw[v] = 0.f;
+  for (int s = 0; s < p.num_samples; ++s) {
+    const float rp = r.Uniform() - FLT_EPSILON;
+    for (int v = 0; v < N; ++v)
+      if (probs[v] > rp) {
+        if (p.random_opt) vw[v] = 1.0f; else vw[v] += 1.0f;
+        break;
+      }
+  }
+  float wn = 0.f;
+  for (int v = 0; v < N; ++v) wn += vw[v];
+  if (wn <= 1e-5f) return;
+  const float iwn = 1.0f / wn;
+  uint32_t sel = 0;
+  for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
+  float costs[kMaxHyp];
+  for (int h = 0; h < ns; ++h) {
+    float cs = 0.f;
+    for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
+    costs[h] = cs;
+  }
+  p.view_sel[pix] = sel;
+  int mi = -1;
+  {
+    float m = FLT_MAX;
+    for (int h = 0; h < ns; ++h)
+      if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
+  }
+  if (mi < 0) return;
+  depth = hyp[mi][3];
+  normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
+
+  // Refinement, :2449-2520.
+  float nn[3];
+  const float pd_min = (1.0f - p.rand_depth_ratio) * depth, pd_max = (1.0f + p.rand_depth_ratio) * depth;
+  const float ndepth = r.Uniform() * (pd_max - pd_min) + pd_min;  // PerturbDepth :141-147
+  PerturbNormalACMH(normal, nn, a1, a2, r);
+  CorrectNormal(nn, vd, ivl);
+  const float rdepth = r.Uniform() * (depth_max - depth_min) + depth_min;
+  float rn[3];
+  RandomNormal(r, vd, rn);
+  CorrectNormal(rn, vd, ivl);
+  float rh[5][4] = {{normal[0], normal[1], normal[2], depth},
+                    {nn[0], nn[1], nn[2], depth},
+                    {normal[0], normal[1], normal[2], ndepth},
+                    {rn[0], rn[1], rn[2], depth},
+                    {normal[0], normal[1], normal[2], rdepth}};
+  if (mi != 0)
+    for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
+  costs[0] = 0.f;
+  for (int v = 0; v < N; ++v) costs[0] += vw[v] * M[0][v];
+  for (int h = 1; h < 5; ++h) {
+    float cs = 0.f;
+    for (int v = 0; v < N; ++v) {
+      M[h][v] = ViewCost<R, S>(p, poses, v, row, col, rh[h][3], rh[h], vd, pr);
+      cs += vw[v] * M[h][v];
+    }
+    costs[h] = cs;
+  }
+  mi = -1;
+  {
+    float m = FLT_MAX;
+    for (int h = 0; h < 5; ++h)
+      if (costs[h] <= m) { m = costs[h]; mi = h; }
+  }
+  if (mi != -1) {
+    p.conf[pix] = costs[mi];
+    p.depth[pix] = rh[mi][3];
+    p.normal[pix] = rh[mi][0]; p.normal[WH + pix] = rh[mi][1]; p.normal[2 * WH + pix] = rh[mi][2];
+    for (int v = 0; v < N; ++v) p.cost[(size_t)v * WH + pix] = M[mi][v];
+  }
+}
+
+// LocalOptimization, kernel_functions.cu:2736-2931.
+template <int R, int S, int NB>
+__global__ void __launch_bounds__(kBX * kBY) LocalOptKernel(JobParams p, int colour) {
+  extern __shared__ float smem[];
+  constexpr int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
+  float* tile = smem;
+  float* poses = smem + tw * th;
+  const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
+  StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
+  __syncthreads();
+  const int row = row0 + threadIdx.y;
+  const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;
+  const int W = p.W, H = p.H, N = p.N;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  Rng r(p.stage_key, (uint32_t)pix);
+  float conf = p.conf[pix];
+  float depth = p.depth[pix];
+  float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const uint32_t sel = p.view_sel[pix];
+  const float a1 = (float)(4.0 * 0.0174532925199432), a2 = (float)(2.0 * 0.0174532925199432);
+  const float* iK = p.refiK;
+  const float np[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
+  float m[3] = {normal[0], normal[1], normal[2]};
+  float lo = depth, hi = depth;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int u = kNeighborOffs[i][1] + col, v = kNeighborOffs[i][0] + row;
+    if (u < 0 || u >= W || v < 0 || v >= H) continue;
+    const size_t q = (size_t)v * W + u;
+    const float nd = p.depth[q];
+    m[0] += p.normal[q]; m[1] += p.normal[WH + q]; m[2] += p.normal[2 * WH + q];
+    if (nd <= lo) lo = nd;
+    if (nd > hi) hi = nd;
+  }
+  const float inv_norm = rsqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  m[0] *= inv_norm; m[1] *= inv_norm; m[2] *= inv_norm;
+  PixRef pr;
+  pr.center = p.ref[pix];
+  pr.rsum = p.ref_sum[pix];
+  pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
+  pr.ws = tw;
+  pr.win = tile + threadIdx.y * tw + (col - col0);
+  float M[5][NB];
+  float hyp[5][4];
+  int mi = -1;
+  for (int it = 0; it < 5; ++it) {
+    hyp[it][3] = r.Uniform() * (hi - lo) + lo;
+    PerturbNormalACMH(m, hyp[it], a1, a2, r);
+    float mconf = 0.f, mw = 0.f;
+    for (int v = 0; v < N; ++v) {
+      if (!((sel >> v) & 1u)) continue;
+      const float cost = ViewCost<R, S>(p, poses, v, row, col, hyp[it][3], hyp[it], np, pr);
+      M[it][v] = cost;
+      mconf += cost;
+      mw += 1.f;
+    }
+    if (mw <= 0.f) return;
+    mconf /= mw;
+    if (mconf < conf) {
+      conf = mconf;
+      depth = hyp[it][3];
+      normal[0] = hyp[it][0]; normal[1] = hyp[it][1]; normal[2] = hyp[it][2];
+      mi = it;
+    }
+  }
+  if (mi != -1) {
+    p.conf[pix] = conf;
+    p.depth[pix] = depth;
+    p.normal[pix] = normal[0]; p.normal[WH + pix] = normal[1]; p.normal[2 * WH + pix] = normal[2];
+    for (int v = 0; v < N; ++v) {
+      if ((sel >> v) & 1u) {
+        p.cost[(size_t)v * WH + pix] = M[mi][v];
+      } else {
+        const float* pose = poses + v * SMVS_POSE_FLOATS;
+        float cost = NccCost<R, S>(p.src_tex[v], pose, row, col, depth, normal, p.refiK, W, H, pr.center, pr.rsum,
+                                   pr.rvar, pr.win, pr.ws, p.sn, p.cn);
+        // [quirk] :2916-2919 passes the inverse intrinsics where K is expected.
+        if (p.geom)
+          cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, p.refiK, p.geom_max);
+        p.cost[(size_t)v * WH + pix] = cost;
+      }
+    }
+  }
+}
+
+template <int R, int S>
+size_t SweepSmem(int N) {
+  return sizeof(float) * ((2 * kBX + 2 * R) * (kBY + 2 * R) + N * SMVS_POSE_FLOATS);
+}
+
+dim3 SweepGrid(const JobParams& p) {
+  return dim3((unsigned)((p.W + 2 * kBX - 1) / (2 * kBX)), (unsigned)((p.H + kBY - 1) / kBY));
+}
+
+template <int R, int S, int NB>
+cudaError_t LaunchSweepT(const JobParams& p, int colour, bool local, cudaStream_t stream) {
+  const size_t smem = SweepSmem<R, S>(p.N);
+  if (local)
+    LocalOptKernel<R, S, NB><<<SweepGrid(p), dim3(kBX, kBY), smem, stream>>>(p, colour);
+  else
+    SweepKernel<R, S, NB><<<SweepGrid(p), dim3(kBX, kBY), smem, stream>>>(p, colour);
+  return cudaGetLastError();
+}
+
+template <int R, int S>
+cudaError_t LaunchSweepNB(const JobParams& p, int colour, bool local, cudaStream_t stream) {
+  if (p.N <= 8) return LaunchSweepT<R, S, 8>(p, colour, local, stream);
+  if (p.N <= 16) return LaunchSweepT<R, S, 16>(p, colour, local, stream);
+  return LaunchSweepT<R, S, SMVS_MAX_SRC>(p, colour, local, stream);
+}
+
+template <int R, int S>
+cudaError_t LaunchInitConfT(const JobParams& p, cudaStream_t stream) {
+  const size_t smem = sizeof(float) * ((kBX + 2 * R) * (kBY + 2 * R) + p.N * SMVS_POSE_FLOATS);
+  dim3 grid((p.W + kBX - 1) / kBX, (p.H + kBY - 1) / kBY);
+  InitConfKernel<R, S><<<grid, dim3(kBX, kBY), smem, stream>>>(p);
+  return cudaGetLastError();
+}
+
+
+}  // namespace
+
+// One entry point per window: op 0 = InitConf, 1 = sweep, 2 = local optimisation.
+template <int R, int S>
+cudaError_t LaunchWindow(const JobParams& p, int op, int colour, cudaStream_t stream) {
+  if (op == 0) return LaunchInitConfT<R, S>(p, stream);
+  return LaunchSweepNB<R, S>(p, colour, op == 2, stream);
+}
+
+}  // namespace detail
+}  // namespace smvs

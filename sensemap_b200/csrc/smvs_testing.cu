@@ -1,0 +1,197 @@
+// smvs_testing.cu — test hooks (include/smvs_testing.h).
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "../../include/smvs_testing.h"
+
+extern "C" void smvs_internal_set_error(const char* msg);
+
+namespace {
+
+__global__ void SampleKernel(cudaTextureObject_t tex, const float* __restrict__ xy, int n, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = tex2D<float>(tex, xy[2 * i], xy[2 * i + 1]);
+}
+
+int Err(cudaError_t e, const char* what) {
+  std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+  smvs_internal_set_error(m.c_str());
+  return SMVS_ECUDA;
+}
+
+}  // namespace
+
+extern "C" int smvs_test_sample_texture(const float* image, int w, int h, int storage, const float* xy, int n,
+                                        float* out) {
+  if (!image || !xy || !out || w <= 0 || h <= 0 || n < 0 || storage < SMVS_STORE_U8 || storage > SMVS_STORE_F32) {
+    smvs_internal_set_error("smvs_test_sample_texture: bad arguments");
+    return SMVS_EINVAL;
+  }
+  const size_t elem = storage == SMVS_STORE_U8 ? 1 : (storage == SMVS_STORE_F16 ? 2 : 4);
+  std::vector<unsigned char> host(elem * (size_t)w * h);
+  for (size_t i = 0; i < (size_t)w * h; ++i) {
+    if (storage == SMVS_STORE_U8) {
+      float v = image[i] < 0 ? 0 : (image[i] > 255 ? 255 : image[i]);
+      host[i] = (unsigned char)(v + 0.5f);
+    } else if (storage == SMVS_STORE_F16) {
+      __half hv = __float2half_rn(image[i]);
+      memcpy(&host[2 * i], &hv, 2);
+    } else {
+      memcpy(&host[4 * i], &image[i], 4);
+    }
+  }
+  void* dimg = nullptr;
+  size_t pitch = 0;
+  float *dxy = nullptr, *dout = nullptr;
+  cudaTextureObject_t tex = 0;
+  int rc = SMVS_OK;
+  cudaError_t e;
+  if ((e = cudaMallocPitch(&dimg, &pitch, elem * w, h)) != cudaSuccess) return Err(e, "cudaMallocPitch");
+  do {
+    if ((e = cudaMemcpy2D(dimg, pitch, host.data(), elem * w, elem * w, h, cudaMemcpyHostToDevice)) != cudaSuccess) { rc = Err(e, "upload"); break; }
+    if ((e = cudaMalloc(&dxy, sizeof(float) * 2 * (n > 0 ? n : 1))) != cudaSuccess) { rc = Err(e, "cudaMalloc"); break; }
+    if ((e = cudaMalloc(&dout, sizeof(float) * (n > 0 ? n : 1))) != cudaSuccess) { rc = Err(e, "cudaMalloc"); break; }
+    if (n > 0 && (e = cudaMemcpy(dxy, xy, sizeof(float) * 2 * n, cudaMemcpyHostToDevice)) != cudaSuccess) { rc = Err(e, "upload"); break; }
+    cudaResourceDesc rd;
+    memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypePitch2D;
+    rd.res.pitch2D.devPtr = dimg;
+    rd.res.pitch2D.width = w;
+    rd.res.pitch2D.height = h;
+    rd.res.pitch2D.pitchInBytes = pitch;
+    cudaTextureDesc td;
+    memset(&td, 0, sizeof(td));
+    td.addressMode[0] = td.addressMode[1] = td.addressMode[2] = cudaAddressModeBorder;
+    td.filterMode = cudaFilterModeLinear;
+    td.normalizedCoords = 0;
+    if (storage == SMVS_STORE_U8) {
+      rd.res.pitch2D.desc = cudaCreateChannelDesc<unsigned char>();
+      td.readMode = cudaReadModeNormalizedFloat;
+    } else if (storage == SMVS_STORE_F16) {
+      rd.res.pitch2D.desc = cudaCreateChannelDescHalf();
+      td.readMode = cudaReadModeElementType;
+    } else {
+      rd.res.pitch2D.desc = cudaCreateChannelDesc<float>();
+      td.readMode = cudaReadModeElementType;
+    }
+    if ((e = cudaCreateTextureObject(&tex, &rd, &td, nullptr)) != cudaSuccess) { rc = Err(e, "texture"); break; }
+    if (n > 0) {
+      SampleKernel<<<(n + 255) / 256, 256>>>(tex, dxy, n, dout);
+      if ((e = cudaGetLastError()) != cudaSuccess) { rc = Err(e, "launch"); break; }
+      if ((e = cudaMemcpy(out, dout, sizeof(float) * n, cudaMemcpyDeviceToHost)) != cudaSuccess) { rc = Err(e, "download"); break; }
+    }
+  } while (0);
+  if (tex) cudaDestroyTextureObject(tex);
+  cudaFree(dimg);
+  cudaFree(dxy);
+  cudaFree(dout);
+  return rc;
+}
+
+namespace {
+
+// Eight independent FMA chains per thread: the FP32 pipe, not latency, bounds it.
+__global__ void FmaKernel(int iters, float seed, float* out) {
+  float a0 = seed + threadIdx.x, a1 = a0 + 1, a2 = a0 + 2, a3 = a0 + 3, a4 = a0 + 4, a5 = a0 + 5, a6 = a0 + 6,
+        a7 = a0 + 7;
+  const float m = 0.999f, c = 1e-3f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fmaf(a0, m, c); a1 = fmaf(a1, m, c); a2 = fmaf(a2, m, c); a3 = fmaf(a3, m, c);
+      a4 = fmaf(a4, m, c); a5 = fmaf(a5, m, c); a6 = fmaf(a6, m, c); a7 = fmaf(a7, m, c);
+    }
+  }
+  const float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 12345.678f) out[0] = s;  // keeps the chains live
+}
+
+// Bilinear fetches at warp-coherent positions inside a 2048x2048 texture.
+__global__ void TexKernel(cudaTextureObject_t tex, int iters, float* out) {
+  const int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  float x = 16.3f + (gid & 1023) * 1.37f, y = 16.7f + ((gid >> 10) & 1023) * 1.61f;
+  float acc = 0.f;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      acc += tex2D<float>(tex, x + k * 0.9f, y + k * 0.45f);
+    }
+    x += 0.13f;
+    y += 0.07f;
+    if (x > 1900.f) x -= 1800.f;
+    if (y > 1900.f) y -= 1800.f;
+  }
+  if (acc == -1.f) out[0] = acc;
+}
+
+}  // namespace
+
+extern "C" int smvs_test_calibrate(int kind, double seconds, double* rate) {
+  if (!rate || (kind != 0 && kind != 1)) {
+    smvs_internal_set_error("smvs_test_calibrate: bad arguments");
+    return SMVS_EINVAL;
+  }
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  float* dout = nullptr;
+  cudaError_t e;
+  if ((e = cudaMalloc(&dout, sizeof(float))) != cudaSuccess) return Err(e, "cudaMalloc");
+  void* dimg = nullptr;
+  size_t pitch = 0;
+  cudaTextureObject_t tex = 0;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int blocks = sms * 8, threads = 256;
+  int rc = SMVS_OK;
+  do {
+    if (kind == 1) {
+      if ((e = cudaMallocPitch(&dimg, &pitch, 2048, 2048)) != cudaSuccess) { rc = Err(e, "cudaMallocPitch"); break; }
+      if ((e = cudaMemset2D(dimg, pitch, 77, 2048, 2048)) != cudaSuccess) { rc = Err(e, "memset"); break; }
+      cudaResourceDesc rd;
+      memset(&rd, 0, sizeof(rd));
+      rd.resType = cudaResourceTypePitch2D;
+      rd.res.pitch2D.devPtr = dimg;
+      rd.res.pitch2D.width = 2048;
+      rd.res.pitch2D.height = 2048;
+      rd.res.pitch2D.pitchInBytes = pitch;
+      rd.res.pitch2D.desc = cudaCreateChannelDesc<unsigned char>();
+      cudaTextureDesc td;
+      memset(&td, 0, sizeof(td));
+      td.addressMode[0] = td.addressMode[1] = cudaAddressModeBorder;
+      td.filterMode = cudaFilterModeLinear;
+      td.readMode = cudaReadModeNormalizedFloat;
+      if ((e = cudaCreateTextureObject(&tex, &rd, &td, nullptr)) != cudaSuccess) { rc = Err(e, "texture"); break; }
+    }
+    auto run = [&](int iters) {
+      if (kind == 0) FmaKernel<<<blocks, threads>>>(iters, 0.5f, dout);
+      else TexKernel<<<blocks, threads>>>(tex, iters, dout);
+    };
+    // Warm up, then size the timed launch to about `seconds`.
+    int iters = 64;
+    float ms = 0.f;
+    for (int t = 0; t < 12; ++t) {
+      cudaEventRecord(a);
+      run(iters);
+      cudaEventRecord(b);
+      cudaEventSynchronize(b);
+      cudaEventElapsedTime(&ms, a, b);
+      if (ms > 1000.0 * seconds * 0.5 || iters > (1 << 26)) break;
+      iters *= 4;
+    }
+    if ((e = cudaGetLastError()) != cudaSuccess) { rc = Err(e, "calibration launch"); break; }
+    const double per_iter = (kind == 0) ? 16.0 * 8.0 * 2.0 : 8.0;  // flop or samples per thread-iteration
+    *rate = per_iter * (double)iters * blocks * threads / (ms * 1e-3);
+  } while (0);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  if (tex) cudaDestroyTextureObject(tex);
+  cudaFree(dimg);
+  cudaFree(dout);
+  return rc;
+}

@@ -1,0 +1,8 @@
+// smvs_win_5_1.cu — instantiates the PatchMatch kernels for window radius 5, step 1.
+#include "smvs_sweep.cuh"
+
+namespace smvs {
+namespace detail {
+template cudaError_t LaunchWindow<5, 1>(const JobParams& p, int op, int colour, cudaStream_t stream);
+}  // namespace detail
+}  // namespace smvs

@@ -1,0 +1,8 @@
+// smvs_win_7_2.cu — instantiates the PatchMatch kernels for window radius 7, step 2.
+#include "smvs_sweep.cuh"
+
+namespace smvs {
+namespace detail {
+template cudaError_t LaunchWindow<7, 2>(const JobParams& p, int op, int colour, cudaStream_t stream);
+}  // namespace detail
+}  // namespace smvs

@@ -1,0 +1,320 @@
+"""Seeded synthetic multi-view scenes with analytic ground truth.
+
+These stand in for the public MVS benchmarks the reference evaluates on
+(ETH3D, Tanks and Temples, DTU), which are not available here. Each scene is
+rendered by ray casting the analytic surface (no graphics API): grey images
+quantised to integers 0..255 (returned as float32), ground-truth depth (z in
+the camera frame) and normals (camera frame, facing the camera), and
+cameras as (K, R, T) with x_cam = R x_world + T.
+
+Scenes:
+  * ``planes_scene``      — 3..8 random planes, depths 2..8 m, 3-octave value
+                            noise; 1 reference + 4 sources at 640x480, f=500,
+                            on a 30 degree arc with 0.3 m between neighbours.
+  * ``heightfield_scene`` — a plane plus 20 seeded Gaussians, depths ~3..15 m,
+                            per-view gain U[0.8, 1.2] and Gaussian noise
+                            sigma=2; 1 + 10 views at 1600x1200, f=1200.
+Sizes are parameters so tests can render small versions of the same scenes.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+
+@dataclass
+class SceneView:
+    image: np.ndarray          # H x W float32, integer grey 0..255
+    K: np.ndarray              # 3x3
+    R: np.ndarray              # 3x3 world-to-camera
+    T: np.ndarray              # 3
+    depth_gt: np.ndarray       # H x W float32 (0 where nothing was hit)
+    normal_gt: np.ndarray      # 3 x H x W float32 (camera frame)
+
+
+@dataclass
+class Scene:
+    views: list
+    ref_index: int
+    src_indices: list
+    depth_min: float
+    depth_max: float
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+
+def look_at(pos, target, up=(0.0, 0.0, 1.0)):
+    pos = np.asarray(pos, np.float64)
+    fwd = np.asarray(target, np.float64) - pos
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(fwd, np.asarray(up, np.float64))
+    right /= np.linalg.norm(right)
+    down = np.cross(fwd, right)
+    R = np.stack([right, down, fwd])
+    T = -R @ pos
+    return R, T
+
+
+def intrinsics(f, W, H):
+    return np.array([[f, 0, (W - 1) / 2.0], [0, f, (H - 1) / 2.0], [0, 0, 1]], np.float64)
+
+
+def _hash(ix: torch.Tensor, iy: torch.Tensor, salt: int) -> torch.Tensor:
+    """Integer lattice hash -> [0, 1) (a multiply-xorshift mix on int64)."""
+    m = (1 << 31) - 1
+    h = (ix * 73856093) ^ (iy * 19349663) ^ torch.full_like(ix, (salt * 83492791) & m)
+    h = h & m
+    h = ((h ^ (h >> 13)) * 1274126177) & m
+    h = (h ^ (h >> 16)) & m
+    h = (h * 2654435761) & m
+    h = (h ^ (h >> 15)) & m
+    return h.to(torch.float64) / float(m)
+
+
+def value_noise(u: torch.Tensor, v: torch.Tensor, salt: int, octaves: int = 3) -> torch.Tensor:
+    """Band-limited value noise: smooth (quintic) interpolation of lattice
+    values, octaves at doubling frequency and halving amplitude, in [0, 1]."""
+    total = torch.zeros_like(u)
+    norm = 0.0
+    amp = 1.0
+    for o in range(octaves):
+        s = float(1 << o)
+        x, y = u * s, v * s
+        x0, y0 = torch.floor(x), torch.floor(y)
+        fx, fy = x - x0, y - y0
+        ix, iy = x0.to(torch.int64), y0.to(torch.int64)
+        sx = fx * fx * fx * (fx * (fx * 6 - 15) + 10)
+        sy = fy * fy * fy * (fy * (fy * 6 - 15) + 10)
+        salt_o = salt * 31 + o
+        v00 = _hash(ix, iy, salt_o)
+        v10 = _hash(ix + 1, iy, salt_o)
+        v01 = _hash(ix, iy + 1, salt_o)
+        v11 = _hash(ix + 1, iy + 1, salt_o)
+        a = v00 + (v10 - v00) * sx
+        b = v01 + (v11 - v01) * sx
+        total = total + amp * (a + (b - a) * sy)
+        norm += amp
+        amp *= 0.5
+    return total / norm
+
+
+def _pixel_rays(K, R, T, W, H, device):
+    """Ray origins (3,) and unit directions (H, W, 3) in world coordinates, plus
+    the camera-frame ray with z = 1 per pixel (for depth = t * (d . fwd))."""
+    Ki = np.linalg.inv(K)
+    ys, xs = torch.meshgrid(torch.arange(H, dtype=torch.float64, device=device),
+                            torch.arange(W, dtype=torch.float64, device=device), indexing="ij")
+    pc = torch.stack([xs, ys, torch.ones_like(xs)], -1) @ torch.tensor(Ki.T, device=device)  # z = 1
+    Rt = torch.tensor(R.T, device=device)
+    d = pc @ Rt.T  # world direction (not normalised; camera z component = 1)
+    origin = torch.tensor(-R.T @ T, device=device)
+    return origin, d, pc
+
+
+def _finish_image(albedo: torch.Tensor, gen: np.random.Generator, gain_range, noise_sigma) -> np.ndarray:
+    g = albedo * 255.0
+    if gain_range is not None:
+        g = g * float(gen.uniform(*gain_range))
+    if noise_sigma:
+        noise = torch.from_numpy(gen.normal(0.0, noise_sigma, size=tuple(g.shape))).to(g.device)
+        g = g + noise
+    g = torch.clamp(torch.round(g), 0, 255)
+    return g.to(torch.float32).cpu().numpy()
+
+
+def _camera_normals(n_world: torch.Tensor, R, pc: torch.Tensor) -> torch.Tensor:
+    Rm = torch.tensor(R, device=n_world.device)
+    n_cam = n_world @ Rm.T
+    flip = (n_cam * pc).sum(-1, keepdim=True) > 0
+    n_cam = torch.where(flip, -n_cam, n_cam)
+    return n_cam
+
+
+# ---------------------------------------------------------------------------
+# Planes scene
+# ---------------------------------------------------------------------------
+def planes_scene(seed: int = 0, width: int = 640, height: int = 480, focal: float = 500.0, num_src: int = 4,
+                 arc_degrees: float = 30.0, baseline: float = 0.3, device: str = "cpu") -> Scene:
+    gen = np.random.default_rng(seed)
+    centre = np.array([0.0, 0.0, 5.0])
+    n_cams = num_src + 1
+    # Cameras on a circular arc spanning `arc_degrees` with `baseline` between
+    # neighbours; the arc is centred on the middle camera's optical axis and
+    # every camera looks at the scene centre.
+    step = math.radians(arc_degrees) / max(n_cams - 1, 1)
+    radius = (baseline / 2.0) / math.sin(step / 2.0)
+    arc_centre = np.array([0.0, 0.0, radius])
+    cams = []
+    for i in range(n_cams):
+        a = (i - (n_cams - 1) / 2.0) * step
+        pos = arc_centre + radius * np.array([math.sin(a), 0.0, -math.cos(a)])
+        R, T = look_at(pos, centre, up=(0.0, -1.0, 0.0))
+        cams.append((R, T))
+    ref_index = (n_cams - 1) // 2
+    # Planes in the reference camera's frame (the middle camera sits at the
+    # origin looking down +z). Plane 0 is the unbounded background.
+    n_planes = int(gen.integers(3, 9))
+    planes = []
+    for k in range(n_planes):
+        if k == 0:
+            depth = 8.0
+            half = (np.inf, np.inf)
+        else:
+            depth = float(gen.uniform(2.0, 7.0))
+            half = (float(gen.uniform(0.3, 1.2)) * depth / 4, float(gen.uniform(0.3, 1.2)) * depth / 4)
+        tilt = math.radians(float(gen.uniform(0, 35 if k else 15)))
+        az = float(gen.uniform(0, 2 * math.pi))
+        n = np.array([math.sin(tilt) * math.cos(az), math.sin(tilt) * math.sin(az), -math.cos(tilt)])
+        c = np.array([float(gen.uniform(-0.35, 0.35)) * depth, float(gen.uniform(-0.25, 0.25)) * depth, depth])
+        u = np.cross(n, [0.0, 1.0, 0.0]); u /= np.linalg.norm(u)
+        v = np.cross(n, u)
+        planes.append((c, n, u, v, half, int(gen.integers(1, 1 << 30))))
+    K = intrinsics(focal, width, height)
+    views = []
+    for (R, T) in cams:
+        origin, d, pc = _pixel_rays(K, R, T, width, height, device)
+        best_t = torch.full(d.shape[:2], float("inf"), dtype=torch.float64, device=device)
+        albedo = torch.zeros_like(best_t)
+        n_world = torch.zeros_like(d)
+        for (c, n, u, v, half, salt) in planes:
+            ct, nt = torch.tensor(c, device=device), torch.tensor(n, device=device)
+            denom = d @ nt
+            t = ((ct - origin) @ nt) / denom
+            hit = origin + t[..., None] * d
+            lu = (hit - ct) @ torch.tensor(u, device=device)
+            lv = (hit - ct) @ torch.tensor(v, device=device)
+            ok = (t > 0) & torch.isfinite(t)
+            if np.isfinite(half[0]):
+                ok = ok & (lu.abs() <= half[0]) & (lv.abs() <= half[1])
+            closer = ok & (t < best_t)
+            tex = 0.12 + 0.76 * value_noise(lu / 0.10, lv / 0.10, salt)
+            best_t = torch.where(closer, t, best_t)
+            albedo = torch.where(closer, tex, albedo)
+            n_world = torch.where(closer[..., None], nt.expand_as(d), n_world)
+        depth = torch.where(torch.isfinite(best_t), best_t, torch.zeros_like(best_t))  # camera z (pc.z == 1)
+        normal = _camera_normals(n_world, R, pc)
+        img = _finish_image(albedo, gen, None, 0.0)
+        views.append(SceneView(img, K.copy(), R, T, depth.to(torch.float32).cpu().numpy(),
+                               normal.permute(2, 0, 1).to(torch.float32).cpu().numpy()))
+    src = [i for i in range(n_cams) if i != ref_index]
+    d_ref = views[ref_index].depth_gt
+    valid = d_ref[d_ref > 0]
+    return Scene(views, ref_index, src, float(valid.min()) * 0.9, float(valid.max()) * 1.1,
+                 name=f"planes(seed={seed},{width}x{height},N={num_src})", meta={"n_planes": n_planes})
+
+
+# ---------------------------------------------------------------------------
+# Heightfield scene
+# ---------------------------------------------------------------------------
+def _gaussians(gen, count=20, extent=6.0):
+    cx = gen.uniform(-extent, extent, count)
+    cy = gen.uniform(-extent, extent, count)
+    amp = gen.uniform(0.25, 1.2, count)
+    sig = gen.uniform(0.5, 2.0, count)
+    return cx, cy, amp, sig
+
+
+def _height(X, Y, g):
+    cx, cy, amp, sig = g
+    h = torch.zeros_like(X)
+    hx = torch.zeros_like(X)
+    hy = torch.zeros_like(X)
+    for i in range(len(cx)):
+        dx, dy = X - cx[i], Y - cy[i]
+        e = amp[i] * torch.exp(-(dx * dx + dy * dy) / (2 * sig[i] ** 2))
+        h = h + e
+        hx = hx - e * dx / sig[i] ** 2
+        hy = hy - e * dy / sig[i] ** 2
+    return h, hx, hy
+
+
+def heightfield_scene(seed: int = 0, width: int = 1600, height: int = 1200, focal: float = 1200.0,
+                      num_src: int = 10, gain_range=(0.8, 1.2), noise_sigma: float = 2.0, distance: float = 7.0,
+                      elevation_deg: float = 45.0, ring_radius: float = 0.8, device: str = "cpu",
+                      chunk: int = 1 << 20) -> Scene:
+    gen = np.random.default_rng(seed)
+    g = _gaussians(gen)
+    hmax = float(np.sum(g[2])) + 0.01
+    target = np.array([0.0, 0.0, 0.0])
+    el = math.radians(elevation_deg)
+    ref_pos = target + distance * np.array([0.0, -math.cos(el), math.sin(el)])
+    R0, _ = look_at(ref_pos, target)
+    positions = [ref_pos]
+    for k in range(num_src):
+        a = 2 * math.pi * k / num_src
+        positions.append(ref_pos + ring_radius * (math.cos(a) * R0[0] + math.sin(a) * R0[1]))
+    K = intrinsics(focal, width, height)
+    tex_salt = int(gen.integers(1, 1 << 30))
+    views = []
+    for pos in positions:
+        R, T = look_at(pos, target)
+        origin, d, pc = _pixel_rays(K, R, T, width, height, device)
+        dflat = d.reshape(-1, 3)
+        depth = torch.zeros(dflat.shape[0], dtype=torch.float64, device=device)
+        albedo = torch.zeros_like(depth)
+        nwl = torch.zeros_like(dflat)
+        for s in range(0, dflat.shape[0], chunk):
+            dd = dflat[s:s + chunk]
+            # Enter the slab 0 <= Z <= hmax, march in 2 cm steps of Z-extent, bisect.
+            dz = dd[:, 2]
+            t_top = (hmax - origin[2]) / dz
+            t_bot = (0.0 - origin[2]) / dz
+            t0 = torch.clamp(torch.minimum(t_top, t_bot), min=0.0)
+            t1 = torch.maximum(t_top, t_bot)
+            n_steps = 160
+            lo = t0.clone()
+            hi = t1.clone()
+            found = torch.zeros_like(t0, dtype=torch.bool)
+            prev_t = t0.clone()
+            for i in range(1, n_steps + 1):
+                t = t0 + (t1 - t0) * (i / n_steps)
+                P = origin + t[:, None] * dd
+                h, _, _ = _height(P[:, 0], P[:, 1], g)
+                below = (P[:, 2] <= h) & ~found
+                lo = torch.where(below, prev_t, lo)
+                hi = torch.where(below, t, hi)
+                found = found | below
+                prev_t = t
+            for _ in range(30):
+                mid = 0.5 * (lo + hi)
+                P = origin + mid[:, None] * dd
+                h, _, _ = _height(P[:, 0], P[:, 1], g)
+                below = P[:, 2] <= h
+                hi = torch.where(below, mid, hi)
+                lo = torch.where(below, lo, mid)
+            t = 0.5 * (lo + hi)
+            P = origin + t[:, None] * dd
+            _, hx, hy = _height(P[:, 0], P[:, 1], g)
+            nrm = torch.stack([-hx, -hy, torch.ones_like(hx)], -1)
+            nrm = nrm / nrm.norm(dim=-1, keepdim=True)
+            depth[s:s + chunk] = torch.where(found, t, torch.zeros_like(t))  # camera z, since d.z_cam == 1
+            albedo[s:s + chunk] = 0.12 + 0.76 * value_noise(P[:, 0] / 0.06, P[:, 1] / 0.06, tex_salt)
+            nwl[s:s + chunk] = nrm
+        depth = depth.reshape(height, width)
+        normal = _camera_normals(nwl.reshape(height, width, 3), R, pc)
+        img = _finish_image(albedo.reshape(height, width), gen, gain_range, noise_sigma)
+        views.append(SceneView(img, K.copy(), R, T, depth.to(torch.float32).cpu().numpy(),
+                               normal.permute(2, 0, 1).to(torch.float32).cpu().numpy()))
+    d_ref = views[0].depth_gt
+    valid = d_ref[d_ref > 0]
+    return Scene(views, 0, list(range(1, num_src + 1)), float(valid.min()) * 0.9, float(valid.max()) * 1.1,
+                 name=f"heightfield(seed={seed},{width}x{height},N={num_src})")
+
+
+def depth_accuracy(depth: np.ndarray, gt: np.ndarray, rel: float = 0.01) -> float:
+    """Fraction of pixels with ground truth whose depth is within `rel` of it."""
+    m = gt > 0
+    return float(np.mean(np.abs(depth[m] - gt[m]) <= rel * gt[m]))
+
+
+def normal_accuracy(normal: np.ndarray, gt: np.ndarray, degrees: float = 10.0, mask=None) -> float:
+    """Fraction of pixels whose normal is within `degrees` of the ground truth (3 x H x W inputs)."""
+    nn = normal / np.maximum(np.linalg.norm(normal, axis=0, keepdims=True), 1e-12)
+    cosang = np.clip((nn * gt).sum(0), -1, 1)
+    ok = cosang >= math.cos(math.radians(degrees))
+    if mask is not None:
+        ok = ok[mask]
+    return float(np.mean(ok))
