@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--single", action="store_true",
+                    help="profiling mode: run one photometric pass of view 0 per step (for ncu captures)")
     return ap.parse_args()
 
 
@@ -319,6 +321,9 @@ def main():
     wl = Workload(scene, storage, dev_imgs, host_imgs)
     stream = torch.cuda.current_stream()
     sptr = stream.cuda_stream
+    if args.single:
+        run_single(args, wl, sptr)
+        return
 
     def device_step(keep):
         return wl.step_device(sptr, keep)
@@ -419,6 +424,20 @@ def main():
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_single(args, wl, sptr):
+    """One photometric pass of view 0 per step, nothing else (profiling)."""
+    import torch
+    from sensemap_b200.patch_match import PatchMatchACMMCuda
+    views = wl.views(wl.dev)
+    opt = make_options(wl.scene, wl.storage, False)
+    for i in range(args.warmup + args.steps):
+        with PatchMatchACMMCuda(opt, wl.problem(0, views), stream=sptr) as pm:
+            pm.Run()
+            pm.Synchronize()
+    torch.cuda.synchronize()
+    log("single-pass profiling run done")
 
 
 def ctypes_rate(N, kind):

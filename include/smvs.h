@@ -210,8 +210,15 @@ typedef enum smvs_kernel_kind {
   SMVS_KERNEL_SWEEP = 4,
   SMVS_KERNEL_LOCAL_OPT = 5,
   SMVS_KERNEL_MASK = 6,
-  SMVS_KERNEL_FILTER = 7
+  SMVS_KERNEL_FILTER = 7,
+  SMVS_KERNEL_POST = 8   /* curvature, median and confidence filters */
 } smvs_kernel_kind;
+/* Launch-shape knobs of the checkerboard kernels (results do not depend on
+ * them). No counterpart in the reference. */
+typedef struct smvs_tuning {
+  int sweep_block_x; /* threads per block in x: 8, 16, 32 (default) or 64; 256 / x in y */
+} smvs_tuning;
+int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 /* Record CUDA events around every subsequent launch of this engine. */
 int smvs_set_profiling(smvs_engine* eng, int enable);
 /* Number of timed launches of `kind` and their summed device time (ms); synchronises. */

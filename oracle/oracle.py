@@ -19,7 +19,7 @@ _LIB = None
 
 class orc_outputs(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("depth", "normal", "conf", "cost", "view_sel", "grad", "ref_sum",
-                                           "ref_sqsum", "poses")]
+                                           "ref_sqsum", "poses", "curvature")]
 
 
 def lib():
@@ -97,7 +97,7 @@ def run(options: PatchMatchOptions, problem: Problem, rows=None) -> dict:
            "conf": np.zeros((H, W), np.float32), "cost": np.zeros((Nn, H, W), np.float32),
            "view_sel": np.zeros((H, W), np.uint32), "grad": np.zeros((H, W), np.float32),
            "ref_sum": np.zeros((H, W), np.float32), "ref_sqsum": np.zeros((H, W), np.float32),
-           "poses": np.zeros((Nn, 43), np.float32)}
+           "poses": np.zeros((Nn, 43), np.float32), "curvature": np.zeros((2, H, W), np.uint16)}
     oo = orc_outputs(**{k: v.ctypes.data for k, v in out.items()})
     r0, r1 = (0, 0) if rows is None else rows
     st = lib().orc_run(C.byref(options.to_c()), C.byref(prob), r0, r1, C.byref(oo))

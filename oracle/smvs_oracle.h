@@ -37,6 +37,7 @@ typedef struct orc_outputs {
   float* ref_sum;    /* W*H  (bilateral mean of the reference window) */
   float* ref_sqsum;  /* W*H  (bilateral mean of squares) */
   float* poses;      /* N*43 */
+  uint16_t* curvature; /* 2*W*H (est_curvature && geom_consistency) */
 } orc_outputs;
 
 /* PatchMatchACMMCuda(options, problem) + Run() on the CPU, rows [row_begin,

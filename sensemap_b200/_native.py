@@ -18,8 +18,8 @@ PIX_U8, PIX_F32 = 0, 1
 STORE_U8, STORE_F16, STORE_F32 = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 (KERNEL_CONVERT, KERNEL_PREP, KERNEL_INIT, KERNEL_INIT_CONF, KERNEL_SWEEP, KERNEL_LOCAL_OPT, KERNEL_MASK,
- KERNEL_FILTER) = range(8)
-KERNEL_NAMES = ["convert", "prep_ref", "init", "init_conf", "sweep", "local_opt", "mask", "filter"]
+ KERNEL_FILTER, KERNEL_POST) = range(9)
+KERNEL_NAMES = ["convert", "prep_ref", "init", "init_conf", "sweep", "local_opt", "mask", "filter", "post"]
 
 STATUS_NAMES = {0: "SMVS_OK", 1: "SMVS_EINVAL", 2: "SMVS_ENOMEM", 3: "SMVS_ECUDA", 4: "SMVS_ESTATE",
                 5: "SMVS_EIO", 6: "SMVS_ETIMEDOUT", 7: "SMVS_ECANCELED"}
@@ -75,6 +75,10 @@ class smvs_problem(C.Structure):
     ]
 
 
+class smvs_tuning(C.Structure):
+    _fields_ = [("sweep_block_x", C.c_int)]
+
+
 class smvs_device_maps(C.Structure):
     _fields_ = [
         ("width", C.c_int), ("height", C.c_int), ("num_src", C.c_int),
@@ -101,6 +105,7 @@ _SIGNATURES = {
     "smvs_synchronize": (C.c_int, [C.c_void_p]),
     "smvs_launch_count": (C.c_int64, [C.c_void_p]),
     "smvs_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "smvs_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(smvs_tuning)]),
     "smvs_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "smvs_destroy": (None, [C.c_void_p]),
     "smvs_last_error": (C.c_char_p, []),

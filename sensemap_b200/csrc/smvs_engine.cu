@@ -152,6 +152,8 @@ struct smvs_engine {
   float* d_init_depth = nullptr;   // ref.depth as given (init / RunFilter input)
   float* d_init_normal = nullptr;  // ref.normal as given
   uint8_t* d_mask = nullptr;
+  uint16_t* d_curv = nullptr;   // 2*W*H (est_curvature && geom_consistency)
+  float* d_ggrad = nullptr;     // W*H (median_filter)
   bool has_init = false;
   bool has_src_depth = false;
   // Optional per-launch timing (smvs_set_profiling): CUDA events around each
@@ -210,6 +212,9 @@ int CheckLaunch(smvs_engine* e, cudaError_t err, const char* what) {
 // events when profiling is on.
 template <typename Fn>
 int Launch(smvs_engine* e, int kind, const char* what, Fn fn) {
+  // Clear a launch error another library may have left on this thread, so a
+  // failure is only reported against the launch that caused it.
+  (void)cudaGetLastError();
   cudaEvent_t a = nullptr, b = nullptr;
   if (e->profiling) {
     if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess)
@@ -370,6 +375,7 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   p.random_opt = opt->random_optimization;
   p.geom = opt->geom_consistency;
   p.thk = opt->thk < N ? opt->thk : N;  // patch_match_cuda.cu:949-950
+  p.block_x = 32;
   p.geom_reg = (float)opt->geom_consistency_regularizer;
   p.geom_max = (float)opt->geom_consistency_max_cost;
   const float* K = prob->ref.K;
@@ -460,6 +466,8 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
     e->has_init = (prob->ref.normal != nullptr);
   }
   if (prob->ref_mask) TRY(StageIn(e, prob->ref_mask, WH, prob->memory, (void**)&e->d_mask));
+  if (opt->est_curvature && opt->geom_consistency) TRY(e->Alloc((void**)&e->d_curv, 2 * WH * sizeof(uint16_t)));
+  if (opt->median_filter) TRY(e->Alloc((void**)&e->d_ggrad, WH * sizeof(float)));
   // Source pixels/depths staged from host memory must stay valid until the
   // copies complete; the caller's buffers are only guaranteed during this call.
   if (prob->memory == SMVS_MEM_HOST) {
@@ -503,6 +511,26 @@ int smvs_run(smvs_engine* e) {
       }
     }
   }
+  // Post-processing in the reference's order (patch_match_cuda.cu:985-1052).
+  if (e->d_curv && (st = Launch(e, SMVS_KERNEL_POST, "curvature",
+                                [&] { return smvs::LaunchCurvature(p, e->d_curv, e->stream); })))
+    return st;
+  if (o.median_filter) {
+    if ((st = Launch(e, SMVS_KERNEL_POST, "geometric gradient",
+                     [&] { return smvs::LaunchGeomGradient(p, e->d_ggrad, e->stream); })))
+      return st;
+    for (int colour = 0; colour < 2; ++colour)
+      if ((st = Launch(e, SMVS_KERNEL_POST, "median filter", [&] {
+             return smvs::LaunchMedianFilter(p, e->d_ggrad, o.depth_diff_threshold, colour, e->stream);
+           })))
+        return st;
+  }
+  if (o.filter && o.conf_filter)
+    for (int colour = 0; colour < 2; ++colour)
+      if ((st = Launch(e, SMVS_KERNEL_POST, "confidence filter", [&] {
+             return smvs::LaunchConfFilter(p, o.depth_diff_threshold, o.conf_threshold, colour, e->stream);
+           })))
+        return st;
   if (e->d_mask && (st = Launch(e, SMVS_KERNEL_MASK, "mask", [&] { return smvs::LaunchMask(p, e->d_mask, e->stream); })))
     return st;
   e->ran = true;
@@ -555,8 +583,9 @@ int smvs_get_view_sel_map(smvs_engine* e, uint32_t* out) {
   return CopyOut(e, out, e->d_view_sel, (size_t)e->W * e->H * sizeof(uint32_t), true);
 }
 int smvs_get_curvature_map(smvs_engine* e, uint16_t* out) {
-  (void)e; (void)out;
-  return Fail(SMVS_EINVAL, "curvature map not available (est_curvature is not supported by this build)");
+  if (!e) return Fail(SMVS_EINVAL, "null engine");
+  if (!e->d_curv) return Fail(SMVS_EINVAL, "curvature map needs est_curvature and geom_consistency");
+  return CopyOut(e, out, e->d_curv, 2 * (size_t)e->W * e->H * sizeof(uint16_t), true);
 }
 int smvs_get_size(const smvs_engine* e, int* w, int* h, int* n) {
   if (!e) return Fail(SMVS_EINVAL, "null engine");
@@ -577,6 +606,14 @@ int smvs_synchronize(smvs_engine* e) {
   return SMVS_OK;
 }
 int64_t smvs_launch_count(const smvs_engine* e) { return e ? e->launches : -1; }
+
+int smvs_set_tuning(smvs_engine* e, const smvs_tuning* t) {
+  if (!e || !t) return Fail(SMVS_EINVAL, "null argument");
+  const int bx = t->sweep_block_x;
+  if (bx != 8 && bx != 16 && bx != 32 && bx != 64) return Fail(SMVS_EINVAL, "sweep_block_x must be 8, 16, 32 or 64");
+  e->jp.block_x = bx;
+  return SMVS_OK;
+}
 
 int smvs_set_profiling(smvs_engine* e, int enable) {
   if (!e) return Fail(SMVS_EINVAL, "null engine");

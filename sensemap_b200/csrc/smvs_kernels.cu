@@ -110,6 +110,164 @@ __global__ void InitKernel(JobParams p, int random_init, float dmin, float dmax)
   p.view_sel[pix] = 0u;
 }
 
+
+// ComputeCurvatureMap, kernel_functions.cu:1603-1653: slice 0 = Scharr gradient
+// of the reference x 1e4 (clamped to 32767), slice 1 = median angle between
+// the normal and its 5x5 neighbours x 1e4.
+__global__ void CurvatureKernel(JobParams p, uint16_t* __restrict__ curv) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const size_t WH = (size_t)p.W * p.H;
+  const size_t pix = (size_t)row * p.W + col;
+  const float kx[3][3] = {{-3, 0, 3}, {-10, 0, 10}, {-3, 0, 3}};
+  const float ky[3][3] = {{-3, -10, -3}, {0, 0, 0}, {3, 10, 3}};
+  float gx = 0.f, gy = 0.f;
+#pragma unroll
+  for (int dr = -1; dr <= 1; ++dr)
+#pragma unroll
+    for (int dc = -1; dc <= 1; ++dc) {
+      const float color = RefAt(p.ref, p.W, p.H, row + dr, col + dc);
+      gx += color * kx[dr + 1][dc + 1];
+      gy += color * ky[dr + 1][dc + 1];
+    }
+  const float grad = sqrtf(gx * gx + gy * gy);
+  const int min_x = max(col - 2, 0), max_x = min(col + 2, p.W - 1);
+  const int min_y = max(row - 2, 0), max_y = min(row + 2, p.H - 1);
+  const float n0 = p.normal[pix], n1 = p.normal[WH + pix], n2 = p.normal[2 * WH + pix];
+  float angles[24];
+  int cnt = 0;
+  for (int y = min_y; y <= max_y; ++y)
+    for (int x = min_x; x <= max_x; ++x) {
+      if (y == row && x == col) continue;
+      const size_t q = (size_t)y * p.W + x;
+      angles[cnt++] = acosf(n0 * p.normal[q] + n1 * p.normal[WH + q] + n2 * p.normal[2 * WH + q]);
+    }
+  curv[pix] = (uint16_t)fminf(grad * 10000.f, 32767.f);
+  float med = 3.14159265358979323846f * 10000.0f;
+  if (cnt > 0) {
+    for (int i = 0; i < cnt - 1; ++i)  // BubbleSort, utils.h:190-209
+      for (int j = 0; j < cnt - 1 - i; ++j)
+        if (angles[j] > angles[j + 1]) { const float t = angles[j]; angles[j] = angles[j + 1]; angles[j + 1] = t; }
+    med = angles[cnt / 2] * 10000.0f;
+  }
+  // Float to uint16 the way the hardware converts (NaN -> 0, saturating).
+  curv[WH + pix] = (med != med) ? (uint16_t)0 : (uint16_t)fminf(fmaxf(med, 0.f), 65535.f);
+}
+
+// ComputeGeomGradientMap, kernel_functions.cu:3095-3120 (pixels without depth
+// get 0; the reference leaves them unwritten).
+__global__ void GeomGradientKernel(JobParams p, float* __restrict__ ggrad) {
+  const int col = blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  if (col >= p.W || row >= p.H) return;
+  const size_t pix = (size_t)row * p.W + col;
+  const float depth = p.depth[pix];
+  if (depth <= 0) { ggrad[pix] = 0.f; return; }
+  const float kx[3][3] = {{-3, 0, 3}, {-10, 0, 10}, {-3, 0, 3}};
+  const float ky[3][3] = {{-3, -10, -3}, {0, 0, 0}, {3, 10, 3}};
+  float gx = 0.f, gy = 0.f;
+  for (int dr = -1; dr <= 1; ++dr)
+    for (int dc = -1; dc <= 1; ++dc) {
+      const int nr = row + dr, nc = col + dc;
+      if (nr < 0 || nr >= p.H || nc < 0 || nc >= p.W) continue;
+      const float diff = fabsf(p.depth[(size_t)nr * p.W + nc] - depth) / depth;
+      gx += diff * kx[dr + 1][dc + 1];
+      gy += diff * ky[dr + 1][dc + 1];
+    }
+  ggrad[pix] = sqrtf(gx * gx + gy * gy);
+}
+
+// MedianFilter via Black/RedPixelFilter, kernel_functions.cu:3122-3280: edge-aware
+// median of depth and of each normal component over up to 17 taps.
+__global__ void MedianFilterKernel(JobParams p, const float* __restrict__ ggrad, float diff_thres, int colour) {
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  const int col = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;
+  const int W = p.W, H = p.H;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  const float grad_thres = 1.4f * diff_thres;
+  float depths[17], nx[17], ny[17], nz[17];
+  const float grad = ggrad[pix];
+  const float cdepth = p.depth[pix];
+  const float inv_cdepth = 1.0f / cdepth;
+  int index = 0;
+  depths[index] = cdepth;
+  nx[index] = p.normal[pix]; ny[index] = p.normal[WH + pix]; nz[index] = p.normal[2 * WH + pix];
+  index++;
+  auto take = [&](int nr, int nc) {
+    const size_t q = (size_t)nr * W + nc;
+    depths[index] = p.depth[q];
+    const float diff = fabsf(depths[index] - cdepth) * inv_cdepth;
+    if (grad < grad_thres || (grad >= grad_thres && diff < diff_thres)) {
+      nx[index] = p.normal[q]; ny[index] = p.normal[WH + q]; nz[index] = p.normal[2 * WH + q];
+      index++;
+    }
+  };
+  for (int i = 0; i < 2; ++i) {
+    const int o = 2 * i + 1;
+    if (row - o >= 0) take(row - o, col);
+    if (row + o < H) take(row + o, col);
+    if (col - o >= 0) take(row, col - o);
+    if (col + o < W) take(row, col + o);
+  }
+  const int dirs[8][2] = {{-2, 1}, {-1, 2}, {1, 2}, {2, 1}, {2, -1}, {1, -2}, {-1, -2}, {-2, -1}};
+  for (int i = 0; i < 8; ++i) {
+    const int nr = row + dirs[i][0], nc = col + dirs[i][1];
+    if (nr >= 0 && nr < H && nc >= 0 && nc < W) take(nr, nc);
+  }
+  auto sort = [&](float* v) {
+    for (int i = 0; i < index - 1; ++i)
+      for (int j = 0; j < index - 1 - i; ++j)
+        if (v[j] > v[j + 1]) { const float t = v[j]; v[j] = v[j + 1]; v[j + 1] = t; }
+  };
+  sort(depths); sort(nx); sort(ny); sort(nz);
+  const int nth = index >> 1;
+  const float inv_norm = rsqrtf(nx[nth] * nx[nth] + ny[nth] * ny[nth] + nz[nth] * nz[nth]);
+  p.depth[pix] = depths[nth];
+  p.normal[pix] = nx[nth] * inv_norm;
+  p.normal[WH + pix] = ny[nth] * inv_norm;
+  p.normal[2 * WH + pix] = nz[nth] * inv_norm;
+}
+
+// FilterDepthMap (confidence and planar-neighbour filter), kernel_functions.cu:
+// 3282-3354, one checkerboard colour per launch. [quirk] the reference's grid
+// covers rows r with r/2 < ceil((H/2)/16)*16, which skips the last row when H is
+// odd and H/2 is a multiple of 16; the same rows are skipped here.
+__global__ void ConfFilterKernel(JobParams p, float depth_thres, float conf_thres, int colour, int row_pairs) {
+  const int row = blockIdx.y * blockDim.y + threadIdx.y;
+  const int col = 2 * (blockIdx.x * blockDim.x + threadIdx.x) + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H || (row >> 1) >= row_pairs) return;
+  const int W = p.W, H = p.H;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  const float depth = p.depth[pix];
+  if (depth <= 0) return;
+  const float n[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const float conf = p.conf[pix];
+  const float* iK = p.refiK;
+  const float pt[3] = {depth * (iK[0] * col + iK[1]), depth * (iK[2] * row + iK[3]), depth};
+  int good = 0;
+  for (int i = 0; i < 4; ++i) {
+    const int u = col + (i == 0 ? -1 : (i == 2 ? 1 : 0)), v = row + (i == 1 ? -1 : (i == 3 ? 1 : 0));
+    if (u < 0 || u >= W || v < 0 || v >= H) continue;
+    const size_t q = (size_t)v * W + u;
+    const float nd = p.depth[q];
+    const float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
+    const float nconf = p.conf[q];
+    const float np[3] = {nd * (iK[0] * u + iK[1]), nd * (iK[2] * v + iK[3]), nd};
+    const float d1 = fabsf((pt[0] - np[0]) * n[0] + (pt[1] - np[1]) * n[1] + (pt[2] - np[2]) * n[2]);
+    const float d2 = fabsf((pt[0] - np[0]) * nn[0] + (pt[1] - np[1]) * nn[1] + (pt[2] - np[2]) * nn[2]);
+    if ((conf < conf_thres && d1 / depth < depth_thres) || (nconf < conf_thres && d2 / nd < depth_thres)) good++;
+  }
+  if (good < 2) {
+    p.depth[pix] = 0.f;
+    p.normal[pix] = 0.f; p.normal[WH + pix] = 0.f; p.normal[2 * WH + pix] = 0.f;
+    p.conf[pix] = 0.f;
+  }
+}
+
 // MaskDepthMapKernel, kernel_functions.cu:3080-3093 ([quirk] last row and
 // column are left untouched).
 __global__ void MaskKernel(JobParams p, const uint8_t* __restrict__ mask) {
@@ -193,6 +351,33 @@ cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream) {
 
 cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream) {
   return LaunchWindowOp(p, 2, colour, stream);
+}
+
+cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  CurvatureKernel<<<grid, block, 0, stream>>>(p, curv);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchGeomGradient(const JobParams& p, float* ggrad, cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
+  GeomGradientKernel<<<grid, block, 0, stream>>>(p, ggrad);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchMedianFilter(const JobParams& p, const float* ggrad, float diff_thres, int colour,
+                               cudaStream_t stream) {
+  dim3 block(32, 8), grid((p.W + 63) / 64, (p.H + 7) / 8);
+  MedianFilterKernel<<<grid, block, 0, stream>>>(p, ggrad, diff_thres, colour);
+  return cudaGetLastError();
+}
+
+cudaError_t LaunchConfFilter(const JobParams& p, float depth_thres, float conf_thres, int colour,
+                             cudaStream_t stream) {
+  const int row_pairs = ((p.H / 2) + 15) / 16 * 16;  // the reference's grid, patch_match_cuda.cu:1018-1037
+  dim3 block(32, 8), grid((p.W + 63) / 64, (p.H + 7) / 8);
+  ConfFilterKernel<<<grid, block, 0, stream>>>(p, depth_thres, conf_thres, colour, row_pairs);
+  return cudaGetLastError();
 }
 
 cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream) {

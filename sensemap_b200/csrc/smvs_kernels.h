@@ -21,6 +21,7 @@ struct JobParams {
   float geom_reg, geom_max;
   float refK[4], refiK[4];
   uint64_t stage_key;
+  int block_x;             // checkerboard kernels: threads per block in x (256 / block_x in y)
   // State maps (dense row-major; normal and cost planar).
   float* depth;
   float* normal;
@@ -46,6 +47,10 @@ cudaError_t LaunchInitConf(const JobParams& p, cudaStream_t stream);
 cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream);
 cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream);
 cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream);
+cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream);
+cudaError_t LaunchGeomGradient(const JobParams& p, float* ggrad, cudaStream_t stream);
+cudaError_t LaunchMedianFilter(const JobParams& p, const float* ggrad, float diff_thres, int colour, cudaStream_t stream);
+cudaError_t LaunchConfFilter(const JobParams& p, float depth_thres, float conf_thres, int colour, cudaStream_t stream);
 cudaError_t LaunchFilterDepthMaps(const JobParams& p, const float* in_depth, float* out_depth, int min_consistent,
                                   float filter_max_cost, int dedup, cudaStream_t stream);
 

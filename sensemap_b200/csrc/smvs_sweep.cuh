@@ -16,8 +16,7 @@ namespace smvs {
 namespace detail {
 namespace {  // internal linkage: every window translation unit gets its own copy
 
-constexpr int kBX = 32;  // threads per block in x
-constexpr int kBY = 8;   // threads per block in y
+constexpr int kThreads = 256;  // threads per block; the block's x/y split is a tuning knob (JobParams)
 
 __constant__ float kMWeights[5] = {0.f, 1.f, 2.01f, 3.03f, 4.06f};  // kernel_functions.cu:22
 __constant__ int kNeighborOffs[4][2] = {{0, -1}, {-1, 0}, {0, 1}, {1, 0}};  // :23-25 (first four)
@@ -69,17 +68,21 @@ __device__ __forceinline__ float NccCost(cudaTextureObject_t tex, const float* p
   float bcol = col_src, brow = row_src, bz = z;
   const float h0 = S * Hm[0], h1 = S * Hm[1], h3 = S * Hm[3], h4 = S * Hm[4], h6 = S * Hm[6], h7 = S * Hm[7];
   float ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f;
-#pragma unroll
+  // Window rows stay rolled and the taps of a row are unrolled: one copy of
+  // the tap code per call site keeps the kernel inside the instruction cache.
+#pragma unroll 1
   for (int dr = -R; dr <= R; dr += S) {
+    const float* wrow = win + (dr + R) * ws + R;
+    const float sr = (float)(dr * dr);
 #pragma unroll
     for (int dc = -R; dc <= R; dc += S) {
       const float iz = 1.0f / z;
       const float fu = iz * col_src + 0.5f;
       const float fv = iz * row_src + 0.5f;
-      const float rc = win[(dr + R) * ws + (dc + R)];
+      const float rc = wrow[dc];
       const float sc = tex2D<float>(tex, fu, fv);
       const float cd = center - rc;
-      const float wgt = __expf(-(float)(dr * dr + dc * dc) * sn - cd * cd * cn);
+      const float wgt = __expf(-(sr + (float)(dc * dc)) * sn - cd * cd * cn);
       const float wsc = wgt * sc;
       ss += wsc;
       sss += wsc * sc;
@@ -109,20 +112,22 @@ struct PixRef {
 
 template <int R, int S>
 __device__ __forceinline__ float ViewCost(const JobParams& p, const float* poses, int v, int row, int col,
-                                          float depth, const float n[3], const float np[3], const PixRef& pr) {
+                                          float depth, const float n[3], const float np[3], const PixRef& pr,
+                                          const float* Kgeom) {
   const float* pose = poses + v * SMVS_POSE_FLOATS;
   float cost = NccCost<R, S>(p.src_tex[v], pose, row, col, depth, n, p.refiK, p.W, p.H, pr.center, pr.rsum,
                              pr.rvar, pr.win, pr.ws, p.sn, p.cn);
   if (p.geom)
-    cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, p.refK, p.geom_max);
+    cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, Kgeom, p.geom_max);
   return cost;
 }
 
 // InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior).
 template <int R, int S>
-__global__ void __launch_bounds__(kBX * kBY) InitConfKernel(JobParams p) {
+__global__ void __launch_bounds__(kThreads) InitConfKernel(JobParams p) {
   extern __shared__ float smem[];
-  constexpr int tw = kBX + 2 * R, th = kBY + 2 * R;
+  const int kBX = blockDim.x, kBY = blockDim.y;
+  const int tw = kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
   const int col0 = blockIdx.x * kBX, row0 = blockIdx.y * kBY;
@@ -144,7 +149,7 @@ __global__ void __launch_bounds__(kBX * kBY) InitConfKernel(JobParams p) {
   float costs[SMVS_MAX_SRC];
   int order[SMVS_MAX_SRC];
   for (int v = 0; v < p.N; ++v) {
-    costs[v] = ViewCost<R, S>(p, poses, v, row, col, depth, n, np, pr);
+    costs[v] = ViewCost<R, S>(p, poses, v, row, col, depth, n, np, pr, p.refK);
     order[v] = v;
     p.cost[(size_t)v * WH + pix] = costs[v];
   }
@@ -168,9 +173,10 @@ __global__ void __launch_bounds__(kBX * kBY) InitConfKernel(JobParams p) {
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
 // propagate_depth): one checkerboard colour, one thread per pixel.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kBX * kBY) SweepKernel(JobParams p, int colour) {
+__global__ void __launch_bounds__(kThreads) SweepKernel(JobParams p, int colour) {
   extern __shared__ float smem[];
-  constexpr int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
+  const int kBX = blockDim.x, kBY = blockDim.y;
+  const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
   const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
@@ -257,95 +263,98 @@ __global__ void __launch_bounds__(kBX * kBY) SweepKernel(JobParams p, int colour
   pr.win = tile + threadIdx.y * tw + (col - col0);
   float M[kMaxHyp][NB];
   for (int v = 0; v < N; ++v) M[0][v] = p.cost[(size_t)v * WH + pix];
-  for (int h = 1; h < ns; ++h)
-    for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr);
-
-  // ACMM view selection, :2364-2427.
-  uint32_t flags = 0;
-  float probs[NB];
-  for (int v = 0; v < N; ++v) {
-    unsigned n1 = 0, n2 = 0;
-    float pv = 0.f;
-    for (int h = 0; h < ns; ++h) {
-      const float cst = M[h][v];
-      pv += __expf(-cst * cst * p.inv_beta2);
-      n1 += (cst < p.th_mc);
-      n2 += (cst > p.max_mc);
-    }
-    probs[v] = pv;
-    if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
-  }
-  if (flags == 0) return;
-  for (int v = 0; v < N; ++v)
-    if (!((flags >> v) & 1u)) probs[v] = 0.f;
-  {
-    float sum = 0.f;
-    for (int v = 0; v < N; ++v) sum += probs[v];
-    const float inv = 1.0f / sum;
-    float cum = 0.f;
-    for (int v = 0; v < N; ++v) { cum += probs[v] * inv; probs[v] = cum; }
-  }
   float vw[NB];
-  for (int v = 0; v < N; ++v) vw[v] = 0.f;
-  for (int s = 0; s < p.num_samples; ++s) {
-    const float rp = r.Uniform() - FLT_EPSILON;
-    for (int v = 0; v < N; ++v)
-      if (probs[v] > rp) {
-        if (p.random_opt) vw[v] = 1.0f; else vw[v] += 1.0f;
-        break;
-      }
-  }
-  float wn = 0.f;
-  for (int v = 0; v < N; ++v) wn += vw[v];
-  if (wn <= 1e-5f) return;
-  const float iwn = 1.0f / wn;
-  uint32_t sel = 0;
-  for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
   float costs[kMaxHyp];
-  for (int h = 0; h < ns; ++h) {
+  // Two evaluation phases share one call site of the cost code: phase 0 scores
+  // the propagated hypotheses 1..ns-1, phase 1 the refinement hypotheses 1..4.
+  int h_end = ns;
+  for (int phase = 0; phase < 2; ++phase) {
+    for (int h = 1; h < h_end; ++h)
+      for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr, p.refK);
+    if (phase == 1) break;
+
+    // ACMM view selection, :2364-2427.
+    uint32_t flags = 0;
+    float probs[NB];
+    for (int v = 0; v < N; ++v) {
+      unsigned n1 = 0, n2 = 0;
+      float pv = 0.f;
+      for (int h = 0; h < ns; ++h) {
+        const float cst = M[h][v];
+        pv += __expf(-cst * cst * p.inv_beta2);
+        n1 += (cst < p.th_mc);
+        n2 += (cst > p.max_mc);
+      }
+      probs[v] = pv;
+      if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
+    }
+    if (flags == 0) return;
+    for (int v = 0; v < N; ++v)
+      if (!((flags >> v) & 1u)) probs[v] = 0.f;
+    {
+      float sum = 0.f;
+      for (int v = 0; v < N; ++v) sum += probs[v];
+      const float inv = 1.0f / sum;
+      float cum = 0.f;
+      for (int v = 0; v < N; ++v) { cum += probs[v] * inv; probs[v] = cum; }
+    }
+    for (int v = 0; v < N; ++v) vw[v] = 0.f;
+    for (int s = 0; s < p.num_samples; ++s) {
+      const float rp = r.Uniform() - FLT_EPSILON;
+      for (int v = 0; v < N; ++v)
+        if (probs[v] > rp) {
+          if (p.random_opt) vw[v] = 1.0f; else vw[v] += 1.0f;
+          break;
+        }
+    }
+    float wn = 0.f;
+    for (int v = 0; v < N; ++v) wn += vw[v];
+    if (wn <= 1e-5f) return;
+    const float iwn = 1.0f / wn;
+    uint32_t sel = 0;
+    for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
+    for (int h = 0; h < ns; ++h) {
+      float cs = 0.f;
+      for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
+      costs[h] = cs;
+    }
+    p.view_sel[pix] = sel;
+    int mi = -1;
+    {
+      float m = FLT_MAX;
+      for (int h = 0; h < ns; ++h)
+        if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
+    }
+    if (mi < 0) return;
+    depth = hyp[mi][3];
+    normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
+    if (mi != 0)
+      for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
+
+    // Refinement hypotheses, :2449-2486.
+    float nn[3];
+    const float pd_min = (1.0f - p.rand_depth_ratio) * depth, pd_max = (1.0f + p.rand_depth_ratio) * depth;
+    const float ndepth = r.Uniform() * (pd_max - pd_min) + pd_min;  // PerturbDepth :141-147
+    PerturbNormalACMH(normal, nn, a1, a2, r);
+    CorrectNormal(nn, vd, ivl);
+    const float rdepth = r.Uniform() * (depth_max - depth_min) + depth_min;
+    float rn[3];
+    RandomNormal(r, vd, rn);
+    CorrectNormal(rn, vd, ivl);
+    hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
+    hyp[1][0] = nn[0]; hyp[1][1] = nn[1]; hyp[1][2] = nn[2]; hyp[1][3] = depth;
+    hyp[2][0] = normal[0]; hyp[2][1] = normal[1]; hyp[2][2] = normal[2]; hyp[2][3] = ndepth;
+    hyp[3][0] = rn[0]; hyp[3][1] = rn[1]; hyp[3][2] = rn[2]; hyp[3][3] = depth;
+    hyp[4][0] = normal[0]; hyp[4][1] = normal[1]; hyp[4][2] = normal[2]; hyp[4][3] = rdepth;
+    h_end = 5;
+  }
+  // :2488-2559: weighted refinement costs, argmin, write back.
+  for (int h = 0; h < 5; ++h) {
     float cs = 0.f;
     for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
     costs[h] = cs;
   }
-  p.view_sel[pix] = sel;
   int mi = -1;
-  {
-    float m = FLT_MAX;
-    for (int h = 0; h < ns; ++h)
-      if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
-  }
-  if (mi < 0) return;
-  depth = hyp[mi][3];
-  normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
-
-  // Refinement, :2449-2520.
-  float nn[3];
-  const float pd_min = (1.0f - p.rand_depth_ratio) * depth, pd_max = (1.0f + p.rand_depth_ratio) * depth;
-  const float ndepth = r.Uniform() * (pd_max - pd_min) + pd_min;  // PerturbDepth :141-147
-  PerturbNormalACMH(normal, nn, a1, a2, r);
-  CorrectNormal(nn, vd, ivl);
-  const float rdepth = r.Uniform() * (depth_max - depth_min) + depth_min;
-  float rn[3];
-  RandomNormal(r, vd, rn);
-  CorrectNormal(rn, vd, ivl);
-  float rh[5][4] = {{normal[0], normal[1], normal[2], depth},
-                    {nn[0], nn[1], nn[2], depth},
-                    {normal[0], normal[1], normal[2], ndepth},
-                    {rn[0], rn[1], rn[2], depth},
-                    {normal[0], normal[1], normal[2], rdepth}};
-  if (mi != 0)
-    for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
-  costs[0] = 0.f;
-  for (int v = 0; v < N; ++v) costs[0] += vw[v] * M[0][v];
-  for (int h = 1; h < 5; ++h) {
-    float cs = 0.f;
-    for (int v = 0; v < N; ++v) {
-      M[h][v] = ViewCost<R, S>(p, poses, v, row, col, rh[h][3], rh[h], vd, pr);
-      cs += vw[v] * M[h][v];
-    }
-    costs[h] = cs;
-  }
-  mi = -1;
   {
     float m = FLT_MAX;
     for (int h = 0; h < 5; ++h)
@@ -353,17 +362,18 @@ __global__ void __launch_bounds__(kBX * kBY) SweepKernel(JobParams p, int colour
   }
   if (mi != -1) {
     p.conf[pix] = costs[mi];
-    p.depth[pix] = rh[mi][3];
-    p.normal[pix] = rh[mi][0]; p.normal[WH + pix] = rh[mi][1]; p.normal[2 * WH + pix] = rh[mi][2];
+    p.depth[pix] = hyp[mi][3];
+    p.normal[pix] = hyp[mi][0]; p.normal[WH + pix] = hyp[mi][1]; p.normal[2 * WH + pix] = hyp[mi][2];
     for (int v = 0; v < N; ++v) p.cost[(size_t)v * WH + pix] = M[mi][v];
   }
 }
 
 // LocalOptimization, kernel_functions.cu:2736-2931.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kBX * kBY) LocalOptKernel(JobParams p, int colour) {
+__global__ void __launch_bounds__(kThreads) LocalOptKernel(JobParams p, int colour) {
   extern __shared__ float smem[];
-  constexpr int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
+  const int kBX = blockDim.x, kBY = blockDim.y;
+  const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
   const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
@@ -406,17 +416,35 @@ __global__ void __launch_bounds__(kBX * kBY) LocalOptKernel(JobParams p, int col
   float M[5][NB];
   float hyp[5][4];
   int mi = -1;
-  for (int it = 0; it < 5; ++it) {
-    hyp[it][3] = r.Uniform() * (hi - lo) + lo;
-    PerturbNormalACMH(m, hyp[it], a1, a2, r);
+  // Rounds 0..4 score five random hypotheses on the selected views; round 5
+  // rescores the winner on the unselected views. One call site of the cost code.
+  for (int it = 0; it < 6; ++it) {
+    float hcur[4];
+    if (it < 5) {
+      hyp[it][3] = r.Uniform() * (hi - lo) + lo;
+      PerturbNormalACMH(m, hyp[it], a1, a2, r);
+      hcur[0] = hyp[it][0]; hcur[1] = hyp[it][1]; hcur[2] = hyp[it][2]; hcur[3] = hyp[it][3];
+    } else {
+      if (mi == -1) break;
+      hcur[0] = normal[0]; hcur[1] = normal[1]; hcur[2] = normal[2]; hcur[3] = depth;
+    }
+    // [quirk] :2916-2919 passes the inverse intrinsics where K is expected when
+    // rescoring the unselected views.
+    const float* Kg = (it < 5) ? p.refK : p.refiK;
     float mconf = 0.f, mw = 0.f;
     for (int v = 0; v < N; ++v) {
-      if (!((sel >> v) & 1u)) continue;
-      const float cost = ViewCost<R, S>(p, poses, v, row, col, hyp[it][3], hyp[it], np, pr);
-      M[it][v] = cost;
-      mconf += cost;
-      mw += 1.f;
+      const bool selected = (sel >> v) & 1u;
+      if (selected != (it < 5)) continue;
+      const float cost = ViewCost<R, S>(p, poses, v, row, col, hcur[3], hcur, np, pr, Kg);
+      if (it < 5) {
+        M[it][v] = cost;
+        mconf += cost;
+        mw += 1.f;
+      } else {
+        p.cost[(size_t)v * WH + pix] = cost;
+      }
     }
+    if (it == 5) break;
     if (mw <= 0.f) return;
     mconf /= mw;
     if (mconf < conf) {
@@ -430,38 +458,28 @@ __global__ void __launch_bounds__(kBX * kBY) LocalOptKernel(JobParams p, int col
     p.conf[pix] = conf;
     p.depth[pix] = depth;
     p.normal[pix] = normal[0]; p.normal[WH + pix] = normal[1]; p.normal[2 * WH + pix] = normal[2];
-    for (int v = 0; v < N; ++v) {
-      if ((sel >> v) & 1u) {
-        p.cost[(size_t)v * WH + pix] = M[mi][v];
-      } else {
-        const float* pose = poses + v * SMVS_POSE_FLOATS;
-        float cost = NccCost<R, S>(p.src_tex[v], pose, row, col, depth, normal, p.refiK, W, H, pr.center, pr.rsum,
-                                   pr.rvar, pr.win, pr.ws, p.sn, p.cn);
-        // [quirk] :2916-2919 passes the inverse intrinsics where K is expected.
-        if (p.geom)
-          cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, p.refiK, p.geom_max);
-        p.cost[(size_t)v * WH + pix] = cost;
-      }
-    }
+    for (int v = 0; v < N; ++v)
+      if ((sel >> v) & 1u) p.cost[(size_t)v * WH + pix] = M[mi][v];
   }
 }
 
 template <int R, int S>
-size_t SweepSmem(int N) {
-  return sizeof(float) * ((2 * kBX + 2 * R) * (kBY + 2 * R) + N * SMVS_POSE_FLOATS);
+size_t SweepSmem(int N, int bx, int by) {
+  return sizeof(float) * ((2 * bx + 2 * R) * (by + 2 * R) + N * SMVS_POSE_FLOATS);
 }
 
-dim3 SweepGrid(const JobParams& p) {
-  return dim3((unsigned)((p.W + 2 * kBX - 1) / (2 * kBX)), (unsigned)((p.H + kBY - 1) / kBY));
+dim3 SweepGrid(const JobParams& p, int bx, int by) {
+  return dim3((unsigned)((p.W + 2 * bx - 1) / (2 * bx)), (unsigned)((p.H + by - 1) / by));
 }
 
 template <int R, int S, int NB>
 cudaError_t LaunchSweepT(const JobParams& p, int colour, bool local, cudaStream_t stream) {
-  const size_t smem = SweepSmem<R, S>(p.N);
+  const int bx = p.block_x, by = kThreads / p.block_x;
+  const size_t smem = SweepSmem<R, S>(p.N, bx, by);
   if (local)
-    LocalOptKernel<R, S, NB><<<SweepGrid(p), dim3(kBX, kBY), smem, stream>>>(p, colour);
+    LocalOptKernel<R, S, NB><<<SweepGrid(p, bx, by), dim3(bx, by), smem, stream>>>(p, colour);
   else
-    SweepKernel<R, S, NB><<<SweepGrid(p), dim3(kBX, kBY), smem, stream>>>(p, colour);
+    SweepKernel<R, S, NB><<<SweepGrid(p, bx, by), dim3(bx, by), smem, stream>>>(p, colour);
   return cudaGetLastError();
 }
 
@@ -474,9 +492,10 @@ cudaError_t LaunchSweepNB(const JobParams& p, int colour, bool local, cudaStream
 
 template <int R, int S>
 cudaError_t LaunchInitConfT(const JobParams& p, cudaStream_t stream) {
-  const size_t smem = sizeof(float) * ((kBX + 2 * R) * (kBY + 2 * R) + p.N * SMVS_POSE_FLOATS);
-  dim3 grid((p.W + kBX - 1) / kBX, (p.H + kBY - 1) / kBY);
-  InitConfKernel<R, S><<<grid, dim3(kBX, kBY), smem, stream>>>(p);
+  const int bx = 32, by = kThreads / 32;
+  const size_t smem = sizeof(float) * ((bx + 2 * R) * (by + 2 * R) + p.N * SMVS_POSE_FLOATS);
+  dim3 grid((p.W + bx - 1) / bx, (p.H + by - 1) / by);
+  InitConfKernel<R, S><<<grid, dim3(bx, by), smem, stream>>>(p);
   return cudaGetLastError();
 }
 

@@ -267,6 +267,10 @@ class PatchMatchACMMCuda:
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_launch_count(self._h))
 
+    def SetTuning(self, sweep_block_x: int) -> None:
+        t = N.smvs_tuning(sweep_block_x=sweep_block_x)
+        N.check(N.lib().smvs_set_tuning(self._h, C.byref(t)))
+
     def SetProfiling(self, enable: bool = True) -> None:
         N.check(N.lib().smvs_set_profiling(self._h, int(enable)))
 

@@ -106,3 +106,35 @@ def test_missing_library_fails_loudly(monkeypatch, tmp_path):
     monkeypatch.setattr(N, "_LIB", None)
     with pytest.raises(N.NativeLibraryError):
         N.lib()
+
+
+def test_cpp_wrapper_compiles_and_links(tmp_path):
+    """include/smvs.hpp (the C++ shape of the reference operator) compiles
+    against the C ABI and links the in-tree library; only GPU-free calls run."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    src = tmp_path / "use.cpp"
+    src.write_text('''
+#include "smvs.hpp"
+#include <cstdio>
+int main() {
+  smvs_options o = smvs::DefaultOptions();
+  o.depth_min = 1; o.depth_max = 10; o.window_step = 1;
+  smvs::Check(smvs_options_check(&o));
+  o.window_radius = 6;
+  try { smvs::Check(smvs_options_check(&o)); return 1; } catch (const smvs::Error& e) {
+    std::printf("%d %s\\n", e.status, e.what());
+  }
+  return 0;
+}
+''')
+    lib = N.library_path()
+    exe = tmp_path / "use"
+    res = subprocess.run([gxx, "-std=c++17", f"-I{ROOT / 'include'}", str(src), str(lib), f"-Wl,-rpath,{lib.parent}",
+                          "-o", str(exe)], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
+    run = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert run.returncode == 0 and run.stdout.startswith("1 "), (run.stdout, run.stderr)
