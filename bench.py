@@ -59,6 +59,12 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--mode", default="batched", choices=["batched", "engine"],
+                    help="batched: views resident once, all jobs of a pass in one batch (smvs_pool); "
+                         "engine: one smvs_create/smvs_run per reference view and pass")
+    ap.add_argument("--serving-seconds", type=float, default=12.0,
+                    help="length of the Poisson-arrival serving measurement (0 = skip)")
+    ap.add_argument("--serving-rate", type=float, default=2.0, help="job arrivals per second")
     ap.add_argument("--single", action="store_true",
                     help="profiling mode: run one photometric pass of view 0 per step (for ncu captures)")
     return ap.parse_args()
@@ -233,6 +239,59 @@ class Workload:
         return out, h2d, d2h, launches
 
 
+class PoolWorkload:
+    """The same scene step through the batched pool: every view resident once,
+    11 photometric jobs in one batch, then 11 geometric jobs in one batch."""
+
+    def __init__(self, wl: Workload, block_x: int = 32):
+        self.wl = wl
+        self.block_x = block_x
+
+    def _run(self, pool, images):
+        from sensemap_b200.patch_match import View
+        wl, sc = self.wl, self.wl.scene
+        for i, v in enumerate(sc.views):
+            pool.add_view(i, View(images[i], v.K, v.R, v.T))
+        opt_p = make_options(sc, wl.storage, False)
+        photo = []
+        for r in range(wl.V):
+            opt_p.random_seed = r
+            photo.append(pool.submit(opt_p, r, [i for i in range(wl.V) if i != r]))
+        pool.run_until_done(photo)
+        for j in photo:
+            pool.keep_maps(j)
+            pool.release(j)
+        opt_g = make_options(sc, wl.storage, True)
+        geo = []
+        for r in range(wl.V):
+            opt_g.random_seed = 1000 + r
+            geo.append(pool.submit(opt_g, r, [i for i in range(wl.V) if i != r]))
+        pool.run_until_done(geo)
+        return geo
+
+    def new_pool(self, stream):
+        from sensemap_b200.pool import DepthMapPool
+        return DepthMapPool(memory_budget_bytes=64 << 30, max_active_jobs=self.wl.V, image_storage=self.wl.storage,
+                            sweep_block_x=self.block_x, stream=stream)
+
+    def step_device(self, stream):
+        pool = self.new_pool(stream)
+        geo = self._run(pool, self.wl.dev)
+        return pool, geo
+
+    def step_host(self, stream):
+        """Host images in, geometric depth maps back to host."""
+        import sensemap_b200._native as NN
+        pool = self.new_pool(stream)
+        geo = self._run(pool, self.wl.host)
+        out = [pool.get_map(j, NN.MAP_DEPTH) for j in geo]
+        st = pool.stats()
+        pool.close()
+        h2d = sum(int(t.numel()) * 4 for t in self.wl.host)
+        d2h = sum(o.nbytes for o in out)
+        return out, h2d, d2h, st["launches"]
+
+
 def storage_code(name):
     from sensemap_b200 import STORE_F16, STORE_F32, STORE_U8
     return {"u8": STORE_U8, "f16": STORE_F16, "f32": STORE_F32}[name]
@@ -325,15 +384,24 @@ def main():
         run_single(args, wl, sptr)
         return
 
-    def device_step(keep):
-        return wl.step_device(sptr, keep)
+    pw = PoolWorkload(wl)
+    import sensemap_b200._native as NN
+
+    def device_step():
+        """One step; returns (objects to close, launches, geometric depth getters)."""
+        if args.mode == "engine":
+            keep = []
+            geo = wl.step_device(sptr, keep)
+            return keep, sum(pm.LaunchCount() for pm in keep), [pm.GetDepthMap for pm in geo]
+        pool, geo = pw.step_device(sptr)
+        return [pool], pool.stats()["launches"], [lambda j=j: pool.get_map(j, NN.MAP_DEPTH) for j in geo]
 
     # Warm-up.
     for _ in range(args.warmup):
-        keep = []
-        device_step(keep)
+        objs, _, _ = device_step()
         torch.cuda.synchronize()
-        del keep
+        for o in objs:
+            o.close()
     # Timed region (device-resident inputs).
     clocks = ClockSampler(local)
     barrier(world)
@@ -342,12 +410,11 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     keep, launches = [], 0
     ev0.record(stream)
-    last_geo = None
+    getters = None
     for _ in range(args.steps):
-        step_keep = []
-        last_geo = device_step(step_keep)
-        launches += sum(pm.LaunchCount() for pm in step_keep)
-        keep.append(step_keep)
+        objs, n, getters = device_step()
+        launches += n
+        keep.append(objs)
     ev1.record(stream)
     torch.cuda.synchronize()
     barrier(world)
@@ -356,10 +423,10 @@ def main():
     ms = max_over_ranks(ms, world)
     depth_maps = args.steps * wl.V * world
     value = depth_maps / (ms / 1000.0)
-    acc = [syn.depth_accuracy(pm.GetDepthMap(), scene.views[i].depth_gt) for i, pm in enumerate(last_geo)]
-    for k in keep:
-        for pm in k:
-            pm.close()
+    acc = [syn.depth_accuracy(g(), scene.views[i].depth_gt) for i, g in enumerate(getters)]
+    for objs in keep:
+        for o in objs:
+            o.close()
     del keep
 
     # Per-kernel device time (one profiled photometric + geometric pass of view 0).
@@ -392,17 +459,22 @@ def main():
     e2e = None
     if not args.no_e2e:
         # End to end through host buffers (pinned inputs, host outputs).
-        wl.step_host()
+        host_step = wl.step_host if args.mode == "engine" else (lambda: pw.step_host(sptr))
+        host_step()
         torch.cuda.synchronize()
         barrier(world)
         t = time.perf_counter()
         h2d = d2h = 0
         for _ in range(args.steps):
-            _, h2d, d2h, _ = wl.step_host()
+            _, h2d, d2h, _ = host_step()
         torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t, world)
         e2e = {"value": depth_maps / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h}
+
+    serving = None
+    if args.serving_seconds > 0:
+        serving = run_serving(args, wl, sptr)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -414,16 +486,59 @@ def main():
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": f"heightfield scene, {wl.V} views {args.width}x{args.height}, each view "
                                        f"photometric + geometric PatchMatch (R={RADIUS}, S={STEP}, {ITERS} "
-                                       f"iterations), {args.storage} image storage",
+                                       f"iterations), {args.storage} image storage, {args.mode} form",
                            "global_batch": wl.V * world, "parallelism": f"views sharded, {world} replica(s)",
                            "l2": "inputs larger than L2 (11 x 1600x1200 images + maps per step)"},
-                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "serving": serving,
                 "clocks": clock_info,
                 "accuracy": {"within_1pct_gt_mean": float(np.mean(acc)), "per_view": [round(a, 4) for a in acc]}}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def run_serving(args, wl, sptr):
+    """Poisson arrivals of photometric depth-map jobs (random reference view of
+    the scene, the other views as sources) into a continuous-batching pool with
+    every view resident; p50/p99 completion latency and throughput."""
+    from sensemap_b200 import serving as srv
+    from sensemap_b200.patch_match import View
+    from sensemap_b200.pool import DepthMapPool
+    sc = wl.scene
+    n_jobs = max(4, int(args.serving_rate * args.serving_seconds))
+    arrivals = srv.poisson_arrivals(args.serving_rate, n_jobs, seed=1)
+    rng = np.random.default_rng(2)
+    specs = []
+    for k in range(n_jobs):
+        r = int(rng.integers(0, wl.V))
+        o = make_options(sc, wl.storage, False)
+        o.random_seed = 5000 + k
+        specs.append(srv.JobSpec(o, r, [i for i in range(wl.V) if i != r]))
+    pool = DepthMapPool(memory_budget_bytes=32 << 30, max_active_jobs=8, image_storage=wl.storage, stream=sptr)
+    for i, v in enumerate(sc.views):
+        pool.add_view(i, View(wl.dev[i], v.K, v.R, v.T))
+    acc = []
+
+    def done(k, jid):
+        if len(acc) < 8:
+            acc.append(syn_depth_accuracy(pool.get_map(jid, 0), sc.views[specs[k].ref_view].depth_gt))
+        pool.release(jid)
+
+    res = srv.serve(pool, specs, arrivals, on_done=done)
+    st = pool.stats()
+    pool.close()
+    res.pop("latencies")
+    res.update({"arrival_rate_jobs_s": args.serving_rate, "slots": 8, "job": "photometric pass, 1 ref + 10 src, "
+                f"{wl.scene.views[0].image.shape[1]}x{wl.scene.views[0].image.shape[0]}, {ITERS} iterations",
+                "within_1pct_gt_first_jobs": float(np.mean(acc)) if acc else None,
+                "graphs_built": st["graphs_built"], "pool_steps": st["steps"]})
+    return res
+
+
+def syn_depth_accuracy(depth, gt):
+    from sensemap_b200 import synthetic as syn
+    return syn.depth_accuracy(depth, gt)
 
 
 def run_single(args, wl, sptr):

@@ -225,6 +225,68 @@ int smvs_set_profiling(smvs_engine* eng, int enable);
 int smvs_get_profile(smvs_engine* eng, int kind, int* count, double* total_ms);
 void smvs_destroy(smvs_engine* eng);
 
+/* ---- resident views, batched jobs, continuous admission ------------------ */
+/* No counterpart in the reference (which runs one PatchMatchACMMCuda per host
+ * thread and uploads every image again for every reference view,
+ * patch_match_controller.cc:4330-4807). A pool keeps views resident in HBM
+ * under a byte budget (least recently used views that no job references are
+ * evicted), admits submitted jobs while slots and memory allow, and advances
+ * every active job one PatchMatch iteration per smvs_pool_step with one launch
+ * per checkerboard kernel for the whole batch (captured once in a CUDA graph
+ * while the batch is unchanged). A job's maps do not depend on which other
+ * jobs run with it. Not thread-safe: drive a pool from one thread. */
+typedef struct smvs_pool smvs_pool;
+
+typedef struct smvs_pool_options {
+  size_t memory_budget_bytes; /* views + job state + cached blocks */
+  int max_active_jobs;        /* slots */
+  int image_storage;          /* smvs_image_storage of resident views */
+  int sweep_block_x;          /* launch shape (smvs_tuning) */
+  int use_graphs;             /* capture each batch's iteration in a CUDA graph */
+  int gpu_index;              /* -1 = current device */
+} smvs_pool_options;
+
+typedef struct smvs_pool_stats {
+  int queued, active, done;
+  size_t bytes_used, bytes_budget;
+  int views_resident;
+  int64_t launches, graphs_built, evictions, steps;
+} smvs_pool_stats;
+
+typedef enum smvs_job_state { SMVS_JOB_QUEUED = 0, SMVS_JOB_ACTIVE = 1, SMVS_JOB_DONE = 2, SMVS_JOB_FAILED = 3 } smvs_job_state;
+typedef enum smvs_map_kind {
+  SMVS_MAP_DEPTH = 0, SMVS_MAP_NORMAL = 1, SMVS_MAP_CONF = 2, SMVS_MAP_COST = 3, SMVS_MAP_VIEW_SEL = 4
+} smvs_map_kind;
+
+int smvs_pool_options_default(smvs_pool_options* opt);
+int smvs_pool_create(const smvs_pool_options* opt, void* stream, smvs_pool** out);
+/* Make a view resident (image only; K/R/T as in smvs_view). Re-adding a
+ * resident id only refreshes its LRU position. `memory`: smvs_memory of pixels. */
+int smvs_pool_add_view(smvs_pool* pool, int64_t view_id, const smvs_view* view, int memory);
+int smvs_pool_has_view(smvs_pool* pool, int64_t view_id, int* resident);
+/* Resident depth (W*H) and normal (3*W*H, may be NULL) maps of a view: the
+ * initial maps when it is a reference view with init_depth_random == 0, and
+ * its geometric term when it is a source view of a geom_consistency job. */
+int smvs_pool_set_view_maps(smvs_pool* pool, int64_t view_id, const float* depth, const float* normal, int memory);
+/* Queue a job (photometric or geometric pass of one reference view). The
+ * post-filters (median, confidence, curvature) and the mask are not run by
+ * pool jobs (rejected with SMVS_EINVAL); use smvs_create for those. */
+int smvs_pool_submit(smvs_pool* pool, const smvs_options* opt, int64_t ref_view, const int64_t* src_views,
+                     int num_src, int64_t* job_id);
+/* Admit, advance every active job one iteration, retire finished jobs; waits
+ * for the step's GPU work. */
+int smvs_pool_step(smvs_pool* pool, smvs_pool_stats* stats);
+/* smvs_job_state; latency_s (may be NULL) = completion - submission for done jobs, else -1. */
+int smvs_pool_job_state(smvs_pool* pool, int64_t job_id, int* state, double* latency_s);
+/* Copy a done job's map (smvs_map_kind) to `out` (host or device). */
+int smvs_pool_get_map(smvs_pool* pool, int64_t job_id, int which, void* out);
+/* Store a done job's depth/normal as its reference view's resident maps. */
+int smvs_pool_keep_maps(smvs_pool* pool, int64_t job_id);
+/* Drop a queued or done job and return its memory to the pool's cache. */
+int smvs_pool_release(smvs_pool* pool, int64_t job_id);
+int smvs_pool_stats_get(smvs_pool* pool, smvs_pool_stats* stats);
+void smvs_pool_destroy(smvs_pool* pool);
+
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);
 

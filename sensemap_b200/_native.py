@@ -20,6 +20,8 @@ MEM_HOST, MEM_DEVICE = 0, 1
 (KERNEL_CONVERT, KERNEL_PREP, KERNEL_INIT, KERNEL_INIT_CONF, KERNEL_SWEEP, KERNEL_LOCAL_OPT, KERNEL_MASK,
  KERNEL_FILTER, KERNEL_POST) = range(9)
 KERNEL_NAMES = ["convert", "prep_ref", "init", "init_conf", "sweep", "local_opt", "mask", "filter", "post"]
+JOB_QUEUED, JOB_ACTIVE, JOB_DONE, JOB_FAILED = range(4)
+MAP_DEPTH, MAP_NORMAL, MAP_CONF, MAP_COST, MAP_VIEW_SEL = range(5)
 
 STATUS_NAMES = {0: "SMVS_OK", 1: "SMVS_EINVAL", 2: "SMVS_ENOMEM", 3: "SMVS_ECUDA", 4: "SMVS_ESTATE",
                 5: "SMVS_EIO", 6: "SMVS_ETIMEDOUT", 7: "SMVS_ECANCELED"}
@@ -79,6 +81,17 @@ class smvs_tuning(C.Structure):
     _fields_ = [("sweep_block_x", C.c_int)]
 
 
+class smvs_pool_options(C.Structure):
+    _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_active_jobs", C.c_int), ("image_storage", C.c_int),
+                ("sweep_block_x", C.c_int), ("use_graphs", C.c_int), ("gpu_index", C.c_int)]
+
+
+class smvs_pool_stats(C.Structure):
+    _fields_ = [("queued", C.c_int), ("active", C.c_int), ("done", C.c_int), ("bytes_used", C.c_size_t),
+                ("bytes_budget", C.c_size_t), ("views_resident", C.c_int), ("launches", C.c_int64),
+                ("graphs_built", C.c_int64), ("evictions", C.c_int64), ("steps", C.c_int64)]
+
+
 class smvs_device_maps(C.Structure):
     _fields_ = [
         ("width", C.c_int), ("height", C.c_int), ("num_src", C.c_int),
@@ -117,6 +130,20 @@ _SIGNATURES = {
     "smvs_encode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "smvs_decode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "smvs_write_maps": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    "smvs_pool_options_default": (C.c_int, [C.POINTER(smvs_pool_options)]),
+    "smvs_pool_create": (C.c_int, [C.POINTER(smvs_pool_options), C.c_void_p, C.POINTER(C.c_void_p)]),
+    "smvs_pool_add_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(smvs_view), C.c_int]),
+    "smvs_pool_has_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int)]),
+    "smvs_pool_set_view_maps": (C.c_int, [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_int]),
+    "smvs_pool_submit": (C.c_int, [C.c_void_p, C.POINTER(smvs_options), C.c_int64, C.POINTER(C.c_int64), C.c_int,
+                                   C.POINTER(C.c_int64)]),
+    "smvs_pool_step": (C.c_int, [C.c_void_p, C.POINTER(smvs_pool_stats)]),
+    "smvs_pool_job_state": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "smvs_pool_get_map": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]),
+    "smvs_pool_keep_maps": (C.c_int, [C.c_void_p, C.c_int64]),
+    "smvs_pool_release": (C.c_int, [C.c_void_p, C.c_int64]),
+    "smvs_pool_stats_get": (C.c_int, [C.c_void_p, C.POINTER(smvs_pool_stats)]),
+    "smvs_pool_destroy": (None, [C.c_void_p]),
     # include/smvs_testing.h
     "smvs_test_sample_texture": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                            C.c_void_p]),

@@ -153,6 +153,8 @@ struct smvs_engine {
   float* d_init_normal = nullptr;  // ref.normal as given
   uint8_t* d_mask = nullptr;
   uint16_t* d_curv = nullptr;   // 2*W*H (est_curvature && geom_consistency)
+  // One-job batch for the checkerboard kernels: [JobParams | iters | prefix | conf prefix].
+  void* d_batch = nullptr;
   float* d_ggrad = nullptr;     // W*H (median_filter)
   bool has_init = false;
   bool has_src_depth = false;
@@ -240,6 +242,24 @@ int CheckView(const smvs_view& v, const char* what) {
 
 }  // namespace
 
+// Fill the iteration-dependent and tiling fields of a job's parameters.
+int smvs_internal_prepare_job(smvs::JobParams* p, const smvs_options* o) {
+  p->seed = o->random_seed;
+  p->num_iterations = o->num_iterations;
+  p->local_opt = o->local_optimization && !o->has_prior_depth;
+  for (int it = 0; it < smvs::kMaxIterations; ++it)  // patch_match_cuda.cu:778-779
+    p->th_tab[it] = (float)o->init_ncc_matching_cost * expf(-(float)(it * it) / (float)o->alpha);
+  p->blocks_x = (p->W + 2 * p->block_x - 1) / (2 * p->block_x);
+  p->conf_blocks_x = (p->W + 31) / 32;
+  return SMVS_OK;
+}
+
+// The 43-float pose record of one source view, for the other entry points of
+// this library.
+void smvs_internal_pose_record(const smvs_view* ref, const smvs_view* src, float* out43) {
+  BuildPoseRecord(*ref, *src, out43);
+}
+
 extern "C" {
 
 const char* smvs_last_error(void) { return g_last_error.c_str(); }
@@ -313,6 +333,8 @@ int smvs_options_check(const smvs_options* o) {
   if (o->thk < 1 || o->thk > 4) return Fail(SMVS_EINVAL, "thk must be in 1..4 (mweights, kernel_functions.cu:22)");
   if (o->has_prior_depth || o->propagate_depth)
     return Fail(SMVS_EINVAL, "prior-depth and propagate-depth initialisation are not supported");
+  if (o->num_iterations > smvs::kMaxIterations)
+    return Fail(SMVS_EINVAL, "num_iterations must be <= %d", smvs::kMaxIterations);
   if (o->image_storage < SMVS_STORE_U8 || o->image_storage > SMVS_STORE_F32)
     return Fail(SMVS_EINVAL, "unknown image_storage %d", o->image_storage);
   return SMVS_OK;
@@ -467,6 +489,7 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   }
   if (prob->ref_mask) TRY(StageIn(e, prob->ref_mask, WH, prob->memory, (void**)&e->d_mask));
   if (opt->est_curvature && opt->geom_consistency) TRY(e->Alloc((void**)&e->d_curv, 2 * WH * sizeof(uint16_t)));
+  TRY(e->Alloc(&e->d_batch, sizeof(smvs::JobParams) + 8 * sizeof(int)));
   if (opt->median_filter) TRY(e->Alloc((void**)&e->d_ggrad, WH * sizeof(float)));
   // Source pixels/depths staged from host memory must stay valid until the
   // copies complete; the caller's buffers are only guaranteed during this call.
@@ -495,21 +518,44 @@ int smvs_run(smvs_engine* e) {
     return smvs::LaunchInit(p, o.init_depth_random, (float)o.depth_min, (float)o.depth_max, e->stream);
   });
   if (st) return st;
-  if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(p, e->stream); }))) return st;
+  smvs::Batch b;
+  if ((st = smvs_internal_prepare_job(&p, &o))) return st;
+  {
+    // The checkerboard kernels run as a batch of one job.
+    char host[sizeof(smvs::JobParams) + 8 * sizeof(int)];
+    int* ints = reinterpret_cast<int*>(host + sizeof(smvs::JobParams));
+    memcpy(host, &p, sizeof(p));
+    const int by = 256 / p.block_x;
+    const int nb = p.blocks_x * ((e->H + by - 1) / by);
+    const int ncb = p.conf_blocks_x * ((e->H + 7) / 8);
+    ints[0] = 0;             // iteration counter
+    ints[1] = 0; ints[2] = nb;   // checkerboard prefix
+    ints[3] = 0; ints[4] = ncb;  // InitConf prefix
+    SMVS_CUDA(cudaMemcpyAsync(e->d_batch, host, sizeof(host), cudaMemcpyHostToDevice, e->stream));
+    char* dev = static_cast<char*>(e->d_batch);
+    int* dints = reinterpret_cast<int*>(dev + sizeof(smvs::JobParams));
+    b.jobs = reinterpret_cast<const smvs::JobParams*>(dev);
+    b.iters = dints;
+    b.block_start = dints + 1;
+    b.conf_block_start = dints + 3;
+    b.num_jobs = 1;
+    b.total_blocks = nb;
+    b.total_conf_blocks = ncb;
+    b.block_x = p.block_x;
+    b.R = p.R; b.S = p.S; b.NB = smvs::ViewBucket(p.N);
+  }
+  if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(b, e->stream); }))) return st;
+  int* iters = const_cast<int*>(b.iters);
   for (int iter = 0; iter < o.num_iterations; ++iter) {
-    p.th_mc = (float)o.init_ncc_matching_cost * expf(-(float)(iter * iter) / (float)o.alpha);  // :778-779
-    for (int colour = 0; colour < 2; ++colour) {
-      p.stage_key = smvs::StageKey(o.random_seed, smvs::StageSweep(iter, colour));
-      if ((st = Launch(e, SMVS_KERNEL_SWEEP, "sweep", [&] { return smvs::LaunchSweep(p, colour, e->stream); }))) return st;
-    }
-    if (o.local_optimization && iter > 2 && !o.has_prior_depth) {  // :861-880
-      for (int colour = 0; colour < 2; ++colour) {
-        p.stage_key = smvs::StageKey(o.random_seed, smvs::StageLocal(iter, colour));
+    for (int colour = 0; colour < 2; ++colour)
+      if ((st = Launch(e, SMVS_KERNEL_SWEEP, "sweep", [&] { return smvs::LaunchSweep(b, colour, e->stream); }))) return st;
+    if (p.local_opt && iter > 2) {  // :861-880
+      for (int colour = 0; colour < 2; ++colour)
         if ((st = Launch(e, SMVS_KERNEL_LOCAL_OPT, "local optimisation",
-                         [&] { return smvs::LaunchLocalOpt(p, colour, e->stream); })))
+                         [&] { return smvs::LaunchLocalOpt(b, colour, e->stream); })))
           return st;
-      }
     }
+    if ((st = Launch(e, SMVS_KERNEL_INIT, "advance", [&] { return smvs::LaunchAdvance(iters, 1, e->stream); }))) return st;
   }
   // Post-processing in the reference's order (patch_match_cuda.cu:985-1052).
   if (e->d_curv && (st = Launch(e, SMVS_KERNEL_POST, "curvature",

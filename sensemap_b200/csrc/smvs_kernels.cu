@@ -10,7 +10,7 @@ namespace smvs {
 
 namespace detail {
 template <int R, int S>
-cudaError_t LaunchWindow(const JobParams& p, int op, int colour, cudaStream_t stream);
+cudaError_t LaunchWindow(const Batch& b, int op, int colour, cudaStream_t stream);
 }
 
 namespace {
@@ -306,16 +306,21 @@ __global__ void FilterDepthMapsKernel(JobParams p, const float* __restrict__ in_
 
 // Dispatch over the window sizes the reference supports
 // (kernel_functions.cu:1343-1400).
-cudaError_t LaunchWindowOp(const JobParams& p, int op, int colour, cudaStream_t stream) {
-  const int R = p.R, S = p.S;
-  if (R == 5 && S == 1) return detail::LaunchWindow<5, 1>(p, op, colour, stream);
-  if (R == 3 && S == 1) return detail::LaunchWindow<3, 1>(p, op, colour, stream);
-  if (R == 7 && S == 1) return detail::LaunchWindow<7, 1>(p, op, colour, stream);
-  if (R == 3 && S == 2) return detail::LaunchWindow<3, 2>(p, op, colour, stream);
-  if (R == 4 && S == 2) return detail::LaunchWindow<4, 2>(p, op, colour, stream);
-  if (R == 5 && S == 2) return detail::LaunchWindow<5, 2>(p, op, colour, stream);
-  if (R == 7 && S == 2) return detail::LaunchWindow<7, 2>(p, op, colour, stream);
+cudaError_t LaunchWindowOp(const Batch& b, int op, int colour, cudaStream_t stream) {
+  const int R = b.R, S = b.S;
+  if (R == 5 && S == 1) return detail::LaunchWindow<5, 1>(b, op, colour, stream);
+  if (R == 3 && S == 1) return detail::LaunchWindow<3, 1>(b, op, colour, stream);
+  if (R == 7 && S == 1) return detail::LaunchWindow<7, 1>(b, op, colour, stream);
+  if (R == 3 && S == 2) return detail::LaunchWindow<3, 2>(b, op, colour, stream);
+  if (R == 4 && S == 2) return detail::LaunchWindow<4, 2>(b, op, colour, stream);
+  if (R == 5 && S == 2) return detail::LaunchWindow<5, 2>(b, op, colour, stream);
+  if (R == 7 && S == 2) return detail::LaunchWindow<7, 2>(b, op, colour, stream);
   return cudaErrorInvalidValue;
+}
+
+__global__ void AdvanceKernel(int* __restrict__ iters, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) iters[i] += 1;
 }
 
 }  // namespace
@@ -343,15 +348,23 @@ cudaError_t LaunchInit(const JobParams& p, int random_init, float opt_dmin, floa
   return cudaGetLastError();
 }
 
-cudaError_t LaunchInitConf(const JobParams& p, cudaStream_t stream) { return LaunchWindowOp(p, 0, 0, stream); }
+cudaError_t LaunchInitConf(const Batch& b, cudaStream_t stream) { return LaunchWindowOp(b, 0, 0, stream); }
 
-cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream) {
-  return LaunchWindowOp(p, 1, colour, stream);
+cudaError_t LaunchSweep(const Batch& b, int colour, cudaStream_t stream) {
+  return LaunchWindowOp(b, 1, colour, stream);
 }
 
-cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream) {
-  return LaunchWindowOp(p, 2, colour, stream);
+cudaError_t LaunchLocalOpt(const Batch& b, int colour, cudaStream_t stream) {
+  return LaunchWindowOp(b, 2, colour, stream);
 }
+
+cudaError_t LaunchAdvance(int* iters, int num_jobs, cudaStream_t stream) {
+  if (num_jobs <= 0) return cudaSuccess;
+  AdvanceKernel<<<(num_jobs + 127) / 128, 128, 0, stream>>>(iters, num_jobs);
+  return cudaGetLastError();
+}
+
+int ViewBucket(int N) { return N <= 8 ? 8 : (N <= 16 ? 16 : SMVS_MAX_SRC); }
 
 cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream) {
   dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);

@@ -8,20 +8,30 @@
 
 namespace smvs {
 
-// Per-job parameter block passed by value to every kernel. It replaces the
-// reference's __constant__ ref_K/ref_inv_K slots (kernel_functions.cu:18-20)
-// and its SweepOptions struct (kernel_functions.h:67-111).
-struct JobParams {
+constexpr int kMaxIterations = 32;  // th_mc table size (num_iterations limit)
+
+// Per-job parameter block. It replaces the reference's __constant__
+// ref_K/ref_inv_K slots (kernel_functions.cu:18-20) and its SweepOptions
+// struct (kernel_functions.h:67-111). Per-pixel kernels take it by value; the
+// batched checkerboard kernels read an array of them from device memory (one
+// entry per job of a batch) and stage their job's entry in shared memory.
+struct alignas(16) JobParams {
   int W, H, N, R, S;
   float sn, cn;                     // BilateralWeightComputer normalisations (utils.h:72-92)
   float depth_min, depth_max;       // options' depth range (float)
   float rand_depth_ratio, rand_a1, rand_a2;
-  float th_mc, max_mc, inv_beta2;
+  float th_mc, max_mc, inv_beta2;   // th_mc: per-launch value of the per-pixel kernels
   int num_samples, num_good, num_bad, random_opt, geom, thk;
   float geom_reg, geom_max;
   float refK[4], refiK[4];
-  uint64_t stage_key;
-  int block_x;             // checkerboard kernels: threads per block in x (256 / block_x in y)
+  uint64_t stage_key;               // per-launch RNG stage key of the per-pixel kernels
+  uint64_t seed;                    // job seed (batched kernels derive stage keys from it)
+  int block_x;                      // checkerboard kernels: threads per block in x (256 / block_x in y)
+  int num_iterations;
+  int local_opt;
+  int blocks_x;                     // batched launches: this job's checkerboard blocks per row
+  int conf_blocks_x;                // batched InitConf launches: blocks per row
+  float th_tab[kMaxIterations];     // th_mc of each iteration (patch_match_cuda.cu:778-779)
   // State maps (dense row-major; normal and cost planar).
   float* depth;
   float* normal;
@@ -38,14 +48,34 @@ struct JobParams {
   cudaTextureObject_t dep_tex[SMVS_MAX_SRC];
 };
 
+// A batch of jobs for the checkerboard kernels: device arrays of job params,
+// per-job iteration counters and block prefix sums (block_start[j] = first
+// block of job j; block_start[num_jobs] = total blocks).
+struct Batch {
+  const JobParams* jobs;
+  const int* iters;
+  const int* block_start;       // checkerboard tiling (Sweep / LocalOpt)
+  const int* conf_block_start;  // full tiling (InitConf)
+  int num_jobs;
+  int total_blocks;             // checkerboard tiling
+  int total_conf_blocks;        // full tiling
+  int block_x;                  // shared launch shape of the batch
+  int R, S, NB;                 // shared window and view bucket of the batch
+};
+
 // All launchers enqueue on `stream` and return the launch status.
 cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, int w, int h, void* out,
                                int out_storage, size_t out_pitch, int normalise, cudaStream_t stream);
 cudaError_t LaunchPrepRef(const JobParams& p, float* ref_sum, float* ref_sqsum, float* grad, cudaStream_t stream);
 cudaError_t LaunchInit(const JobParams& p, int random_init, float opt_dmin, float opt_dmax, cudaStream_t stream);
-cudaError_t LaunchInitConf(const JobParams& p, cudaStream_t stream);
-cudaError_t LaunchSweep(const JobParams& p, int colour, cudaStream_t stream);
-cudaError_t LaunchLocalOpt(const JobParams& p, int colour, cudaStream_t stream);
+// Batched checkerboard kernels: every job of `b` in one launch.
+cudaError_t LaunchInitConf(const Batch& b, cudaStream_t stream);
+cudaError_t LaunchSweep(const Batch& b, int colour, cudaStream_t stream);
+cudaError_t LaunchLocalOpt(const Batch& b, int colour, cudaStream_t stream);
+// iters[j] += 1 for every job of the batch (after both colours of an iteration).
+cudaError_t LaunchAdvance(int* iters, int num_jobs, cudaStream_t stream);
+// View bucket (max views of the M matrix) for N source views.
+int ViewBucket(int N);
 cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream);
 cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream);
 cudaError_t LaunchGeomGradient(const JobParams& p, float* ggrad, cudaStream_t stream);

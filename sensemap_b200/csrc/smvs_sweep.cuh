@@ -47,6 +47,35 @@ __device__ __forceinline__ void StageShared(const JobParams& p, float* tile, int
   for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += nthr) poses[i] = __ldg(p.poses + i);
 }
 
+// Batched launches: find this block's job (binary search over the block
+// prefix sums), read its iteration counter and stage its parameters in
+// shared memory. Every thread of the block returns the same values.
+__device__ __forceinline__ void DecodeBlock(const Batch& b, const int* prefix, JobParams& sp, int& job, int& blk,
+                                            int& iter) {
+  __shared__ int s_job, s_blk, s_iter;
+  if (threadIdx.x == 0 && threadIdx.y == 0) {
+    const int bid = blockIdx.x;
+    int lo = 0, hi = b.num_jobs - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (__ldg(prefix + mid) <= bid) lo = mid; else hi = mid - 1;
+    }
+    s_job = lo;
+    s_blk = bid - __ldg(prefix + lo);
+    s_iter = b.iters ? b.iters[lo] : 0;
+  }
+  __syncthreads();
+  job = s_job;
+  blk = s_blk;
+  iter = s_iter;
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  const int nthr = blockDim.x * blockDim.y;
+  const int4* src = reinterpret_cast<const int4*>(b.jobs + job);
+  int4* dst = reinterpret_cast<int4*>(&sp);
+  for (int i = tid; i < (int)(sizeof(JobParams) / sizeof(int4)); i += nthr) dst[i] = src[i];
+  __syncthreads();
+}
+
 // ComputeNCCCost<R,S>, kernel_functions.cu:1245-1340. `win` points at the
 // window's top-left in the shared tile (row stride ws).
 template <int R, int S>
@@ -124,13 +153,17 @@ __device__ __forceinline__ float ViewCost(const JobParams& p, const float* poses
 
 // InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior).
 template <int R, int S>
-__global__ void __launch_bounds__(kThreads) InitConfKernel(JobParams p) {
+__global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  int job, blk, iter;
+  DecodeBlock(b, b.conf_block_start, sp, job, blk, iter);
+  const JobParams& p = sp;
   const int kBX = blockDim.x, kBY = blockDim.y;
   const int tw = kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
-  const int col0 = blockIdx.x * kBX, row0 = blockIdx.y * kBY;
+  const int col0 = (blk % p.conf_blocks_x) * kBX, row0 = (blk / p.conf_blocks_x) * kBY;
   StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
   __syncthreads();
   const int col = col0 + threadIdx.x, row = row0 + threadIdx.y;
@@ -173,13 +206,20 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(JobParams p) {
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
 // propagate_depth): one checkerboard colour, one thread per pixel.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) SweepKernel(JobParams p, int colour) {
+__global__ void __launch_bounds__(kThreads) SweepKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  int job, blk, iter;
+  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  const JobParams& p = sp;
+  if (iter >= p.num_iterations) return;  // finished job of the batch (block-uniform)
+  const float th_mc = p.th_tab[iter];
+  const uint64_t skey = StageKey(p.seed, StageSweep(iter, colour));
   const int kBX = blockDim.x, kBY = blockDim.y;
   const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
-  const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
+  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
   StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
   __syncthreads();
   const int row = row0 + threadIdx.y;
@@ -188,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) SweepKernel(JobParams p, int colour)
   const int W = p.W, H = p.H, N = p.N;
   const size_t WH = (size_t)W * H;
   const size_t pix = (size_t)row * W + col;
-  Rng r(p.stage_key, (uint32_t)pix);
+  Rng r(skey, (uint32_t)pix);
   float depth = p.depth[pix];
   float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
   const float grad = p.grad[pix];
@@ -282,7 +322,7 @@ __global__ void __launch_bounds__(kThreads) SweepKernel(JobParams p, int colour)
       for (int h = 0; h < ns; ++h) {
         const float cst = M[h][v];
         pv += __expf(-cst * cst * p.inv_beta2);
-        n1 += (cst < p.th_mc);
+        n1 += (cst < th_mc);
         n2 += (cst > p.max_mc);
       }
       probs[v] = pv;
@@ -370,13 +410,20 @@ __global__ void __launch_bounds__(kThreads) SweepKernel(JobParams p, int colour)
 
 // LocalOptimization, kernel_functions.cu:2736-2931.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) LocalOptKernel(JobParams p, int colour) {
+__global__ void __launch_bounds__(kThreads) LocalOptKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  int job, blk, iter;
+  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  const JobParams& p = sp;
+  // Iterations > 2 only (patch_match_cuda.cu:861-880); block-uniform.
+  if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
+  const uint64_t skey = StageKey(p.seed, StageLocal(iter, colour));
   const int kBX = blockDim.x, kBY = blockDim.y;
   const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
   float* tile = smem;
   float* poses = smem + tw * th;
-  const int col0 = blockIdx.x * 2 * kBX, row0 = blockIdx.y * kBY;
+  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
   StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
   __syncthreads();
   const int row = row0 + threadIdx.y;
@@ -385,7 +432,7 @@ __global__ void __launch_bounds__(kThreads) LocalOptKernel(JobParams p, int colo
   const int W = p.W, H = p.H, N = p.N;
   const size_t WH = (size_t)W * H;
   const size_t pix = (size_t)row * W + col;
-  Rng r(p.stage_key, (uint32_t)pix);
+  Rng r(skey, (uint32_t)pix);
   float conf = p.conf[pix];
   float depth = p.depth[pix];
   float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
@@ -464,49 +511,46 @@ __global__ void __launch_bounds__(kThreads) LocalOptKernel(JobParams p, int colo
 }
 
 template <int R, int S>
-size_t SweepSmem(int N, int bx, int by) {
-  return sizeof(float) * ((2 * bx + 2 * R) * (by + 2 * R) + N * SMVS_POSE_FLOATS);
-}
-
-dim3 SweepGrid(const JobParams& p, int bx, int by) {
-  return dim3((unsigned)((p.W + 2 * bx - 1) / (2 * bx)), (unsigned)((p.H + by - 1) / by));
+size_t SweepSmem(int NB, int bx, int by) {
+  return sizeof(float) * ((2 * bx + 2 * R) * (by + 2 * R) + NB * SMVS_POSE_FLOATS);
 }
 
 template <int R, int S, int NB>
-cudaError_t LaunchSweepT(const JobParams& p, int colour, bool local, cudaStream_t stream) {
-  const int bx = p.block_x, by = kThreads / p.block_x;
-  const size_t smem = SweepSmem<R, S>(p.N, bx, by);
+cudaError_t LaunchSweepT(const Batch& b, int colour, bool local, cudaStream_t stream) {
+  const int bx = b.block_x, by = kThreads / b.block_x;
+  const size_t smem = SweepSmem<R, S>(NB, bx, by);
+  if (b.total_blocks <= 0) return cudaSuccess;
   if (local)
-    LocalOptKernel<R, S, NB><<<SweepGrid(p, bx, by), dim3(bx, by), smem, stream>>>(p, colour);
+    LocalOptKernel<R, S, NB><<<b.total_blocks, dim3(bx, by), smem, stream>>>(b, colour);
   else
-    SweepKernel<R, S, NB><<<SweepGrid(p, bx, by), dim3(bx, by), smem, stream>>>(p, colour);
+    SweepKernel<R, S, NB><<<b.total_blocks, dim3(bx, by), smem, stream>>>(b, colour);
   return cudaGetLastError();
 }
 
 template <int R, int S>
-cudaError_t LaunchSweepNB(const JobParams& p, int colour, bool local, cudaStream_t stream) {
-  if (p.N <= 8) return LaunchSweepT<R, S, 8>(p, colour, local, stream);
-  if (p.N <= 16) return LaunchSweepT<R, S, 16>(p, colour, local, stream);
-  return LaunchSweepT<R, S, SMVS_MAX_SRC>(p, colour, local, stream);
+cudaError_t LaunchSweepNB(const Batch& b, int colour, bool local, cudaStream_t stream) {
+  if (b.NB == 8) return LaunchSweepT<R, S, 8>(b, colour, local, stream);
+  if (b.NB == 16) return LaunchSweepT<R, S, 16>(b, colour, local, stream);
+  if (b.NB == SMVS_MAX_SRC) return LaunchSweepT<R, S, SMVS_MAX_SRC>(b, colour, local, stream);
+  return cudaErrorInvalidValue;
 }
 
 template <int R, int S>
-cudaError_t LaunchInitConfT(const JobParams& p, cudaStream_t stream) {
+cudaError_t LaunchInitConfT(const Batch& b, cudaStream_t stream) {
   const int bx = 32, by = kThreads / 32;
-  const size_t smem = sizeof(float) * ((bx + 2 * R) * (by + 2 * R) + p.N * SMVS_POSE_FLOATS);
-  dim3 grid((p.W + bx - 1) / bx, (p.H + by - 1) / by);
-  InitConfKernel<R, S><<<grid, dim3(bx, by), smem, stream>>>(p);
+  const size_t smem = sizeof(float) * ((bx + 2 * R) * (by + 2 * R) + b.NB * SMVS_POSE_FLOATS);
+  if (b.total_conf_blocks <= 0) return cudaSuccess;
+  InitConfKernel<R, S><<<b.total_conf_blocks, dim3(bx, by), smem, stream>>>(b);
   return cudaGetLastError();
 }
-
 
 }  // namespace
 
 // One entry point per window: op 0 = InitConf, 1 = sweep, 2 = local optimisation.
 template <int R, int S>
-cudaError_t LaunchWindow(const JobParams& p, int op, int colour, cudaStream_t stream) {
-  if (op == 0) return LaunchInitConfT<R, S>(p, stream);
-  return LaunchSweepNB<R, S>(p, colour, op == 2, stream);
+cudaError_t LaunchWindow(const Batch& b, int op, int colour, cudaStream_t stream) {
+  if (op == 0) return LaunchInitConfT<R, S>(b, stream);
+  return LaunchSweepNB<R, S>(b, colour, op == 2, stream);
 }
 
 }  // namespace detail

@@ -3,6 +3,6 @@
 
 namespace smvs {
 namespace detail {
-template cudaError_t LaunchWindow<5, 1>(const JobParams& p, int op, int colour, cudaStream_t stream);
+template cudaError_t LaunchWindow<5, 1>(const Batch& b, int op, int colour, cudaStream_t stream);
 }  // namespace detail
 }  // namespace smvs
