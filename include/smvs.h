@@ -287,6 +287,29 @@ int smvs_pool_release(smvs_pool* pool, int64_t job_id);
 int smvs_pool_stats_get(smvs_pool* pool, smvs_pool_stats* stats);
 void smvs_pool_destroy(smvs_pool* pool);
 
+/* ---- no-allocation variant ----------------------------------------------- */
+/* Largest number of source views smvs_filter_depth_map_noalloc accepts. */
+#define SMVS_NOALLOC_MAX_SRC 32
+/* The geometric-consistency filter of smvs_run_filter, for callers that cannot
+ * allocate device memory: processes with a fixed device-memory budget reserved
+ * at start-up, code issuing work on a stream that is being captured into a
+ * CUDA graph, or hosts whose framework owns every allocation. No counterpart
+ * in the reference. It calls no cudaMalloc, cudaFree or other allocating
+ * routine: every input and output is a caller-owned device buffer
+ * (prob->memory must be SMVS_MEM_DEVICE; prob->ref.depth is the map to filter,
+ * each prob->src[i].depth a source view's map, pixels are not read), and the
+ * kernel's scratch — the pose records of at most SMVS_NOALLOC_MAX_SRC source
+ * views, 5,504 bytes — lives in a fixed device array that every GPU loading
+ * this library holds until the process exits. More source views are rejected
+ * with SMVS_EINVAL. The first call on a device looks up that array's address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.
+ * All calls share the one array and each call overwrites it before its kernel
+ * runs, so calls whose work overlaps on the GPU (different streams, or other
+ * threads) race; serialise them. Work is enqueued on `stream` (NULL = the
+ * default stream); `out_depth` is W*H floats. */
+int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs_problem* prob, float* out_depth,
+                                  int deduplication, void* stream);
+
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);
 

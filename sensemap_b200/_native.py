@@ -144,6 +144,8 @@ _SIGNATURES = {
     "smvs_pool_release": (C.c_int, [C.c_void_p, C.c_int64]),
     "smvs_pool_stats_get": (C.c_int, [C.c_void_p, C.POINTER(smvs_pool_stats)]),
     "smvs_pool_destroy": (None, [C.c_void_p]),
+    "smvs_filter_depth_map_noalloc": (C.c_int, [C.POINTER(smvs_options), C.POINTER(smvs_problem), C.c_void_p,
+                                                C.c_int, C.c_void_p]),
     # include/smvs_testing.h
     "smvs_test_sample_texture": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                            C.c_void_p]),
