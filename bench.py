@@ -40,6 +40,7 @@ W, H, NSRC, ITERS, RADIUS, STEP = 1600, 1200, 10, 6, 5, 1
 HYP_PER_PIXEL = 14          # 10 propagated + 4 refinement hypotheses per pixel per iteration
 FLOP_PER_TAP = 25           # incremental warp, 1/z, bilinear, 4 moment updates
 METRIC = "depth maps/s (1.6MP,10 src)"
+SWEEP_LAUNCH_DRAM_BYTES = 0.5595e9 + 0.5900e9  # ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch
 
 
 def log(*a):
@@ -52,7 +53,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--storage", default="f32", choices=["u8", "f16", "f32"])
+    ap.add_argument("--storage", default="f16", choices=["u8", "f16", "f32"],
+                    help="source image storage: f16 = precision form (FP16 storage, FP32 accumulation), "
+                         "f32 = plain FP32 path, u8 = the reference's 8-bit texture format")
     ap.add_argument("--views", type=int, default=NSRC + 1, help="views per scene (each is a reference once)")
     ap.add_argument("--width", type=int, default=W)
     ap.add_argument("--height", type=int, default=H)
@@ -307,7 +310,10 @@ def cpu_baseline(scene, storage, seconds_target: float) -> dict:
     V = len(scene.views)
     views = [View(v.image, v.K, v.R, v.T) for v in scene.views]
     prob = Problem(0, list(range(1, V)), views)
-    opt = make_options(scene, storage, False)
+    # The reference samples 8-bit textures (patch_match_cuda.cu:229-278): the CPU
+    # transcription runs with that storage whatever the GPU form uses.
+    from sensemap_b200 import STORE_U8
+    opt = make_options(scene, STORE_U8, False)
     Hh = scene.views[0].image.shape[0]
     r0 = Hh // 2
     t = time.perf_counter()
@@ -320,7 +326,8 @@ def cpu_baseline(scene, storage, seconds_target: float) -> dict:
     per_pass = dt * Hh / rows
     value = 1.0 / (2.0 * per_pass)
     return {"value": value, "unit": "depth maps/s", "cores": orc.num_threads(), "kind": "port",
-            "sample": (f"oracle photometric pass (6 iterations, N={V - 1}) over rows {r0}..{r0 + rows} of a "
+            "sample": (f"oracle (OpenMP transcription of the reference kernel logic, 8-bit sources) photometric "
+                       f"pass (6 iterations, N={V - 1}) over rows {r0}..{r0 + rows} of a "
                        f"{scene.views[0].image.shape[1]}x{Hh} view in {dt:.1f} s; scaled by {Hh}/{rows} rows and x2 "
                        f"for the geometric pass (extrapolated)")}
 
@@ -446,8 +453,11 @@ def main():
     fp32 = ctypes_rate(N, 0)
     tex = ctypes_rate(N, 1)
     peak_taps = min(fp32 / FLOP_PER_TAP, tex)
-    roof = {"bound": "fp32-pipe/texture", "achieved": achieved_tflops, "peak": peak_taps * FLOP_PER_TAP / 1e12,
-            "unit": "TFLOP/s", "frac": (taps_per_launch / sweep_avg_s) / peak_taps, "traffic": None,
+    roof = {"bound": "texture-sampling", "achieved": achieved_tflops, "peak": peak_taps * FLOP_PER_TAP / 1e12,
+            "unit": "TFLOP/s", "frac": (taps_per_launch / sweep_avg_s) / peak_taps,
+            # DRAM bytes (read + write) of one launch of this kernel on this workload
+            # (f16 storage), measured with ncu on B200.
+            "traffic": SWEEP_LAUNCH_DRAM_BYTES if (args.width, args.height, args.views) == (W, H, NSRC + 1) else None,
             "kernel": "SweepKernel<5,1,16>", "taps_per_launch": taps_per_launch, "flop_per_tap": FLOP_PER_TAP,
             "avg_launch_ms": sweep_avg_s * 1000.0,
             "peak_source": (f"measured in this process: FP32 FMA {fp32 / 1e12:.1f} TFLOP/s, bilinear texture "

@@ -62,16 +62,23 @@ static inline int f2i_rz(float x) { /* cvt.rzi.s32.f32: saturating, NaN -> 0 */
 static inline float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
 
 /* Round a float to the nearest FP16 value (round-to-nearest-even), for the
- * precision form's FP16 image storage. Inputs are in [0, 1]. */
+ * precision form's FP16 storage. Inputs are in [0, 1] (no overflow). */
 static float round_to_half(float f) {
-  if (f == 0.0f || f != f) return f;
-  int e;
-  float m = frexpf(fabsf(f), &e); /* f = m * 2^e, m in [0.5,1) */
-  int ulp_exp = e - 11;            /* 11 significant bits */
-  if (e - 1 < -14) ulp_exp = -24;  /* subnormal half */
-  float q = ldexpf(nearbyintf(ldexpf(fabsf(f), -ulp_exp)), ulp_exp);
-  (void)m;
-  return f < 0 ? -q : q;
+  union { float f; uint32_t u; } v = {f};
+  const uint32_t sign = v.u & 0x80000000u;
+  uint32_t a = v.u & 0x7fffffffu;
+  const int exp = (int)(a >> 23) - 127;
+  if (a == 0 || exp >= 16) return f;
+  if (exp < -14) {  /* subnormal half: quantum 2^-24 */
+    const float q = nearbyintf(fabsf(f) * 16777216.0f) / 16777216.0f;
+    return sign ? -q : q;
+  }
+  /* keep 10 mantissa bits, round to nearest even */
+  const uint32_t lsb = (a >> 13) & 1u;
+  a += 0x0fffu + lsb;
+  a &= ~0x1fffu;
+  v.u = sign | a;
+  return v.f;
 }
 
 /* CUDA texture linear filtering, unnormalised coordinates, border address mode

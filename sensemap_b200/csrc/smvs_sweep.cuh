@@ -17,6 +17,9 @@ namespace detail {
 namespace {  // internal linkage: every window translation unit gets its own copy
 
 constexpr int kThreads = 256;  // threads per block; the block's x/y split is a tuning knob (JobParams)
+#ifndef SMVS_SWEEP_MIN_BLOCKS
+#define SMVS_SWEEP_MIN_BLOCKS 1  // resident blocks per SM the register allocation must allow
+#endif
 
 __constant__ float kMWeights[5] = {0.f, 1.f, 2.01f, 3.03f, 4.06f};  // kernel_functions.cu:22
 __constant__ int kNeighborOffs[4][2] = {{0, -1}, {-1, 0}, {0, 1}, {1, 0}};  // :23-25 (first four)
@@ -206,7 +209,7 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
 // propagate_depth): one checkerboard colour, one thread per pixel.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) SweepKernel(const Batch b, int colour) {
+__global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) SweepKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   int job, blk, iter;
@@ -410,7 +413,7 @@ __global__ void __launch_bounds__(kThreads) SweepKernel(const Batch b, int colou
 
 // LocalOptimization, kernel_functions.cu:2736-2931.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) LocalOptKernel(const Batch b, int colour) {
+__global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) LocalOptKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   int job, blk, iter;
