@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=2.0, help="job arrivals per second")
     ap.add_argument("--single", action="store_true",
                     help="profiling mode: run one photometric pass of view 0 per step (for ncu captures)")
+    ap.add_argument("--workload", default="patchmatch", choices=["patchmatch", "cross-filter"],
+                    help="patchmatch: the depth-map stage (default); cross-filter: CrossFilterCuda::Run + "
+                         "DedupRun over the views' depth/normal maps")
     return ap.parse_args()
 
 
@@ -366,6 +369,12 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 def main():
     args = parse()
+    if args.workload == "cross-filter":
+        if args.impl == "reference":
+            run_cross_filter_reference(args)
+        else:
+            run_cross_filter(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return
@@ -563,6 +572,195 @@ def run_single(args, wl, sptr):
             pm.Synchronize()
     torch.cuda.synchronize()
     log("single-pass profiling run done")
+
+
+# ---------------------------------------------------------------------------
+# Cross-view filter workload
+# ---------------------------------------------------------------------------
+CF_METRIC = "cross-filtered depth maps/s (1.6MP,10 src)"
+
+
+def cross_filter_set(args, rank, device):
+    """The bench scene's views with noisy ground-truth depth/normal maps (what
+    the PatchMatch passes hand over) and one problem per view against the
+    other views."""
+    from sensemap_b200 import synthetic as syn
+    scene = syn.heightfield_scene(seed=rank, width=args.width, height=args.height, num_src=args.views - 1,
+                                  device=device)
+    maps = syn.noisy_maps(scene, seed=100 + rank)
+    problems = [(r, [s for s in range(len(scene.views)) if s != r]) for r in range(len(scene.views))]
+    return scene, maps, problems
+
+
+def cross_filter_bytes(shapes, problems, per_ref, per_src):
+    """Algorithmic bytes of one launch: every problem reads its reference maps
+    and writes its output once (per_ref B/px) and reads each source's maps once
+    (per_src B/px)."""
+    total = 0
+    for r, srcs in problems:
+        total += per_ref * shapes[r][0] * shapes[r][1]
+        total += sum(per_src * shapes[q][0] * shapes[q][1] for q in srcs)
+    return total
+
+
+def cpu_cross_filter(scene, maps, problems, steps=1) -> dict:
+    """The oracle (OpenMP restatement of CrossFilterKernel/DeduplicFilterKernel)
+    over the whole set: Run + DedupRun, filtered depth maps/s."""
+    import oracle.oracle as orc
+    from sensemap_b200.patch_match import PatchMatchOptions
+    views = [orc.FilterView(v.K, v.R, v.T, d, n, ref_flag=True) for v, (d, n) in zip(scene.views, maps)]
+    opt = PatchMatchOptions()
+    t = time.perf_counter()
+    for _ in range(steps):
+        refined = orc.cross_filter_run(opt, views, problems)
+        orc.cross_filter_dedup(opt, views, problems, refined)
+    dt = (time.perf_counter() - t) / steps
+    return {"value": len(problems) / dt, "unit": "depth maps/s", "cores": orc.num_threads(), "kind": "port",
+            "sample": f"oracle Run + DedupRun over the whole {len(views)}-view set, {steps} pass(es), {dt:.2f} s each"}
+
+
+def run_cross_filter_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import torch
+    from oracle import build as oracle_build
+    oracle_build.build()
+    scene, maps, problems = cross_filter_set(args, 0, "cuda" if torch.cuda.is_available() else "cpu")
+    samples, cb = [], None
+    for i in range(args.warmup + args.steps):
+        cb = cpu_cross_filter(scene, maps, problems)
+        if i >= args.warmup:
+            samples.append(cb["value"])
+    value = statistics.median(samples)
+    line = {"metric": CF_METRIC, "value": value, "unit": "depth maps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * len(problems) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"cross filter + dedup, {args.views} views {args.width}x{args.height}, each view "
+                                   f"against the other {args.views - 1}", "global_batch": len(problems),
+                       "parallelism": "cpu-openmp"},
+            "cpu_baseline": {**cb, "value": value},
+            "e2e": {"value": value, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_cross_filter(args):
+    import torch
+    world, rank, local = dist_setup()
+    from sensemap_b200 import build as engine_build
+    from sensemap_b200.cross_filter import CrossFilterCuda
+    from sensemap_b200.patch_match import PatchMatchOptions, Problem, View
+    engine_build.build()
+    scene, maps, problems = cross_filter_set(args, rank, "cuda")
+    V = len(scene.views)
+    shapes = [d.shape for d, _ in maps]
+    dev = [(torch.from_numpy(d).cuda(), torch.from_numpy(n).cuda()) for d, n in maps]
+    host = [(torch.from_numpy(d).pin_memory(), torch.from_numpy(n).pin_memory()) for d, n in maps]
+
+    def api_args(pairs):
+        ims = [View(None, v.K, v.R, v.T, depth=d, normal=n) for v, (d, n) in zip(scene.views, pairs)]
+        probs = [Problem(r, [], ims, src_image_extend_idxs=s) for r, s in problems]
+        return probs, list(range(V)), [True] * V
+
+    opt = PatchMatchOptions()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+    dev_args, host_args = api_args(dev), api_args(host)
+
+    def step(args_, fetch, profile=False):
+        cf = CrossFilterCuda(opt, *args_, stream=sptr)
+        if profile:
+            cf.SetProfiling(True)
+        cf.Run()
+        out = [cf.GetRefineDepthMap(r) for r, _ in problems] if fetch else None
+        cf.DedupRun()
+        if fetch:
+            out += [cf.GetDeduplicDepthMap(k) for k in range(V)]
+        return cf, out
+
+    for _ in range(args.warmup):
+        cf, _ = step(dev_args, False)
+        cf.close()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        cf, _ = step(dev_args, False)
+        launches += cf.LaunchCount()
+        cf.close()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    value = args.steps * V * world / (ms / 1000.0)
+
+    # Kernel times (CUDA events on the filter's stream) for the roofline.
+    cf, _ = step(dev_args, False, profile=True)
+    prof = cf.Profile()
+    refined = {r: cf.GetRefineDepthMap(r) for r, _ in problems}
+    cf.close()
+    run_n, run_ms = prof.get("cross_filter", (1, float("nan")))
+    ded_n, ded_ms = prof.get("dedup", (1, float("nan")))
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    run_bytes = cross_filter_bytes(shapes, problems, 12, 8)
+    ded_bytes = cross_filter_bytes(shapes, problems, 16, 8)
+    run_gbs = run_bytes / (run_ms / run_n / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": run_gbs, "peak": hbm, "unit": "GB/s", "frac": run_gbs / hbm,
+            "traffic": None, "kernel": "CrossFilterRunKernel", "bytes_per_launch": run_bytes,
+            "avg_launch_ms": run_ms / run_n,
+            "bytes_model": "per problem: reference depth + normal code read, refined map written (12 B/px); "
+                           "each source's depth + normal code read once (8 B/px)",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+            "dedup": {"launches": ded_n, "avg_launch_ms": ded_ms / ded_n,
+                      "achieved_gbs": ded_bytes / (ded_ms / 1000.0) / 1e9, "bytes_per_step": ded_bytes},
+            "kernel_ms": {k: round(v[1], 3) for k, v in prof.items()}}
+
+    e2e = None
+    if not args.no_e2e:
+        cf, _ = step(host_args, True)
+        cf.close()
+        torch.cuda.synchronize()
+        barrier(world)
+        t = time.perf_counter()
+        for _ in range(args.steps):
+            cf, out = step(host_args, True)
+            cf.close()
+        torch.cuda.synchronize()
+        el = max_over_ranks(time.perf_counter() - t, world)
+        h2d = sum(d.numel() * 4 + n.numel() * 4 for d, n in host)
+        d2h = sum(o.nbytes for o in out)
+        e2e = {"value": args.steps * V * world / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_cross_filter(scene, maps, problems)
+    kept = float(np.mean([(refined[r] > 0).mean() for r in refined]))
+    def kept_accuracy(d, gt):
+        m = (d > 0) & (gt > 0)
+        return float(np.mean(np.abs(d[m] - gt[m]) <= 0.01 * gt[m])) if m.any() else 0.0
+
+    acc = float(np.mean([kept_accuracy(refined[r], scene.views[r].depth_gt) for r in refined]))
+    if rank == 0:
+        line = {"metric": CF_METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"cross filter + dedup (CrossFilterCuda::Run + DedupRun), {V} views "
+                                       f"{args.width}x{args.height}, each view against the other {V - 1}; noisy "
+                                       f"ground-truth depth/normal maps of the heightfield scene",
+                           "global_batch": V * world, "parallelism": f"view sets sharded, {world} replica(s)",
+                           "l2": f"inputs larger than L2 ({V} x {args.width}x{args.height} depth + normal maps)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clock_info,
+                "filter": {"refined_kept_fraction": kept, "kept_within_1pct_gt": acc}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
 
 
 def ctypes_rate(N, kind):

@@ -82,6 +82,7 @@ typedef struct smvs_options {
   int filter;                              /* :125 */
   int filter_min_num_consistent;           /* :135 */
   double filter_geom_consistency_max_cost; /* :139 */
+  double max_normal_error;                 /* :141 (degrees; cross-view filter) */
   int init_depth_random;                   /* :164 */
   float random_depth_ratio;                /* :166 */
   float random_angle1_range;               /* :167 (radians) */
@@ -309,6 +310,93 @@ void smvs_pool_destroy(smvs_pool* pool);
  * default stream); `out_depth` is W*H floats. */
 int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs_problem* prob, float* out_depth,
                                   int deduplication, void* stream);
+
+/* ---- cross-view filter and deduplication -------------------------------- */
+/* CrossFilterCuda (src/mvs/patch_match_cuda.h:205-269, patch_match_cuda.cu:
+ * 1111-1710): after every view of a cluster has a depth and normal map, each
+ * problem's reference map is re-estimated as the median of the depths its
+ * source views agree on (Run), then the cluster is deduplicated: a pixel seen
+ * consistently by an earlier-processed view is dropped (DedupRun). The
+ * controller drives it at patch_match_controller.cc:5575-6460.
+ *
+ * The set is the cluster's whole_ids / ref_flags (constructor arguments);
+ * problems name views by their index in the set (the reference looks image ids
+ * up in whole_ids, FindSrcImageIds :1427-1455). Run processes every problem in
+ * one launch; DedupRun keeps the reference's sequential problem order wherever
+ * two problems touch the same visibility layer and batches the rest. */
+
+/* Most source views of one cross-filter problem (MAX_NUM_CROSS_SRC,
+ * src/mvs/utils.h:39). */
+#define SMVS_CROSS_MAX_SRC 31
+
+/* One view of the set: an Image's size and K/R/T plus its DepthMap and
+ * NormalMap (patch_match_cuda.cu:1139-1258). */
+typedef struct smvs_filter_view {
+  int width;
+  int height;
+  float K[9];
+  float R[9];
+  float T[3];
+  const float* depth;   /* W*H */
+  const float* normal;  /* 3*W*H planar; NULL when only dedup_run is used */
+  int ref_flag;         /* ref_flags[i]: this view's dedup input is its refined map */
+} smvs_filter_view;
+
+/* One problem: Problem::ref_image_idx and src_image_extend_idxs
+ * (patch_match_options.h:306-353), as indices into the view set. */
+typedef struct smvs_filter_problem {
+  int ref;
+  const int* src;
+  int num_src;          /* 0..SMVS_CROSS_MAX_SRC; 0 = skipped, as the reference does */
+} smvs_filter_problem;
+
+typedef struct smvs_cross_filter smvs_cross_filter;
+
+/* CrossFilterCuda(options, problems, whole_ids, ref_flags) (:1111-1124) plus
+ * InitDepthMaps/InitNormalMaps (:1139-1258): uploads every view's depth map and
+ * encoded normal map (NormalMap::Encode, normal_map.cc:159-181). Views are
+ * copied before the call returns. Reads options depth_diff_threshold,
+ * filter_min_num_consistent, filter_geom_consistency_max_cost,
+ * max_normal_error and gpu_index. Two problems may not share a reference view. */
+int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* views, int num_views,
+                             const smvs_filter_problem* problems, int num_problems, int memory,
+                             void* stream, smvs_cross_filter** out);
+/* CrossFilterCuda::Run (:1493-1559), CrossFilterKernel (kernel_functions.cu:3561-3778). */
+int smvs_cross_filter_run(smvs_cross_filter* cf);
+/* CrossFilterCuda::DedupRun (:1561-1625), DeduplicFilterKernel
+ * (kernel_functions.cu:3780-3916). Views with ref_flag read their refined map
+ * (all zero if no problem refined them), the others their input map
+ * (ResetDepthMaps :1260-1318). Needs filter_min_num_consistent >= 1. */
+int smvs_cross_filter_dedup_run(smvs_cross_filter* cf);
+/* GetRefineDepthMap (:1627-1639): W*H floats; SMVS_ESTATE unless run refined the view. */
+int smvs_cross_filter_get_refined_depth_map(smvs_cross_filter* cf, int view, float* out);
+/* GetDeduplicDepthMap (:1641-1664): the dedup input map where the view's
+ * visibility keeps bit 31, else 0 (GetDeduplicDepthMapsLayer, kernel_functions.cu:3943-3960). */
+int smvs_cross_filter_get_dedup_depth_map(smvs_cross_filter* cf, int view, float* out);
+/* GetDeltDepthMap (:1666-1676): median |depth difference| / (threshold * depth)
+ * per kept pixel; SMVS_ESTATE unless dedup_run processed the view as a reference. */
+int smvs_cross_filter_get_delta_depth_map(smvs_cross_filter* cf, int view, float* out);
+/* GetVisibilyMap (:1678-1704): bit 31 = kept, bit (30 - i) = consistent with source i. */
+int smvs_cross_filter_get_visibility_map(smvs_cross_filter* cf, int view, uint32_t* out);
+/* Device addresses of a view's maps (valid until destroy; NULL where absent). */
+int smvs_cross_filter_get_device_maps(smvs_cross_filter* cf, int view, const float** refined,
+                                      const float** delta, const uint32_t** visibility);
+/* Kernel kinds of smvs_cross_filter_get_profile. */
+typedef enum smvs_cross_filter_kernel {
+  SMVS_CF_KERNEL_RUN = 0,    /* CrossFilterKernel, all problems */
+  SMVS_CF_KERNEL_DEDUP = 1,  /* DeduplicFilterKernel, one launch per level */
+  SMVS_CF_KERNEL_OTHER = 2   /* visibility fill, dedup depth maps */
+} smvs_cross_filter_kernel;
+/* Times every later launch with CUDA events on the filter's stream. */
+int smvs_cross_filter_set_profiling(smvs_cross_filter* cf, int enable);
+/* Timed launches of `kind` and their summed device time (ms); synchronises. */
+int smvs_cross_filter_get_profile(smvs_cross_filter* cf, int kind, int* count, double* total_ms);
+/* Number of kernels this filter launched so far. */
+int64_t smvs_cross_filter_launch_count(smvs_cross_filter* cf);
+/* Number of sequential dedup passes (launches) the last dedup_run needed. */
+int smvs_cross_filter_dedup_levels(smvs_cross_filter* cf);
+int smvs_cross_filter_synchronize(smvs_cross_filter* cf);
+void smvs_cross_filter_destroy(smvs_cross_filter* cf);
 
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);

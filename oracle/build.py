@@ -13,9 +13,13 @@ from pathlib import Path
 ORACLE_DIR = Path(__file__).resolve().parent
 BUILD_DIR = ORACLE_DIR / "_build"
 LIB_PATH = BUILD_DIR / "libsmvs_oracle.so"
-SOURCES = [ORACLE_DIR / "smvs_oracle.c"]
-DEPS = SOURCES + [ORACLE_DIR / "smvs_oracle.h", ORACLE_DIR.parent / "include" / "smvs.h", Path(__file__)]
-CFLAGS = ["-std=c11", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-Wall", "-Wextra"]
+# (source, extra flags). The cross-filter unit performs exactly the IEEE
+# operations its CUDA counterpart spells out, so nothing may be contracted.
+SOURCES = [(ORACLE_DIR / "smvs_oracle.c", []),
+           (ORACLE_DIR / "smvs_oracle_filter.c", ["-ffp-contract=off"])]
+DEPS = [src for src, _ in SOURCES] + [ORACLE_DIR / "smvs_oracle.h", ORACLE_DIR / "orc_pose.h",
+                                      ORACLE_DIR.parent / "include" / "smvs.h", Path(__file__)]
+CFLAGS = ["-std=c11", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-Wall", "-Wextra"]
 
 
 def needs_build() -> bool:
@@ -33,11 +37,21 @@ def build(force: bool = False) -> Path:
     errors = []
     # The system gcc ships libgomp; a CC wrapper may not, so it is the fallback.
     for cc in dict.fromkeys(c for c in (shutil.which("gcc"), os.environ.get("CC"), "cc") if c):
-        cmd = [cc, *CFLAGS, *map(str, SOURCES), "-o", str(tmp), "-lm"]
-        res = subprocess.run(cmd, capture_output=True, text=True)
-        if res.returncode == 0:
-            break
-        errors.append(f"{cc}: {res.stderr}")
+        objs, failed = [], None
+        for src, extra in SOURCES:
+            obj = BUILD_DIR / (src.stem + ".o")
+            res = subprocess.run([cc, *CFLAGS, *extra, "-c", str(src), "-o", str(obj)], capture_output=True, text=True)
+            if res.returncode != 0:
+                failed = res.stderr
+                break
+            objs.append(str(obj))
+        if failed is None:
+            res = subprocess.run([cc, "-shared", "-fopenmp", *objs, "-o", str(tmp), "-lm"], capture_output=True,
+                                 text=True)
+            if res.returncode == 0:
+                break
+            failed = res.stderr
+        errors.append(f"{cc}: {failed}")
     else:
         raise RuntimeError("oracle build failed:\n" + "\n".join(errors))
     os.replace(tmp, LIB_PATH)

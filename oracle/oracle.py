@@ -40,6 +40,19 @@ def lib():
         h.orc_tex_bilinear.restype = C.c_float
         h.orc_tex_bilinear.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
         h.orc_num_threads.restype = C.c_int
+        vp = C.POINTER(N.smvs_filter_view)
+        pp = C.POINTER(N.smvs_filter_problem)
+        h.orc_cross_filter_run.restype = C.c_int
+        h.orc_cross_filter_run.argtypes = [C.POINTER(N.smvs_options), vp, C.c_int, pp, C.c_int, C.c_void_p]
+        h.orc_cross_filter_dedup.restype = C.c_int
+        h.orc_cross_filter_dedup.argtypes = [C.POINTER(N.smvs_options), vp, C.c_int, pp, C.c_int, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+        h.orc_cross_filter_dedup_depth.restype = C.c_int
+        h.orc_cross_filter_dedup_depth.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_encode_normal_map.restype = C.c_int
+        h.orc_encode_normal_map.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        h.orc_cross_filter_poses.restype = C.c_int
+        h.orc_cross_filter_poses.argtypes = [vp, C.c_int, pp, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = h
     return _LIB
 
@@ -141,3 +154,95 @@ def uniform(seed: int, stage: int, pixel: int, draw: int) -> float:
 
 def num_threads() -> int:
     return int(lib().orc_num_threads())
+
+
+# ---------------------------------------------------------------------------
+# Cross-view filter (CrossFilterCuda). A view set is a list of FilterView and
+# problems are (ref, [src, ...]) pairs of indices into it.
+# ---------------------------------------------------------------------------
+class FilterView:
+    def __init__(self, K, R, T, depth, normal=None, ref_flag=False):
+        self.K, self.R, self.T = K, R, T
+        self.depth = np.ascontiguousarray(depth, dtype=np.float32)
+        self.normal = None if normal is None else np.ascontiguousarray(normal, dtype=np.float32)
+        self.ref_flag = bool(ref_flag)
+
+    @property
+    def shape(self):
+        return self.depth.shape
+
+
+def _filter_structs(views, problems):
+    keep = []
+    vs = (N.smvs_filter_view * len(views))()
+    for k, v in enumerate(views):
+        cv = vs[k]
+        cv.height, cv.width = v.depth.shape
+        cv.K[:] = list(np.asarray(v.K, np.float64).reshape(9))
+        cv.R[:] = list(np.asarray(v.R, np.float64).reshape(9))
+        cv.T[:] = list(np.asarray(v.T, np.float64).reshape(3))
+        cv.depth = v.depth.ctypes.data
+        cv.normal = None if v.normal is None else v.normal.ctypes.data
+        cv.ref_flag = int(v.ref_flag)
+    ps = (N.smvs_filter_problem * max(len(problems), 1))()
+    for k, (ref, srcs) in enumerate(problems):
+        arr = (C.c_int * max(len(srcs), 1))(*srcs)
+        keep.append(arr)
+        ps[k].ref, ps[k].src, ps[k].num_src = int(ref), C.cast(arr, C.POINTER(C.c_int)), len(srcs)
+    return vs, ps, keep
+
+
+def cross_filter_run(options: PatchMatchOptions, views, problems) -> dict:
+    """{view index: refined map} for every problem with at least one source."""
+    vs, ps, keep = _filter_structs(views, problems)
+    refined = {r: np.zeros(views[r].shape, np.float32) for r, s in problems if len(s) > 0}
+    ptrs = (C.c_void_p * len(views))(*[refined[k].ctypes.data if k in refined else None for k in range(len(views))])
+    st = lib().orc_cross_filter_run(C.byref(options.to_c()), vs, len(views), ps, len(problems), ptrs)
+    if st:
+        raise RuntimeError(f"orc_cross_filter_run failed ({st})")
+    return refined
+
+
+def cross_filter_dedup(options: PatchMatchOptions, views, problems, refined: dict):
+    """(visibility maps of every view, {view index: delta map})."""
+    vs, ps, keep = _filter_structs(views, problems)
+    vis = [np.zeros(v.shape, np.uint32) for v in views]
+    delta = {r: np.zeros(views[r].shape, np.float32) for r, s in problems if len(s) > 0}
+    rp = (C.c_void_p * len(views))(*[refined[k].ctypes.data if k in refined else None for k in range(len(views))])
+    vp = (C.c_void_p * len(views))(*[v.ctypes.data for v in vis])
+    dp = (C.c_void_p * len(views))(*[delta[k].ctypes.data if k in delta else None for k in range(len(views))])
+    st = lib().orc_cross_filter_dedup(C.byref(options.to_c()), vs, len(views), ps, len(problems), rp, vp, dp)
+    if st:
+        raise RuntimeError(f"orc_cross_filter_dedup failed ({st})")
+    return vis, delta
+
+
+def cross_filter_dedup_depth(view: FilterView, refined, vis) -> np.ndarray:
+    vs, _, keep = _filter_structs([view], [])
+    out = np.zeros(view.shape, np.float32)
+    r = None if refined is None else np.ascontiguousarray(refined, dtype=np.float32)
+    st = lib().orc_cross_filter_dedup_depth(vs, None if r is None else r.ctypes.data,
+                                            np.ascontiguousarray(vis, dtype=np.uint32).ctypes.data, out.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_cross_filter_dedup_depth failed ({st})")
+    return out
+
+
+def cross_filter_poses(views, problem):
+    """(refK[4], refiK[4], poses[num_src, 43]) of one problem."""
+    vs, ps, keep = _filter_structs(views, [problem])
+    refK, refiK = np.zeros(4, np.float32), np.zeros(4, np.float32)
+    poses = np.zeros((max(len(problem[1]), 1), N.SMVS_POSE_FLOATS), np.float32)
+    st = lib().orc_cross_filter_poses(vs, len(views), ps, refK.ctypes.data, refiK.ctypes.data, poses.ctypes.data)
+    if st:
+        raise RuntimeError(f"orc_cross_filter_poses failed ({st})")
+    return refK, refiK, poses[:len(problem[1])]
+
+
+def encode_normal_map(normal) -> np.ndarray:
+    """NormalMap::Encode of a 3 x H x W map (uint32 H x W)."""
+    n = np.ascontiguousarray(normal, dtype=np.float32)
+    out = np.zeros(n.shape[1:], np.uint32)
+    if lib().orc_encode_normal_map(n.ctypes.data, n.shape[2], n.shape[1], out.ctypes.data):
+        raise RuntimeError("orc_encode_normal_map failed")
+    return out

@@ -269,3 +269,151 @@ extern "C" int ref_filter(const RefJob* jp, const float* depth_in, int min_consi
   depth_map.CopyToHost(depth_out, j.W * sizeof(float));
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Cross-view filter: CrossFilterCuda::Run and ::DedupRun
+// (patch_match_cuda.cu:1139-1625) around the reference's CrossFilterKernel and
+// DeduplicFilterKernel. The caller supplies the views' maps (the dedup inputs
+// for ref_dedup, i.e. what ResetDepthMaps uploads), encoded normals and the
+// per-problem pose records.
+// ---------------------------------------------------------------------------
+extern "C" {
+
+struct RefCfView {
+  int W, H;
+  const float* depth;
+  const uint32_t* code;  // may be NULL for ref_dedup
+  int ref_flag;
+};
+
+struct RefCfProblem {
+  int ref, num_src;
+  const int* src;
+  const float* poses;  // num_src * 43
+  float refK[4], refiK[4];
+};
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+std::unique_ptr<CudaArrayWrapper<T>> Layered(int nv, const RefCfView* views, size_t max_w, size_t max_h,
+                                             bool codes) {
+  // InitDepthMaps / InitNormalMaps: every view padded to max_w x max_h with 0.
+  std::vector<T> host(max_w * max_h * nv, T(0));
+  for (int v = 0; v < nv; ++v) {
+    const T* src = codes ? reinterpret_cast<const T*>(views[v].code) : reinterpret_cast<const T*>(views[v].depth);
+    if (!src) continue;
+    for (int r = 0; r < views[v].H; ++r)
+      memcpy(host.data() + max_w * max_h * v + max_w * r, src + (size_t)r * views[v].W, sizeof(T) * views[v].W);
+  }
+  std::unique_ptr<CudaArrayWrapper<T>> dev(new CudaArrayWrapper<T>(max_w, max_h, nv));
+  dev->CopyToDevice(host.data());
+  return dev;
+}
+
+cudaTextureObject_t PosesTexture(const RefCfProblem& p, std::unique_ptr<CudaArrayWrapper<float>>& holder) {
+  SetRefK(p.refK, 0);
+  SetRefInvK(p.refiK, 0);
+  holder.reset(new CudaArrayWrapper<float>(K_NUM_TFORM_PARAMS, p.num_src, 1));
+  holder->CopyToDevice(p.poses);
+  return MakeArrayTexture(holder->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
+}
+
+}  // namespace
+
+extern "C" int ref_cross_filter(int nv, const RefCfView* views, int np, const RefCfProblem* probs,
+                                float filter_max_cost, float max_normal_error, float depth_diff, int min_consistent,
+                                float* const* refined_out) {
+  size_t max_w = 0, max_h = 0;
+  for (int v = 0; v < nv; ++v) {
+    max_w = std::max<size_t>(max_w, views[v].W);
+    max_h = std::max<size_t>(max_h, views[v].H);
+  }
+  auto depth_dev = Layered<float>(nv, views, max_w, max_h, false);
+  auto code_dev = Layered<unsigned int>(nv, views, max_w, max_h, true);
+  cudaTextureObject_t depth_tex = MakeArrayTexture(depth_dev->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
+  cudaTextureObject_t code_tex = MakeArrayTexture(code_dev->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
+  int rc = 0;
+  for (int k = 0; k < np && rc == 0; ++k) {
+    const RefCfProblem& p = probs[k];
+    if (p.num_src < 1) continue;  // :1504-1506
+    if (p.num_src > MAX_NUM_CROSS_SRC) { rc = 1; break; }
+    std::unique_ptr<CudaArrayWrapper<float>> poses_dev;
+    cudaTextureObject_t poses_tex = PosesTexture(p, poses_dev);
+    const int W = views[p.ref].W, H = views[p.ref].H;
+    GpuMat<float> refined(W, H);
+    CUDA_SAFE_CALL(cudaMemset2D(refined.GetPtr(), refined.GetPitch(), 0, W * sizeof(float), H));
+    ImageIdxs idxs;
+    memset(&idxs, 0, sizeof(idxs));
+    idxs.list[0] = p.ref;
+    for (int i = 0; i < p.num_src; ++i) idxs.list[i + 1] = p.src[i];
+    idxs.length = p.num_src + 1;
+    // 32x8 blocks over the padded size (the reference uses 32x32; every
+    // thread is independent and indexes from blockDim).
+    dim3 b(THREADS_PER_BLOCK, 8), g((max_w - 1) / THREADS_PER_BLOCK + 1, (max_h - 1) / 8 + 1);
+    CrossFilterKernel<<<g, b>>>(p.num_src, W, H, 0.0f, filter_max_cost, max_normal_error, depth_diff,
+                                std::min(min_consistent, p.num_src), idxs, refined, depth_tex, code_tex, poses_tex, 0);
+    if (cudaGetLastError() != cudaSuccess) rc = 2;
+    CUDA_SYNC_AND_CHECK();
+    if (rc == 0) refined.CopyToHost(refined_out[p.ref], W * sizeof(float));
+    cudaDestroyTextureObject(poses_tex);
+  }
+  cudaDestroyTextureObject(depth_tex);
+  cudaDestroyTextureObject(code_tex);
+  return rc;
+}
+
+extern "C" int ref_dedup(int nv, const RefCfView* views, int np, const RefCfProblem* probs, float filter_max_cost,
+                         float depth_diff, int min_consistent, uint32_t* const* vis_out, float* const* delta_out) {
+  size_t max_w = 0, max_h = 0;
+  for (int v = 0; v < nv; ++v) {
+    max_w = std::max<size_t>(max_w, views[v].W);
+    max_h = std::max<size_t>(max_h, views[v].H);
+  }
+  auto depth_dev = Layered<float>(nv, views, max_w, max_h, false);
+  cudaTextureObject_t depth_tex = MakeArrayTexture(depth_dev->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
+  GpuMat<uint32_t> vis(max_w, max_h, nv);
+  dim3 b(THREADS_PER_BLOCK, 8), g((max_w - 1) / THREADS_PER_BLOCK + 1, (max_h - 1) / 8 + 1);
+  FillGpuMat<<<g, b>>>(max_w, max_h, vis);
+  int rc = cudaGetLastError() != cudaSuccess ? 3 : 0;
+  CUDA_SYNC_AND_CHECK();
+  for (int k = 0; k < np && rc == 0; ++k) {
+    const RefCfProblem& p = probs[k];
+    if (p.num_src < 1) continue;  // :1568-1570
+    if (p.num_src > MAX_NUM_CROSS_SRC) { rc = 1; break; }
+    std::unique_ptr<CudaArrayWrapper<float>> poses_dev;
+    cudaTextureObject_t poses_tex = PosesTexture(p, poses_dev);
+    const int W = views[p.ref].W, H = views[p.ref].H;
+    ImageLists lists;
+    memset(&lists, 0, sizeof(lists));
+    lists.list[0].id = p.ref;
+    lists.list[0].flag = views[p.ref].ref_flag != 0;
+    for (int i = 0; i < p.num_src; ++i) {
+      lists.list[i + 1].id = p.src[i];
+      lists.list[i + 1].flag = views[p.src[i]].ref_flag != 0;
+    }
+    lists.length = p.num_src + 1;
+    GpuMat<float> delta(W, H);
+    // The reference's FillWithScalar clears W*H*4 bytes of a pitched buffer
+    // (gpu_mat.h:240-243), leaving later rows unset; clear all rows.
+    CUDA_SAFE_CALL(cudaMemset2D(delta.GetPtr(), delta.GetPitch(), 0, W * sizeof(float), H));
+    DeduplicFilterKernel<<<g, b>>>(p.num_src, W, H, filter_max_cost, depth_diff, std::min(min_consistent, p.num_src),
+                                   lists, delta, vis, depth_tex, poses_tex, 0);
+    if (cudaGetLastError() != cudaSuccess) rc = 2;
+    CUDA_SYNC_AND_CHECK();
+    if (rc == 0) delta.CopyToHost(delta_out[p.ref], W * sizeof(float));
+    cudaDestroyTextureObject(poses_tex);
+  }
+  if (rc == 0) {
+    std::vector<uint32_t> all(max_w * max_h * nv);
+    vis.CopyToHost(all.data(), max_w * sizeof(uint32_t));
+    for (int v = 0; v < nv; ++v)
+      for (int r = 0; r < views[v].H; ++r)
+        memcpy(vis_out[v] + (size_t)r * views[v].W, all.data() + max_w * max_h * v + max_w * r,
+               sizeof(uint32_t) * views[v].W);
+  }
+  cudaDestroyTextureObject(depth_tex);
+  return rc;
+}

@@ -40,6 +40,15 @@ class RefOut(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("depth", "normal", "conf", "cost", "view_sel")]
 
 
+class RefCfView(C.Structure):
+    _fields_ = [("W", C.c_int), ("H", C.c_int), ("depth", C.c_void_p), ("code", C.c_void_p), ("ref_flag", C.c_int)]
+
+
+class RefCfProblem(C.Structure):
+    _fields_ = [("ref", C.c_int), ("num_src", C.c_int), ("src", C.POINTER(C.c_int)), ("poses", C.c_void_p),
+                ("refK", C.c_float * 4), ("refiK", C.c_float * 4)]
+
+
 def available() -> bool:
     return LIB_PATH.exists()
 
@@ -55,6 +64,12 @@ def lib():
         h.ref_filter.restype = C.c_int
         h.ref_filter.argtypes = [C.POINTER(RefJob), C.c_void_p, C.c_int, C.c_float, C.c_void_p]
         h.ref_max_num_src.restype = C.c_int
+        h.ref_cross_filter.restype = C.c_int
+        h.ref_cross_filter.argtypes = [C.c_int, C.POINTER(RefCfView), C.c_int, C.POINTER(RefCfProblem), C.c_float,
+                                       C.c_float, C.c_float, C.c_int, C.c_void_p]
+        h.ref_dedup.restype = C.c_int
+        h.ref_dedup.argtypes = [C.c_int, C.POINTER(RefCfView), C.c_int, C.POINTER(RefCfProblem), C.c_float,
+                                C.c_float, C.c_int, C.c_void_p, C.c_void_p]
         _LIB = h
     return _LIB
 
@@ -141,3 +156,69 @@ def run_filter(options: PatchMatchOptions, problem: Problem, poses: np.ndarray) 
                         out.ctypes.data) != 0:
         raise RuntimeError("reference filter rejected the job")
     return out
+
+
+# ---------------------------------------------------------------------------
+# Cross-view filter through the reference's CrossFilterKernel /
+# DeduplicFilterKernel. Views are oracle.oracle.FilterView; problems are
+# (ref, [src, ...]) index pairs; pose records come from the CPU oracle.
+# ---------------------------------------------------------------------------
+def _cf_structs(views, problems, depths, codes):
+    from oracle import oracle as O
+    keep = []
+    vs = (RefCfView * len(views))()
+    for k, v in enumerate(views):
+        d = np.ascontiguousarray(depths[k], np.float32)
+        keep.append(d)
+        vs[k].H, vs[k].W = d.shape
+        vs[k].depth = d.ctypes.data
+        if codes is not None and codes[k] is not None:
+            c = np.ascontiguousarray(codes[k], np.uint32)
+            keep.append(c)
+            vs[k].code = c.ctypes.data
+        vs[k].ref_flag = int(v.ref_flag)
+    ps = (RefCfProblem * max(len(problems), 1))()
+    for k, (ref, srcs) in enumerate(problems):
+        arr = (C.c_int * max(len(srcs), 1))(*srcs)
+        keep.append(arr)
+        ps[k].ref, ps[k].num_src, ps[k].src = int(ref), len(srcs), C.cast(arr, C.POINTER(C.c_int))
+        if srcs:
+            refK, refiK, poses = O.cross_filter_poses(views, (ref, srcs))
+            poses = np.ascontiguousarray(poses, np.float32)
+            keep.append(poses)
+            ps[k].poses = poses.ctypes.data
+            ps[k].refK[:] = list(refK)
+            ps[k].refiK[:] = list(refiK)
+    return vs, ps, keep
+
+
+def cross_filter(options: PatchMatchOptions, views, problems) -> dict:
+    """{view index: refined map} from the reference's CrossFilterKernel."""
+    from oracle import oracle as O
+    codes = [None if v.normal is None else O.encode_normal_map(v.normal) for v in views]
+    vs, ps, keep = _cf_structs(views, problems, [v.depth for v in views], codes)
+    refined = {r: np.zeros(views[r].shape, np.float32) for r, s in problems if len(s) > 0}
+    ptrs = (C.c_void_p * len(views))(*[refined[k].ctypes.data if k in refined else None for k in range(len(views))])
+    rc = lib().ref_cross_filter(len(views), vs, len(problems), ps, options.filter_geom_consistency_max_cost,
+                                options.max_normal_error, options.depth_diff_threshold,
+                                options.filter_min_num_consistent, ptrs)
+    if rc:
+        raise RuntimeError(f"reference cross filter failed (driver status {rc})")
+    return refined
+
+
+def dedup(options: PatchMatchOptions, views, problems, refined: dict):
+    """(visibility maps, {view index: delta map}) from the reference's
+    DeduplicFilterKernel, on the dedup inputs ResetDepthMaps builds."""
+    depths = [(refined[k] if k in refined else np.zeros(v.shape, np.float32)) if v.ref_flag else v.depth
+              for k, v in enumerate(views)]
+    vs, ps, keep = _cf_structs(views, problems, depths, None)
+    vis = [np.zeros(v.shape, np.uint32) for v in views]
+    delta = {r: np.zeros(views[r].shape, np.float32) for r, s in problems if len(s) > 0}
+    vp = (C.c_void_p * len(views))(*[v.ctypes.data for v in vis])
+    dp = (C.c_void_p * len(views))(*[delta[k].ctypes.data if k in delta else None for k in range(len(views))])
+    rc = lib().ref_dedup(len(views), vs, len(problems), ps, options.filter_geom_consistency_max_cost,
+                         options.depth_diff_threshold, options.filter_min_num_consistent, vp, dp)
+    if rc:
+        raise RuntimeError(f"reference dedup failed (driver status {rc})")
+    return vis, delta

@@ -57,6 +57,32 @@ int orc_eval_costs(const smvs_options* opt, const smvs_problem* prob, int n_pix,
                    const int* rows, const int* cols, const float* depths,
                    const float* normals /* n_pix*3 */, float* costs32, double* costs64);
 
+/* CrossFilterCuda::Run over a view set (patch_match_cuda.cu:1493-1559): for each
+ * problem with at least one source, refined[ref] (W*H of the reference view) is
+ * written; other entries of `refined` are not touched and may be NULL. */
+int orc_cross_filter_run(const smvs_options* opt, const smvs_filter_view* views, int num_views,
+                         const smvs_filter_problem* problems, int num_problems, float* const* refined);
+
+/* CrossFilterCuda::DedupRun (:1561-1625). Dedup input of view v: refined[v]
+ * when views[v].ref_flag (an all-zero map when refined or refined[v] is NULL),
+ * else views[v].depth. vis[v] (W*H, every view) is initialised and updated;
+ * delta[ref] (W*H) is written for each problem with at least one source. */
+int orc_cross_filter_dedup(const smvs_options* opt, const smvs_filter_view* views, int num_views,
+                           const smvs_filter_problem* problems, int num_problems, const float* const* refined,
+                           uint32_t* const* vis, float* const* delta);
+
+/* GetDeduplicDepthMap (:1641-1664) of one view after orc_cross_filter_dedup. */
+int orc_cross_filter_dedup_depth(const smvs_filter_view* view, const float* refined, const uint32_t* vis,
+                                 float* out);
+
+/* The reference K, its inverse and the 43-float source pose records of one
+ * cross-filter problem (InitTransforms, patch_match_cuda.cu:1320-1407). */
+int orc_cross_filter_poses(const smvs_filter_view* views, int num_views, const smvs_filter_problem* problem,
+                           float refK[4], float refiK[4], float* poses);
+
+/* NormalMap::Encode (normal_map.cc:159-181) of a planar 3*W*H map. */
+int orc_encode_normal_map(const float* normal, int width, int height, uint32_t* code);
+
 /* The generator shared with the engine: uniform in (0, 1]. */
 float orc_uniform(uint64_t seed, uint32_t stage, uint32_t pixel, uint32_t draw);
 

@@ -12,6 +12,7 @@ from pathlib import Path
 
 SMVS_MAX_SRC = 32
 SMVS_POSE_FLOATS = 43
+SMVS_CROSS_MAX_SRC = 31
 
 SMVS_OK, SMVS_EINVAL, SMVS_ENOMEM, SMVS_ECUDA, SMVS_ESTATE, SMVS_EIO, SMVS_ETIMEDOUT, SMVS_ECANCELED = range(8)
 PIX_U8, PIX_F32 = 0, 1
@@ -22,6 +23,8 @@ MEM_HOST, MEM_DEVICE = 0, 1
 KERNEL_NAMES = ["convert", "prep_ref", "init", "init_conf", "sweep", "local_opt", "mask", "filter", "post"]
 JOB_QUEUED, JOB_ACTIVE, JOB_DONE, JOB_FAILED = range(4)
 MAP_DEPTH, MAP_NORMAL, MAP_CONF, MAP_COST, MAP_VIEW_SEL = range(5)
+CF_KERNEL_RUN, CF_KERNEL_DEDUP, CF_KERNEL_OTHER = range(3)
+CF_KERNEL_NAMES = ["cross_filter", "dedup", "other"]
 
 STATUS_NAMES = {0: "SMVS_OK", 1: "SMVS_EINVAL", 2: "SMVS_ENOMEM", 3: "SMVS_ECUDA", 4: "SMVS_ESTATE",
                 5: "SMVS_EIO", 6: "SMVS_ETIMEDOUT", 7: "SMVS_ECANCELED"}
@@ -47,6 +50,7 @@ class smvs_options(C.Structure):
         ("geom_consistency_regularizer", C.c_double), ("geom_consistency_max_cost", C.c_double),
         ("filter", C.c_int), ("filter_min_num_consistent", C.c_int),
         ("filter_geom_consistency_max_cost", C.c_double),
+        ("max_normal_error", C.c_double),
         ("init_depth_random", C.c_int),
         ("random_depth_ratio", C.c_float), ("random_angle1_range", C.c_float), ("random_angle2_range", C.c_float),
         ("init_ncc_matching_cost", C.c_double), ("max_ncc_matching_cost", C.c_double),
@@ -100,6 +104,18 @@ class smvs_device_maps(C.Structure):
     ]
 
 
+class smvs_filter_view(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int),
+        ("K", C.c_float * 9), ("R", C.c_float * 9), ("T", C.c_float * 3),
+        ("depth", C.c_void_p), ("normal", C.c_void_p), ("ref_flag", C.c_int),
+    ]
+
+
+class smvs_filter_problem(C.Structure):
+    _fields_ = [("ref", C.c_int), ("src", C.POINTER(C.c_int)), ("num_src", C.c_int)]
+
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "smvs_options_default": (C.c_int, [C.POINTER(smvs_options)]),
@@ -130,6 +146,23 @@ _SIGNATURES = {
     "smvs_encode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "smvs_decode_normal_map": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p]),
     "smvs_write_maps": (C.c_int, [C.c_void_p, C.c_char_p, C.c_char_p, C.c_char_p]),
+    "smvs_cross_filter_create": (C.c_int, [C.POINTER(smvs_options), C.POINTER(smvs_filter_view), C.c_int,
+                                           C.POINTER(smvs_filter_problem), C.c_int, C.c_int, C.c_void_p,
+                                           C.POINTER(C.c_void_p)]),
+    "smvs_cross_filter_run": (C.c_int, [C.c_void_p]),
+    "smvs_cross_filter_dedup_run": (C.c_int, [C.c_void_p]),
+    "smvs_cross_filter_get_refined_depth_map": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "smvs_cross_filter_get_dedup_depth_map": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "smvs_cross_filter_get_delta_depth_map": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "smvs_cross_filter_get_visibility_map": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "smvs_cross_filter_get_device_maps": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
+                                                    C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "smvs_cross_filter_launch_count": (C.c_int64, [C.c_void_p]),
+    "smvs_cross_filter_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "smvs_cross_filter_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "smvs_cross_filter_dedup_levels": (C.c_int, [C.c_void_p]),
+    "smvs_cross_filter_synchronize": (C.c_int, [C.c_void_p]),
+    "smvs_cross_filter_destroy": (None, [C.c_void_p]),
     "smvs_pool_options_default": (C.c_int, [C.POINTER(smvs_pool_options)]),
     "smvs_pool_create": (C.c_int, [C.POINTER(smvs_pool_options), C.c_void_p, C.POINTER(C.c_void_p)]),
     "smvs_pool_add_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(smvs_view), C.c_int]),

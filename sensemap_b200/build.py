@@ -19,8 +19,13 @@ BUILD_DIR = PKG_DIR / "_build"
 INCLUDE_DIR = PKG_DIR.parent / "include"
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "--use_fast_math", "-lineinfo", "-Xcompiler", "-fPIC,-O3",
-              "-Xptxas", "-v"]
+COMMON_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-v"]
+NVCC_FLAGS = COMMON_FLAGS + ["--use_fast_math"]
+# Units whose kernels must reproduce IEEE single-precision results exactly
+# (no contraction into FMA, correctly rounded division and square root, no
+# flush to zero): the cross-view filter's decisions and medians.
+EXACT_FLAGS = COMMON_FLAGS + ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
+EXACT_UNITS = {"smvs_cross_filter.cu"}
 
 
 def _nvcc() -> str:
@@ -48,7 +53,8 @@ def needs_build() -> bool:
 
 def _compile(src: Path, nvcc: str) -> tuple[Path, str]:
     obj = BUILD_DIR / (src.name + ".o")
-    cmd = [nvcc, *NVCC_FLAGS, *ARCH_FLAGS, "-c", str(src), "-o", str(obj)]
+    flags = EXACT_FLAGS if src.name in EXACT_UNITS else NVCC_FLAGS
+    cmd = [nvcc, *flags, *ARCH_FLAGS, "-c", str(src), "-o", str(obj)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"nvcc failed on {src.name}:\n{res.stderr}")

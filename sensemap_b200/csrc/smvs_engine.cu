@@ -284,6 +284,7 @@ int smvs_options_default(smvs_options* o) {
   o->filter = 1;
   o->filter_min_num_consistent = 1;
   o->filter_geom_consistency_max_cost = 1.0f;
+  o->max_normal_error = 15.0f;
   o->init_depth_random = 0;  // = !geom_consistency (patch_match_options.h:164)
   o->random_depth_ratio = 0.004f;
   o->random_angle1_range = (float)(20.0 * M_PI / 180.0);

@@ -6,6 +6,7 @@
 // quantised coordinates. Paths: <stereo>/{depth_maps,normal_maps,conf_maps}/
 // <image>.<photometric|geometric>.bin (src/base/common.h:16-33).
 #include <cerrno>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -105,8 +106,9 @@ int smvs_encode_normal_map(const float* normal, int w, int h, uint32_t* code) {
     const float m = 1.0f / std::sqrt(1 - s);
     float q1 = (float)(n1 * 0.5 * m);
     float q2 = (float)(n2 * 0.5 * m);
-    q1 = std::fmin(0.999999f, std::fmax(q1, -0.999999f));
-    q2 = std::fmin(0.999999f, std::fmax(q2, -0.999999f));
+    // std::min / std::max as the reference calls them: a NaN (n0 == -1) clamps to +0.999999.
+    q1 = std::min(0.999999f, std::max(q1, -0.999999f));
+    q2 = std::min(0.999999f, std::max(q2, -0.999999f));
     const uint32_t iq1 = (uint32_t)((q1 + 1) * decode_factor);
     const uint32_t iq2 = (uint32_t)((q2 + 1) * decode_factor);
     code[i] = (iq1 << 16) | iq2;

@@ -39,6 +39,7 @@ class PatchMatchOptions:
     filter: bool = True
     filter_min_num_consistent: int = 1
     filter_geom_consistency_max_cost: float = 1.0
+    max_normal_error: float = 15.0
     init_depth_random: bool = False
     random_depth_ratio: float = 0.004
     random_angle1_range: float = math.radians(20.0)
@@ -105,6 +106,7 @@ class Problem:
     images: Sequence[View]
     src_image_scales: Sequence[float] = field(default_factory=list)
     mask: Optional[object] = None  # H x W uint8 mask of the reference view
+    src_image_extend_idxs: Sequence[int] = field(default_factory=list)  # cross-filter neighbours (:314)
 
 
 class DeviceBuffer:

@@ -318,3 +318,25 @@ def normal_accuracy(normal: np.ndarray, gt: np.ndarray, degrees: float = 10.0, m
     if mask is not None:
         ok = ok[mask]
     return float(np.mean(ok))
+
+
+def noisy_maps(scene: Scene, seed: int = 0, rel_noise: float = 0.002, outlier_frac: float = 0.03,
+               hole_frac: float = 0.02, normal_noise_deg: float = 3.0) -> list:
+    """(depth, normal) per view: the scene's ground truth with the errors a
+    PatchMatch pass leaves — relative depth noise, outliers drawn from
+    [0.5, 1.5] x depth, holes (0) and perturbed normals. The input of the
+    cross-view filter."""
+    gen = np.random.default_rng(seed)
+    out = []
+    for v in scene.views:
+        gt = v.depth_gt.astype(np.float64)
+        d = gt * (1.0 + rel_noise * gen.standard_normal(gt.shape))
+        u = gen.random(gt.shape)
+        out_m = u < outlier_frac
+        d[out_m] = gt[out_m] * gen.uniform(0.5, 1.5, size=int(out_m.sum()))
+        d[(u >= outlier_frac) & (u < outlier_frac + hole_frac)] = 0.0
+        d[gt <= 0] = 0.0
+        n = v.normal_gt.astype(np.float64) + math.radians(normal_noise_deg) * gen.standard_normal(v.normal_gt.shape)
+        n /= np.maximum(np.linalg.norm(n, axis=0, keepdims=True), 1e-12)
+        out.append((d.astype(np.float32), n.astype(np.float32)))
+    return out

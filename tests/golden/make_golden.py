@@ -11,6 +11,12 @@ reference's outputs), so tests replay it on the CPU oracle without rendering:
   ref_filter_planes.npz    FilterDepthMapsKernel decisions on perturbed maps
   ref_run_planes.npz       a full photometric run (6 iterations) of the
                            reference (cuRAND draws; compared statistically)
+  ref_crossfilter_planes.npz  CrossFilterKernel refined maps and
+                           DeduplicFilterKernel visibility/delta maps of a
+                           6-view set (CrossFilterCuda::Run + DedupRun)
+
+    python tests/golden/make_golden.py [out_dir] --only crossfilter
+regenerates the last fixture alone.
 """
 from __future__ import annotations
 
@@ -38,8 +44,36 @@ def pack_scene(scene, prob, opt, poses):
     return d
 
 
-def main(out_dir: Path):
+def cross_filter_case(out_dir: Path):
+    from sensemap_b200.patch_match import PatchMatchOptions
+    from tests.helpers import filter_set
+    scene, views, problems = filter_set(seed=21, w=96, h=72, f=75.0, n_views=6,
+                                        ref_flags=[True, True, True, True, True, False])
+    problems = [(r, s) for r, s in problems if r != 5]  # view 5 is a source only
+    opt = PatchMatchOptions(filter_min_num_consistent=2)
+    refined = ref.cross_filter(opt, views, problems)
+    vis, delta = ref.dedup(opt, views, problems, refined)
+    refs = sorted(refined)
+    src = np.full((len(problems), max(len(s) for _, s in problems)), -1, np.int32)
+    for k, (_, s_) in enumerate(problems):
+        src[k, :len(s_)] = s_
+    np.savez_compressed(out_dir / "ref_crossfilter_planes.npz",
+                        K=np.stack([v.K for v in views]), R=np.stack([v.R for v in views]),
+                        T=np.stack([v.T for v in views]), depth=np.stack([v.depth for v in views]),
+                        normal=np.stack([v.normal for v in views]),
+                        ref_flag=np.array([v.ref_flag for v in views]),
+                        problem_ref=np.array([r for r, _ in problems], np.int32), problem_src=src,
+                        filter_min_num_consistent=opt.filter_min_num_consistent,
+                        refined_views=np.array(refs, np.int32), refined=np.stack([refined[r] for r in refs]),
+                        vis=np.stack(vis), delta=np.stack([delta[r] for r in refs]))
+
+
+def main(out_dir: Path, only: str = ""):
     out_dir.mkdir(parents=True, exist_ok=True)
+    if only == "crossfilter":
+        cross_filter_case(out_dir)
+        print("written to", out_dir)
+        return
     scene = syn.planes_scene(seed=11, width=96, height=72, focal=75.0, num_src=4)
     base_opt = photometric_options(scene, iters=0, init_depth_random=False)
     # Case A: InitConfMapKernel on given hypotheses.
@@ -73,8 +107,12 @@ def main(out_dir: Path):
     np.savez_compressed(out_dir / "ref_run_planes.npz", **pack_scene(scene_c, cprob, copt, cposes),
                         depth=rc["depth"], normal=rc["normal"].astype(np.float16),
                         gt_accuracy=syn.depth_accuracy(rc["depth"], scene_c.views[cprob.ref_image_idx].depth_gt))
+    cross_filter_case(out_dir)
     print("written to", out_dir)
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path(__file__).resolve().parent)
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    only = sys.argv[sys.argv.index("--only") + 1] if "--only" in sys.argv else ""
+    args = [a for a in args if a != only]
+    main(Path(args[0]) if args else Path(__file__).resolve().parent, only)

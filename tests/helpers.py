@@ -57,3 +57,33 @@ def frac_close(a, b, rel=0.01, mask=None):
     if mask is not None:
         ok = ok[mask]
     return float(np.mean(ok))
+
+
+def filter_set(seed=0, w=160, h=120, f=125.0, n_views=6, ref_flags=None, neighbours=None, **noise):
+    """A cross-filter view set from a planes scene: (scene, oracle FilterViews,
+    problems as (ref, [src...]) with every view a reference of all others
+    unless `neighbours` (a per-view source list) is given)."""
+    from oracle import oracle as O
+    scene = syn.planes_scene(seed=seed, width=w, height=h, focal=f, num_src=n_views - 1)
+    maps = syn.noisy_maps(scene, seed=seed + 100, **noise)
+    flags = [True] * n_views if ref_flags is None else ref_flags
+    views = [O.FilterView(v.K, v.R, v.T, d, n, ref_flag=fl) for v, (d, n), fl in zip(scene.views, maps, flags)]
+    if neighbours is None:
+        neighbours = [[s for s in range(n_views) if s != r] for r in range(n_views)]
+    problems = [(r, list(nb)) for r, nb in enumerate(neighbours)]
+    return scene, views, problems
+
+
+def filter_api_inputs(views, problems, device=False):
+    """The same set as CrossFilterCuda arguments: (problems, whole_ids, ref_flags)
+    over View objects (image ids = set indices)."""
+    import torch
+    ims = []
+    for v in views:
+        d, n = v.depth, v.normal
+        if device:
+            d = torch.from_numpy(d).cuda()
+            n = None if n is None else torch.from_numpy(n).cuda()
+        ims.append(View(None, v.K, v.R, v.T, depth=d, normal=n))
+    probs = [Problem(r, [], ims, src_image_extend_idxs=list(s)) for r, s in problems]
+    return probs, list(range(len(views))), [v.ref_flag for v in views]

@@ -78,3 +78,32 @@ def test_oracle_run_matches_reference_statistically():
     assert abs(acc_oracle - acc_ref) < 0.03, (acc_oracle, acc_ref)
     agree = np.mean(np.abs(out["depth"] - z["depth"]) <= 0.01 * np.abs(z["depth"]))
     assert agree > 0.8, agree
+
+
+def test_oracle_cross_filter_matches_reference_kernels():
+    """CrossFilterCuda::Run + DedupRun through the reference's CrossFilterKernel
+    and DeduplicFilterKernel (fast-math, texture point sampling) against the
+    oracle's IEEE restatement on the same 6-view set."""
+    z = load("ref_crossfilter_planes.npz")
+    views = [orc.FilterView(z["K"][k], z["R"][k], z["T"][k], z["depth"][k], z["normal"][k], bool(z["ref_flag"][k]))
+             for k in range(len(z["depth"]))]
+    problems = [(int(r), [int(s) for s in row if s >= 0]) for r, row in zip(z["problem_ref"], z["problem_src"])]
+    opt = PatchMatchOptions(filter_min_num_consistent=int(z["filter_min_num_consistent"]))
+    refined = orc.cross_filter_run(opt, views, problems)
+    for k, r in enumerate(z["refined_views"]):
+        got, ref = refined[int(r)], z["refined"][k]
+        # measured: identical decisions, kept depths within 2 ulp (fast-math reciprocals)
+        assert np.mean((got > 0) == (ref > 0)) > 0.999
+        both = (got > 0) & (ref > 0)
+        np.testing.assert_allclose(got[both], ref[both], rtol=1e-6)
+    # dedup replayed on the reference's refined maps (its own dedup inputs)
+    ref_refined = {int(r): z["refined"][k] for k, r in enumerate(z["refined_views"])}
+    vis, delta = orc.cross_filter_dedup(opt, views, problems, ref_refined)
+    for k in range(len(views)):
+        assert np.mean(vis[k] == z["vis"][k]) > 0.999
+    for k, r in enumerate(z["refined_views"]):
+        keep = (z["vis"][int(r)] & 0x80000000) != 0
+        if not keep.any():
+            continue
+        d, rd = delta[int(r)][keep], z["delta"][k][keep]
+        assert np.mean(np.abs(d - rd) <= 1e-4 + 1e-4 * np.abs(rd)) > 0.99
