@@ -354,10 +354,14 @@ typedef struct smvs_cross_filter smvs_cross_filter;
 
 /* CrossFilterCuda(options, problems, whole_ids, ref_flags) (:1111-1124) plus
  * InitDepthMaps/InitNormalMaps (:1139-1258): uploads every view's depth map and
- * encoded normal map (NormalMap::Encode, normal_map.cc:159-181). Views are
- * copied before the call returns. Reads options depth_diff_threshold,
- * filter_min_num_consistent, filter_geom_consistency_max_cost,
- * max_normal_error and gpu_index. Two problems may not share a reference view. */
+ * its normal map as the kernel sees it (NormalMap::Encode, normal_map.cc:
+ * 159-181, then the kernel's decode). Host maps (memory SMVS_MEM_HOST) are
+ * copied before the call returns; device maps are read in stream order on
+ * `stream`. Reads options depth_diff_threshold, filter_min_num_consistent,
+ * filter_geom_consistency_max_cost, max_normal_error and gpu_index. Two
+ * problems may not share a reference view; a view has fewer than 2^31 pixels.
+ * Run, dedup_run and the device-map query only enqueue work; the host getters
+ * wait for it. */
 int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* views, int num_views,
                              const smvs_filter_problem* problems, int num_problems, int memory,
                              void* stream, smvs_cross_filter** out);
@@ -397,6 +401,39 @@ int64_t smvs_cross_filter_launch_count(smvs_cross_filter* cf);
 int smvs_cross_filter_dedup_levels(smvs_cross_filter* cf);
 int smvs_cross_filter_synchronize(smvs_cross_filter* cf);
 void smvs_cross_filter_destroy(smvs_cross_filter* cf);
+/* Cross filters allocate from a per-device stream-ordered pool that keeps
+ * freed blocks for the next filter; this returns them to the device
+ * (synchronises the device). gpu_index -1 = current device. */
+int smvs_cross_filter_release_cache(int gpu_index);
+
+/* ---- initial depth/normal maps from the model ---------------------------- */
+/* The maps PatchMatchController builds for a view before a PatchMatch pass
+ * with init_depth_random == 0 (patch_match_controller.cc:4376-4460), as GPU
+ * scatters with the reference's depth tests (results do not depend on the
+ * order of points or faces). `view` supplies width, height, K, R and T (pixels
+ * are not read). Outputs: depth W*H (0 where nothing landed), normal 3*W*H
+ * planar (0 where nothing landed), and optionally depth_range[2], the pair
+ * the reference returns (first = 1e-6, second = 1.1 x the largest depth
+ * written, or 110 when nothing was). `memory` says where every array lives;
+ * with SMVS_MEM_DEVICE and depth_range NULL the call only enqueues work on
+ * `stream`, otherwise it waits for it. */
+/* InitDepthMap (:1205-1307) + InitDepthMapFromSparsePoint (:483-518): `xyz`
+ * are the sparse points whose track contains the view (n x 3 float); each
+ * lands in a 7x7 window at its truncated pixel, nearest depth kept, normal 0. */
+int smvs_init_depth_from_sparse_points(const smvs_view* view, const float* xyz, size_t num_points, int memory,
+                                       float* depth, float* normal, float* depth_range, void* stream);
+/* Model2Depth (:520-642): TriangleMesh vertices_ (n x 3 double), faces_
+ * (m x 3 int32) and face_normals_ (m x 3 double), rasterised with back-face
+ * and field-of-view culling; normals are the camera-frame face normals. */
+int smvs_init_depth_from_mesh(const smvs_view* view, const double* vertices, size_t num_vertices,
+                              const int32_t* faces, size_t num_faces, const double* face_normals, int memory,
+                              float* depth, float* normal, float* depth_range, void* stream);
+/* Ply2Depth (:643-750): oriented dense points (PlyPoint x/y/z and nx/ny/nz as
+ * two n x 3 float arrays) splatted into the odd pixels of a window of
+ * 2^level pixels around each (level = PLY_INIT_DEPTH_LEVEL = 2, utils.h:40). */
+int smvs_init_depth_from_dense_points(const smvs_view* view, const float* xyz, const float* normals,
+                                      size_t num_points, int level, int memory, float* depth, float* normal,
+                                      float* depth_range, void* stream);
 
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);

@@ -51,6 +51,14 @@ def lib():
         h.orc_cross_filter_dedup_depth.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_encode_normal_map.restype = C.c_int
         h.orc_encode_normal_map.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        for name in ("orc_init_from_sparse_points", "orc_init_from_mesh", "orc_init_from_dense_points"):
+            getattr(h, name).restype = C.c_int
+        h.orc_init_from_sparse_points.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_size_t, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p]
+        h.orc_init_from_mesh.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                         C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_init_from_dense_points.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_cross_filter_poses.restype = C.c_int
         h.orc_cross_filter_poses.argtypes = [vp, C.c_int, pp, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = h
@@ -246,3 +254,45 @@ def encode_normal_map(normal) -> np.ndarray:
     if lib().orc_encode_normal_map(n.ctypes.data, n.shape[2], n.shape[1], out.ctypes.data):
         raise RuntimeError("orc_encode_normal_map failed")
     return out
+
+
+# ---------------------------------------------------------------------------
+# Initial maps from the model (InitDepthMap / Model2Depth / Ply2Depth).
+# ---------------------------------------------------------------------------
+def _init_view(width, height, K, R, T):
+    from sensemap_b200.init_maps import _view
+    return _view(width, height, K, R, T)
+
+
+def _init_out(width, height):
+    return np.zeros((height, width), np.float32), np.zeros((3, height, width), np.float32), np.zeros(2, np.float32)
+
+
+def init_from_sparse_points(width, height, K, R, T, xyz):
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    d, n, r = _init_out(width, height)
+    if lib().orc_init_from_sparse_points(C.byref(_init_view(width, height, K, R, T)), x.ctypes.data, len(x),
+                                         d.ctypes.data, n.ctypes.data, r.ctypes.data):
+        raise RuntimeError("orc_init_from_sparse_points failed")
+    return d, n, (r[0], r[1])
+
+
+def init_from_mesh(width, height, K, R, T, vertices, faces, face_normals):
+    v = np.ascontiguousarray(vertices, np.float64).reshape(-1, 3)
+    f = np.ascontiguousarray(faces, np.int32).reshape(-1, 3)
+    fn = np.ascontiguousarray(face_normals, np.float64).reshape(-1, 3)
+    d, n, r = _init_out(width, height)
+    if lib().orc_init_from_mesh(C.byref(_init_view(width, height, K, R, T)), v.ctypes.data, len(v), f.ctypes.data,
+                                len(f), fn.ctypes.data, d.ctypes.data, n.ctypes.data, r.ctypes.data):
+        raise RuntimeError("orc_init_from_mesh failed")
+    return d, n, (r[0], r[1])
+
+
+def init_from_dense_points(width, height, K, R, T, xyz, normals, level=2):
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    nn = np.ascontiguousarray(normals, np.float32).reshape(-1, 3)
+    d, n, r = _init_out(width, height)
+    if lib().orc_init_from_dense_points(C.byref(_init_view(width, height, K, R, T)), x.ctypes.data, nn.ctypes.data,
+                                        len(x), int(level), d.ctypes.data, n.ctypes.data, r.ctypes.data):
+        raise RuntimeError("orc_init_from_dense_points failed")
+    return d, n, (r[0], r[1])

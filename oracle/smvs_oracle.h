@@ -83,6 +83,17 @@ int orc_cross_filter_poses(const smvs_filter_view* views, int num_views, const s
 /* NormalMap::Encode (normal_map.cc:159-181) of a planar 3*W*H map. */
 int orc_encode_normal_map(const float* normal, int width, int height, uint32_t* code);
 
+/* Initial maps from the model (patch_match_controller.cc): InitDepthMap +
+ * InitDepthMapFromSparsePoint (:1205-1307, :483-518), Model2Depth (:520-642),
+ * Ply2Depth (:643-750). `view` gives width, height, K, R, T; depth is W*H,
+ * normal 3*W*H planar; range[2] is the returned depth range. */
+int orc_init_from_sparse_points(const smvs_view* view, const float* xyz, size_t n, float* depth, float* normal,
+                                float* range);
+int orc_init_from_mesh(const smvs_view* view, const double* vertices, size_t num_vertices, const int32_t* faces,
+                       size_t num_faces, const double* face_normals, float* depth, float* normal, float* range);
+int orc_init_from_dense_points(const smvs_view* view, const float* xyz, const float* normals, size_t n, int level,
+                               float* depth, float* normal, float* range);
+
 /* The generator shared with the engine: uniform in (0, 1]. */
 float orc_uniform(uint64_t seed, uint32_t stage, uint32_t pixel, uint32_t draw);
 

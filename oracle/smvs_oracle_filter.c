@@ -9,8 +9,8 @@
  * (src/mvs/kernel_functions.cu:3561-3960) on the CPU, problem by problem in the
  * reference's order. Built with -ffp-contract=off: the same IEEE single-
  * precision operations, in the same order, as the CUDA unit (compiled with
- * -fmad=false, -prec-div=true, -prec-sqrt=true, -ftz=false), so the two agree
- * bit for bit.
+ * -fmad=false, -prec-div=true, -prec-sqrt=true, -ftz=false), with fused
+ * multiply-adds only where both write fmaf, so the two agree bit for bit.
  * Differences from the reference, shared with the CUDA kernels:
  *   - depth and normal maps are read with exact point sampling (texel
  *     floor(x + 0.5)) instead of the texture unit's fixed-point coordinates;
@@ -49,7 +49,7 @@ static uint32_t encode_normal(float n0, float n1, float n2) {
 static void decode_normal(uint32_t code, float n[3]) {
   const uint32_t iq1 = code >> 16, iq2 = code & 0x0000ffffu;
   const float q1 = (float)iq1 / 32767.f - 1, q2 = (float)iq2 / 32767.f - 1;
-  const float s = q1 * q1 + q2 * q2;
+  const float s = fmaf(q1, q1, q2 * q2);
   n[0] = (float)(1.0 - 2.0 * s);
   n[1] = 2 * q1 * sqrtf(1 - s);
   n[2] = 2 * q2 * sqrtf(1 - s);
@@ -93,11 +93,18 @@ static void problem_poses(const smvs_filter_view* views, const smvs_filter_probl
 
 /* Projection into a source view and back (kernel_functions.cu:3627-3673 and
  * :3822-3868, the same expressions in both kernels). */
+/* a . x + t with explicit fused multiply-adds: the one rounding order the CUDA
+ * kernels use too (the reference's fast-math build contracts these sums). */
+static inline float affine3(const float a[3], const float x[3], float t) {
+  return fmaf(a[0], x[0], fmaf(a[1], x[1], fmaf(a[2], x[2], t)));
+}
+static inline float dot3f(const float a[3], const float b[3]) { return fmaf(a[0], b[0], fmaf(a[1], b[1], a[2] * b[2])); }
+
 static inline void project(const float* pose, const float X[3], float* scol, float* srow) {
   const float* P = pose + 19;
-  const float ifz = 1.0f / (P[8] * X[0] + P[9] * X[1] + P[10] * X[2] + P[11]);
-  *scol = ifz * (P[0] * X[0] + P[1] * X[1] + P[2] * X[2] + P[3]);
-  *srow = ifz * (P[4] * X[0] + P[5] * X[1] + P[6] * X[2] + P[7]);
+  const float ifz = 1.0f / affine3(P + 8, X, P[11]);
+  *scol = ifz * affine3(P, X, P[3]);
+  *srow = ifz * affine3(P + 4, X, P[7]);
 }
 
 /* Point sample at (x + 0.5, y + 0.5) with border zero: texel floor(x + 0.5). */
@@ -112,16 +119,15 @@ static inline int texel(float scol, float srow, int w, int h, int* sx, int* sy) 
 static inline float back_project(const float* pose, const float refK[4], float scol, float srow, float sd,
                                  int col, int row, float* err) {
   const float* iP = pose + 31;
-  scol *= sd;
-  srow *= sd;
-  const float bx = iP[0] * scol + iP[1] * srow + iP[2] * sd + iP[3];
-  const float by = iP[4] * scol + iP[5] * srow + iP[6] * sd + iP[7];
-  const float bz = iP[8] * scol + iP[9] * srow + iP[10] * sd + iP[11];
+  const float x[3] = {scol * sd, srow * sd, sd};
+  const float bx = affine3(iP, x, iP[3]);
+  const float by = affine3(iP + 4, x, iP[7]);
+  const float bz = affine3(iP + 8, x, iP[11]);
   const float ibz = 1.0f / bz;
-  const float bcol = ibz * (refK[0] * bx + refK[1] * bz);
-  const float brow = ibz * (refK[2] * by + refK[3] * bz);
+  const float bcol = ibz * fmaf(refK[0], bx, refK[1] * bz);
+  const float brow = ibz * fmaf(refK[2], by, refK[3] * bz);
   const float dc = (float)col - bcol, dr = (float)row - brow;
-  *err = sqrtf(dc * dc + dr * dr);
+  *err = sqrtf(fmaf(dc, dc, dr * dr));
   return bz;
 }
 
@@ -176,11 +182,11 @@ int orc_cross_filter_run(const smvs_options* o, const smvs_filter_view* views, i
         if ((double)depth < 1e-6 || col < 3 || col > W - 3 || row < 3 || row > H - 3) { out[pix] = 0.0f; continue; }
         float rn[3];
         decode_normal(codes[pr->ref][pix], rn);
-        float vr[3] = {refiK[0] * (float)col + refiK[1], refiK[2] * (float)row + refiK[3], 1.0f};
-        const float nvr = sqrtf(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+        float vr[3] = {fmaf(refiK[0], (float)col, refiK[1]), fmaf(refiK[2], (float)row, refiK[3]), 1.0f};
+        const float X[3] = {depth * vr[0], depth * vr[1], depth};
+        const float nvr = sqrtf(dot3f(vr, vr));
         vr[0] /= nvr; vr[1] /= nvr; vr[2] /= nvr;
-        if (rn[0] * vr[0] + rn[1] * vr[1] + rn[2] * vr[2] >= max_view_cos) { out[pix] = 0.0f; continue; }
-        const float X[3] = {depth * (refiK[0] * (float)col + refiK[1]), depth * (refiK[2] * (float)row + refiK[3]), depth};
+        if (dot3f(rn, vr) >= max_view_cos) { out[pix] = 0.0f; continue; }
         float depths[SMVS_CROSS_MAX_SRC + 1];
         int good = 0;
         depths[0] = depth;
@@ -203,11 +209,10 @@ int orc_cross_filter_run(const smvs_options* o, const smvs_filter_view* views, i
           if (err > fmax_err || (depth - bz) * (depth - bz) > depth * depth * thr2) continue;
           float sn[3];
           decode_normal(scode, sn);
-          const float* R = pose + 4;
-          const float r0 = R[0] * sn[0] + R[3] * sn[1] + R[6] * sn[2];
-          const float r1 = R[1] * sn[0] + R[4] * sn[1] + R[7] * sn[2];
-          const float r2 = R[2] * sn[0] + R[5] * sn[1] + R[8] * sn[2];
-          if (rn[0] * r0 + rn[1] * r1 + rn[2] * r2 < max_cos) continue;
+          const float* R = pose + 4;  /* R^T n (kernel_functions.cu:3742-3747) */
+          const float Rc0[3] = {R[0], R[3], R[6]}, Rc1[3] = {R[1], R[4], R[7]}, Rc2[3] = {R[2], R[5], R[8]};
+          const float rs[3] = {dot3f(Rc0, sn), dot3f(Rc1, sn), dot3f(Rc2, sn)};
+          if (dot3f(rn, rs) < max_cos) continue;
           depths[++good] = bz;
         }
         const int nth = (int)(good * 0.5);
@@ -280,7 +285,8 @@ int orc_cross_filter_dedup(const smvs_options* o, const smvs_filter_view* views,
         int good = 0, num_vis = 0;
         int idx[SMVS_CROSS_MAX_SRC + 1];
         float dd[SMVS_CROSS_MAX_SRC + 1];
-        const float X[3] = {depth * (refiK[0] * (float)col + refiK[1]), depth * (refiK[2] * (float)row + refiK[3]), depth};
+        const float X[3] = {depth * fmaf(refiK[0], (float)col, refiK[1]), depth * fmaf(refiK[2], (float)row, refiK[3]),
+                            depth};
         for (int i = 0; i < N; ++i) {
           const float* pose = poses + (size_t)i * SMVS_POSE_FLOATS;
           const int sv_i = pr->src[i];

@@ -163,6 +163,13 @@ _SIGNATURES = {
     "smvs_cross_filter_dedup_levels": (C.c_int, [C.c_void_p]),
     "smvs_cross_filter_synchronize": (C.c_int, [C.c_void_p]),
     "smvs_cross_filter_destroy": (None, [C.c_void_p]),
+    "smvs_cross_filter_release_cache": (C.c_int, [C.c_int]),
+    "smvs_init_depth_from_sparse_points": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_size_t, C.c_int,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_init_depth_from_mesh": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                            C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_init_depth_from_dense_points": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
+                                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_pool_options_default": (C.c_int, [C.POINTER(smvs_pool_options)]),
     "smvs_pool_create": (C.c_int, [C.POINTER(smvs_pool_options), C.c_void_p, C.POINTER(C.c_void_p)]),
     "smvs_pool_add_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(smvs_view), C.c_int]),

@@ -23,9 +23,10 @@ COMMON_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-X
 NVCC_FLAGS = COMMON_FLAGS + ["--use_fast_math"]
 # Units whose kernels must reproduce IEEE single-precision results exactly
 # (no contraction into FMA, correctly rounded division and square root, no
-# flush to zero): the cross-view filter's decisions and medians.
+# flush to zero): the cross-view filter's decisions and medians, and the
+# depth tests of the initial maps.
 EXACT_FLAGS = COMMON_FLAGS + ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-EXACT_UNITS = {"smvs_cross_filter.cu"}
+EXACT_UNITS = {"smvs_cross_filter.cu", "smvs_init_maps.cu"}
 
 
 def _nvcc() -> str:

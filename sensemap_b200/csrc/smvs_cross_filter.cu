@@ -6,28 +6,38 @@
 // the largest view, launches one kernel per problem with a device-wide sync
 // after each, and for deduplication copies every map back to the host and up
 // again. Here:
-//   - every view's depth map, encoded normal map, visibility layer, refined
+//   - every view's depth map, decoded normal map, visibility layer, refined
 //     map and delta map is a dense W*H region of one HBM buffer per kind
 //     (regions start on 128-byte boundaries), read with plain loads;
 //   - normals are encoded on the device (NormalMap::Encode, normal_map.cc:
-//     159-181) from the planar maps, 4 B/px resident instead of 12;
-//   - Run is one launch over all problems: a block decodes its problem from a
-//     prefix sum of per-problem block counts and stages that problem's
-//     parameter block (pose records included) in shared memory;
+//     159-181) and kept as 4-byte codes; the kernel decodes a code only for
+//     the sources that pass the depth tests, with an exact short form of the
+//     reference's decode;
+//   - Run is one launch over all problems. Its blocks are ordered by image
+//     row band first and problem second, so the blocks resident at one time
+//     cover the same band of every reference view and read overlapping parts
+//     of the source maps from L2; a block stages its problem's parameter block
+//     (projection records included) in shared memory, read back with 16-byte
+//     loads;
 //   - DedupRun keeps the reference's sequential problem order only where two
 //     problems touch the same visibility layer: problems are levelled so that
 //     any pair with a write/read, read/write or write/write conflict on a layer
 //     runs in order, and each level is one launch;
-//   - the dedup input of ref_flag views is their refined map in place (no copy).
+//   - the dedup input of ref_flag views is their refined map in place (no copy);
+//   - device memory comes from a per-device stream-ordered pool that keeps
+//     freed blocks for the next filter, and no call waits for the GPU except
+//     the getters (which copy to the host) and set-up from host memory.
 // The unit is compiled without FMA contraction and with IEEE division and
-// square root so that its decisions and medians reproduce the CPU oracle bit
-// for bit; its cost is in loads and the per-pixel sort, not in those operations.
+// square root; the fused multiply-adds it performs are written out (fmaf), in
+// the same places as in the CPU oracle, so the two agree bit for bit.
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstddef>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -41,6 +51,7 @@ namespace {
 
 constexpr uint32_t kVisKeep = 0x80000000u;
 constexpr int kBlockX = 32, kBlockY = 8, kThreads = kBlockX * kBlockY;
+constexpr int kRec = 36;  // per-source record: P (12) | P^-1 (12) | R (9) + 3 pad
 
 int Fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -61,11 +72,11 @@ int Fail(int code, const char* fmt, ...) {
 // One source view of a problem as the kernels see it.
 struct CfSrc {
   const float* depth;   // depth map (run: input map; dedup: the view's dedup input)
-  const uint32_t* aux;  // run: encoded normals; dedup: visibility layer
+  const uint32_t* aux;  // run: normal codes; dedup: visibility layer
   int width, height, ref_flag, pad;
 };
 
-// Parameter block of one problem. Staged into shared memory up to the pose
+// Parameter block of one problem. Staged into shared memory up to the
 // records of its num_src sources.
 struct alignas(16) CfJob {
   int width, height, num_src, min_cons;
@@ -77,9 +88,10 @@ struct alignas(16) CfJob {
   uint32_t* vis;          // dedup: reference visibility layer
   float* out;             // run: refined map; dedup: delta map
   CfSrc src[SMVS_CROSS_MAX_SRC];
-  float pose[SMVS_CROSS_MAX_SRC][SMVS_POSE_FLOATS];
+  alignas(16) float rec[SMVS_CROSS_MAX_SRC][kRec];
 };
 static_assert(sizeof(CfJob) % 16 == 0, "CfJob is staged in 16-byte units");
+static_assert(offsetof(CfJob, rec) % 16 == 0, "records are read with 16-byte loads");
 
 // Thresholds shared by every problem (options of the set).
 struct CfConsts {
@@ -93,40 +105,58 @@ struct CfConsts {
 // ---------------------------------------------------------------------------
 // Device helpers
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ int FindJob(const int* __restrict__ block_start, int num_jobs, int block) {
-  int lo = 0, hi = num_jobs - 1;
-  while (lo < hi) {  // largest j with block_start[j] <= block
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(block_start + mid) <= block) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
-// Copies the job's header, source table and the pose records it uses.
+// Copies the job's header, source table and the records it uses.
 __device__ __forceinline__ void StageJob(CfJob* sj, const CfJob* __restrict__ gj) {
   const int ns = __ldg(&gj->num_src);
-  const int n16 = (int)((offsetof(CfJob, pose) + (size_t)ns * SMVS_POSE_FLOATS * sizeof(float) + 15) / 16);
+  const int n16 = (int)((offsetof(CfJob, rec) + (size_t)ns * kRec * sizeof(float) + 15) / 16);
   const int4* g = reinterpret_cast<const int4*>(gj);
   int4* s = reinterpret_cast<int4*>(sj);
   for (int i = threadIdx.x; i < n16; i += kThreads) s[i] = __ldg(g + i);
 }
 
-// The in-kernel normal decode (kernel_functions.cu:3592-3601, decode_factor 32767).
-__device__ __forceinline__ void DecodeNormal(uint32_t code, float n[3]) {
-  const uint32_t iq1 = code >> 16, iq2 = code & 0x0000ffffu;
-  const float q1 = (float)iq1 / 32767.f - 1, q2 = (float)iq2 / 32767.f - 1;
-  const float s = q1 * q1 + q2 * q2;
-  n[0] = (float)(1.0 - 2.0 * s);
-  n[1] = 2 * q1 * sqrtf(1 - s);
-  n[2] = 2 * q2 * sqrtf(1 - s);
+// a . x + t and a . b with explicit fused multiply-adds (the oracle's order).
+__device__ __forceinline__ float Affine3(float a0, float a1, float a2, const float x[3], float t) {
+  return fmaf(a0, x[0], fmaf(a1, x[1], fmaf(a2, x[2], t)));
+}
+__device__ __forceinline__ float Dot3(const float a[3], const float b[3]) {
+  return fmaf(a[0], b[0], fmaf(a[1], b[1], a[2] * b[2]));
+}
+
+// NormalMap::Encode (normal_map.cc:159-181).
+__device__ __forceinline__ uint32_t Encode(float n0, float n1, float n2) {
+  const float s0 = (float)((1 - n0) * 0.5);
+  const float m = 1.0f / sqrtf(1 - s0);
+  float q1 = (float)(n1 * 0.5 * m), q2 = (float)(n2 * 0.5 * m);
+  // std::min(0.999999f, std::max(q, -0.999999f)): a NaN clamps to +0.999999.
+  q1 = q1 < -0.999999f ? -0.999999f : q1;
+  q1 = q1 < 0.999999f ? q1 : 0.999999f;
+  q2 = q2 < -0.999999f ? -0.999999f : q2;
+  q2 = q2 < 0.999999f ? q2 : 0.999999f;
+  const uint32_t iq1 = (uint32_t)((q1 + 1) * 32767.f), iq2 = (uint32_t)((q2 + 1) * 32767.f);
+  return (iq1 << 16) | iq2;
+}
+
+// The kernel's decode (kernel_functions.cu:3592-3601, decode_factor 32767) in
+// an exact short form: for every 16-bit iq, (float)((double)iq * (1/32767))
+// equals the IEEE quotient (float)iq / 32767.f, and 1 - 2s rounded once in
+// float equals (float)(1.0 - 2.0 * s), the double difference being exact.
+__device__ __forceinline__ void Decode(uint32_t code, float n[3]) {
+  const double kInv = 1.0 / 32767.0;
+  const float q1 = (float)((double)(code >> 16) * kInv) - 1.0f;
+  const float q2 = (float)((double)(code & 0x0000ffffu) * kInv) - 1.0f;
+  const float s = fmaf(q1, q1, q2 * q2);
+  const float root = sqrtf(1 - s);
+  n[0] = 1.0f - 2.0f * s;
+  n[1] = 2 * q1 * root;
+  n[2] = 2 * q2 * root;
 }
 
 // Forward projection into a source view (kernel_functions.cu:3630-3640).
-__device__ __forceinline__ void Project(const float* pose, const float X[3], float* scol, float* srow) {
-  const float* P = pose + 19;
-  const float ifz = 1.0f / (P[8] * X[0] + P[9] * X[1] + P[10] * X[2] + P[11]);
-  *scol = ifz * (P[0] * X[0] + P[1] * X[1] + P[2] * X[2] + P[3]);
-  *srow = ifz * (P[4] * X[0] + P[5] * X[1] + P[6] * X[2] + P[7]);
+__device__ __forceinline__ void Project(const float4* rec, const float X[3], float* scol, float* srow) {
+  const float4 p0 = rec[0], p1 = rec[1], p2 = rec[2];  // P rows
+  const float ifz = 1.0f / Affine3(p2.x, p2.y, p2.z, X, p2.w);
+  *scol = ifz * Affine3(p0.x, p0.y, p0.z, X, p0.w);
+  *srow = ifz * Affine3(p1.x, p1.y, p1.z, X, p1.w);
 }
 
 // Point sample at (x + 0.5, y + 0.5), border zero: texel floor(x + 0.5).
@@ -138,19 +168,18 @@ __device__ __forceinline__ bool Texel(float scol, float srow, int w, int h, int*
 }
 
 // Back-projection into the reference view (kernel_functions.cu:3650-3673).
-__device__ __forceinline__ float BackProject(const float* pose, const float refK[4], float scol, float srow,
-                                             float sd, int col, int row, float* err) {
-  const float* iP = pose + 31;
-  scol *= sd;
-  srow *= sd;
-  const float bx = iP[0] * scol + iP[1] * srow + iP[2] * sd + iP[3];
-  const float by = iP[4] * scol + iP[5] * srow + iP[6] * sd + iP[7];
-  const float bz = iP[8] * scol + iP[9] * srow + iP[10] * sd + iP[11];
+__device__ __forceinline__ float BackProject(const float4* rec, const float refK[4], float scol, float srow, float sd,
+                                             int col, int row, float* err) {
+  const float4 q0 = rec[3], q1 = rec[4], q2 = rec[5];  // P^-1 rows
+  const float x[3] = {scol * sd, srow * sd, sd};
+  const float bx = Affine3(q0.x, q0.y, q0.z, x, q0.w);
+  const float by = Affine3(q1.x, q1.y, q1.z, x, q1.w);
+  const float bz = Affine3(q2.x, q2.y, q2.z, x, q2.w);
   const float ibz = 1.0f / bz;
-  const float bcol = ibz * (refK[0] * bx + refK[1] * bz);
-  const float brow = ibz * (refK[2] * by + refK[3] * bz);
+  const float bcol = ibz * fmaf(refK[0], bx, refK[1] * bz);
+  const float brow = ibz * fmaf(refK[2], by, refK[3] * bz);
   const float dc = (float)col - bcol, dr = (float)row - brow;
-  *err = sqrtf(dc * dc + dr * dr);
+  *err = sqrtf(fmaf(dc, dc, dr * dr));
   return bz;
 }
 
@@ -173,21 +202,10 @@ __device__ __forceinline__ bool PixelOf(const CfJob& j, int local, int* col, int
 // ---------------------------------------------------------------------------
 // Kernels
 // ---------------------------------------------------------------------------
-// NormalMap::Encode (normal_map.cc:159-181) of a planar 3*W*H map.
-__global__ void EncodeNormalsKernel(const float* __restrict__ n, size_t wh, uint32_t* __restrict__ code) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < wh; i += (size_t)gridDim.x * blockDim.x) {
-    const float n0 = n[i], n1 = n[wh + i], n2 = n[2 * wh + i];
-    const float s = (float)((1 - n0) * 0.5);
-    const float m = 1.0f / sqrtf(1 - s);
-    float q1 = (float)(n1 * 0.5 * m), q2 = (float)(n2 * 0.5 * m);
-    // std::min(0.999999f, std::max(q, -0.999999f)): a NaN clamps to +0.999999.
-    q1 = q1 < -0.999999f ? -0.999999f : q1;
-    q1 = q1 < 0.999999f ? q1 : 0.999999f;
-    q2 = q2 < -0.999999f ? -0.999999f : q2;
-    q2 = q2 < 0.999999f ? q2 : 0.999999f;
-    const uint32_t iq1 = (uint32_t)((q1 + 1) * 32767.f), iq2 = (uint32_t)((q2 + 1) * 32767.f);
-    code[i] = (iq1 << 16) | iq2;
-  }
+// Planar 3*W*H normals -> codes.
+__global__ void EncodeKernel(const float* __restrict__ n, size_t wh, uint32_t* __restrict__ out) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < wh; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = Encode(n[i], n[wh + i], n[2 * wh + i]);
 }
 
 __global__ void FillU32Kernel(uint32_t* __restrict__ p, size_t n, uint32_t v) {
@@ -196,52 +214,47 @@ __global__ void FillU32Kernel(uint32_t* __restrict__ p, size_t n, uint32_t v) {
 
 // CrossFilterKernel (kernel_functions.cu:3561-3778) for every problem at once.
 __global__ void __launch_bounds__(kThreads) CrossFilterRunKernel(const CfJob* __restrict__ jobs,
-                                                                 const int* __restrict__ block_start,
-                                                                 int num_jobs, CfConsts c) {
+                                                                 const int2* __restrict__ blocks, CfConsts c) {
   __shared__ CfJob sj;
-  const int jid = FindJob(block_start, num_jobs, (int)blockIdx.x);
-  StageJob(&sj, jobs + jid);
+  const int2 blk = __ldg(blocks + blockIdx.x);  // (problem, tile)
+  StageJob(&sj, jobs + blk.x);
   __syncthreads();
   int col, row;
-  if (!PixelOf(sj, (int)blockIdx.x - __ldg(block_start + jid), &col, &row)) return;
+  if (!PixelOf(sj, blk.y, &col, &row)) return;
   const int W = sj.width, H = sj.height;
   const size_t pix = (size_t)row * W + col;
   const float depth = sj.depth[pix];
   if ((double)depth < 1e-6 || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.out[pix] = 0.0f; return; }
   float rn[3];
-  DecodeNormal(sj.code[pix], rn);
-  float vr[3] = {sj.refiK[0] * (float)col + sj.refiK[1], sj.refiK[2] * (float)row + sj.refiK[3], 1.0f};
-  const float nvr = sqrtf(vr[0] * vr[0] + vr[1] * vr[1] + vr[2] * vr[2]);
+  Decode(__ldg(sj.code + pix), rn);
+  float vr[3] = {fmaf(sj.refiK[0], (float)col, sj.refiK[1]), fmaf(sj.refiK[2], (float)row, sj.refiK[3]), 1.0f};
+  const float X[3] = {depth * vr[0], depth * vr[1], depth};
+  const float nvr = sqrtf(Dot3(vr, vr));
   vr[0] /= nvr; vr[1] /= nvr; vr[2] /= nvr;
-  if (rn[0] * vr[0] + rn[1] * vr[1] + rn[2] * vr[2] >= c.max_view_cos) { sj.out[pix] = 0.0f; return; }
-  const float X[3] = {depth * (sj.refiK[0] * (float)col + sj.refiK[1]),
-                      depth * (sj.refiK[2] * (float)row + sj.refiK[3]), depth};
+  if (Dot3(rn, vr) >= c.max_view_cos) { sj.out[pix] = 0.0f; return; }
   float depths[SMVS_CROSS_MAX_SRC + 1];
   int good = 0;
   depths[0] = depth;
   for (int i = 0; i < sj.num_src; ++i) {
-    const float* pose = sj.pose[i];
+    const float4* rec = reinterpret_cast<const float4*>(sj.rec[i]);
     const CfSrc& s = sj.src[i];
     float scol, srow;
-    Project(pose, X, &scol, &srow);
+    Project(rec, X, &scol, &srow);
     int q;
-    float sd = 0.0f;
-    uint32_t scode = 0;
-    if (Texel(scol, srow, s.width, s.height, &q)) {
-      sd = __ldg(s.depth + q);
-      scode = __ldg(s.aux + q);
-    }
+    if (!Texel(scol, srow, s.width, s.height, &q)) continue;  // border: depth 0 < 1e-4
+    const float sd = __ldg(s.depth + q);
     if ((double)sd < 1e-4) continue;
     float err;
-    const float bz = BackProject(pose, sj.refK, scol, srow, sd, col, row, &err);
-    if (err > c.fmax_err || (depth - bz) * (depth - bz) > depth * depth * c.thr2) continue;
+    const float bz = BackProject(rec, sj.refK, scol, srow, sd, col, row, &err);
+    const float dd = depth - bz;
+    if (err > c.fmax_err || dd * dd > depth * depth * c.thr2) continue;
     float sn[3];
-    DecodeNormal(scode, sn);
-    const float* R = pose + 4;
-    const float r0 = R[0] * sn[0] + R[3] * sn[1] + R[6] * sn[2];
-    const float r1 = R[1] * sn[0] + R[4] * sn[1] + R[7] * sn[2];
-    const float r2 = R[2] * sn[0] + R[5] * sn[1] + R[8] * sn[2];
-    if (rn[0] * r0 + rn[1] * r1 + rn[2] * r2 < c.max_cos) continue;
+    Decode(__ldg(s.aux + q), sn);
+    const float4 r0 = rec[6], r1 = rec[7], r2 = rec[8];  // R row-major, then padding
+    // R^T n (kernel_functions.cu:3742-3747)
+    const float Rc0[3] = {r0.x, r0.w, r1.z}, Rc1[3] = {r0.y, r1.x, r1.w}, Rc2[3] = {r0.z, r1.y, r2.x};
+    const float rs[3] = {Dot3(Rc0, sn), Dot3(Rc1, sn), Dot3(Rc2, sn)};
+    if (Dot3(rn, rs) < c.max_cos) continue;
     depths[++good] = bz;
   }
   const int nth = (int)(good * 0.5);
@@ -255,37 +268,37 @@ __global__ void __launch_bounds__(kThreads) CrossFilterRunKernel(const CfJob* __
 
 // DeduplicFilterKernel (kernel_functions.cu:3780-3916) for the problems of one level.
 __global__ void __launch_bounds__(kThreads) DedupKernel(const CfJob* __restrict__ jobs,
-                                                        const int* __restrict__ block_start, int num_jobs,
-                                                        CfConsts c) {
+                                                        const int2* __restrict__ blocks, CfConsts c) {
   __shared__ CfJob sj;
-  const int jid = FindJob(block_start, num_jobs, (int)blockIdx.x);
-  StageJob(&sj, jobs + jid);
+  const int2 blk = __ldg(blocks + blockIdx.x);  // (problem, tile)
+  StageJob(&sj, jobs + blk.x);
   __syncthreads();
   int col, row;
-  if (!PixelOf(sj, (int)blockIdx.x - __ldg(block_start + jid), &col, &row)) return;
+  if (!PixelOf(sj, blk.y, &col, &row)) return;
   const int W = sj.width, H = sj.height;
   const size_t pix = (size_t)row * W + col;
   const float depth = sj.depth[pix];
   if ((double)depth < 1e-6 || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.vis[pix] = 0u; return; }
   const uint32_t vis0 = sj.vis[pix];
   if (!(vis0 >> 3)) { sj.vis[pix] = 0u; return; }  // [quirk] :3803 shifts by sizeof(uint32_t) - 1
-  const float X[3] = {depth * (sj.refiK[0] * (float)col + sj.refiK[1]),
-                      depth * (sj.refiK[2] * (float)row + sj.refiK[3]), depth};
+  const float X[3] = {depth * fmaf(sj.refiK[0], (float)col, sj.refiK[1]),
+                      depth * fmaf(sj.refiK[2], (float)row, sj.refiK[3]), depth};
   float dd[SMVS_CROSS_MAX_SRC];
   int good = 0, num_vis = 0;
   uint32_t bits = vis0;
   for (int i = 0; i < sj.num_src; ++i) {
-    const float* pose = sj.pose[i];
+    const float4* rec = reinterpret_cast<const float4*>(sj.rec[i]);
     const CfSrc& s = sj.src[i];
     float scol, srow;
-    Project(pose, X, &scol, &srow);
-    int q = 0;
-    float sd = 0.0f;
-    if (Texel(scol, srow, s.width, s.height, &q)) sd = __ldg(s.depth + q);
+    Project(rec, X, &scol, &srow);
+    int q;
+    if (!Texel(scol, srow, s.width, s.height, &q)) continue;  // border: depth 0
+    const float sd = __ldg(s.depth + q);
     if (sd == 0.0f) continue;
     float err;
-    const float bz = BackProject(pose, sj.refK, scol, srow, sd, col, row, &err);
-    if (err > c.fmax_err || (depth - bz) * (depth - bz) > depth * depth * c.thr2) continue;
+    const float bz = BackProject(rec, sj.refK, scol, srow, sd, col, row, &err);
+    const float d = depth - bz;
+    if (err > c.fmax_err || d * d > depth * depth * c.thr2) continue;
     dd[good++] = fabsf(bz - depth);
     bits |= 1u << (SMVS_CROSS_MAX_SRC - 1 - i);
     // Another problem's writes to this layer finished in an earlier launch.
@@ -302,12 +315,33 @@ __global__ void __launch_bounds__(kThreads) DedupKernel(const CfJob* __restrict_
 __global__ void DedupDepthKernel(const float* __restrict__ depth, const uint32_t* __restrict__ vis, size_t wh,
                                  float* __restrict__ out) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < wh; i += (size_t)gridDim.x * blockDim.x)
-    out[i] = (depth && (vis[i] & kVisKeep)) ? depth[i] : 0.0f;
+    out[i] = (vis[i] & kVisKeep) ? depth[i] : 0.0f;
 }
 
 int GridFor(size_t n) {
   const size_t b = (n + 255) / 256;
-  return (int)std::min<size_t>(b, 148 * 16);
+  return (int)std::max<size_t>(1, std::min<size_t>(b, 148 * 16));
+}
+
+// Stream-ordered pool per device; freed blocks stay cached for the next filter
+// (smvs_cross_filter_release_cache returns them).
+cudaMemPool_t DevicePool(int device) {
+  static std::mutex mu;
+  static std::map<int, cudaMemPool_t> pools;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = pools.find(device);
+  if (it != pools.end()) return it->second;
+  cudaMemPoolProps props;
+  memset(&props, 0, sizeof(props));
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) return nullptr;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  pools[device] = pool;
+  return pool;
 }
 
 }  // namespace
@@ -319,30 +353,29 @@ struct smvs_cross_filter {
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  cudaMemPool_t pool = nullptr;
   smvs_options opt;
   std::vector<smvs_filter_view> views;  // host copy of the metadata (map pointers cleared)
-  std::vector<int> ref_of_view;         // problem index whose reference is the view, or -1
   std::vector<std::vector<int>> srcs;   // per problem
   std::vector<int> refs;                // per problem
   std::vector<size_t> off;              // element offset of each view's region
   size_t total = 0;
-  bool has_normals = false;
   float* d_depth = nullptr;
   uint32_t* d_code = nullptr;
   float* d_refined = nullptr;
   float* d_delta = nullptr;
   uint32_t* d_vis = nullptr;
-  float* d_scratch = nullptr;  // largest view, for dedup depth maps
+  float* d_scratch = nullptr;  // 3 x largest view: host normal staging, dedup depth maps
   CfJob* d_jobs = nullptr;
-  int* d_block_start = nullptr;
-  size_t job_capacity = 0, prefix_capacity = 0;
-  std::vector<uint8_t> has_normal;      // per view
+  int2* d_blocks = nullptr;
+  size_t job_capacity = 0, block_capacity = 0;
+  std::vector<uint8_t> has_normal;          // per view
   std::vector<uint8_t> refined, dedup_ref;  // per view
-  bool ran = false, deduped = false;
+  bool deduped = false;
   int dedup_levels = 0;
   int64_t launches = 0;
-  std::vector<CfJob> h_jobs;  // kept alive until the stream drains
-  std::vector<int> h_block_start;
+  std::vector<CfJob> h_jobs;
+  std::vector<int2> h_blocks;
   // Profiling: (kind, start, stop) per timed launch, harvested on demand.
   bool profiling = false;
   struct Timed { int kind; cudaEvent_t a, b; };
@@ -383,17 +416,39 @@ void Harvest(smvs_cross_filter* f) {
   f->timed.clear();
 }
 
+template <typename T>
+int PoolAlloc(smvs_cross_filter* f, T** p, size_t bytes) {
+  cudaError_t err = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), std::max<size_t>(bytes, 16), f->pool,
+                                            f->stream);
+  if (err != cudaSuccess) {
+    *p = nullptr;
+    return Fail(SMVS_ENOMEM, "cross filter: device allocation of %zu bytes: %s", bytes, cudaGetErrorString(err));
+  }
+  return SMVS_OK;
+}
+
+template <typename T>
+void PoolFree(smvs_cross_filter* f, T*& p) {
+  if (p) cudaFreeAsync(p, f->stream);
+  p = nullptr;
+}
+
 void FreeAll(smvs_cross_filter* f) {
   Harvest(f);
-  cudaFree(f->d_depth);
-  cudaFree(f->d_code);
-  cudaFree(f->d_refined);
-  cudaFree(f->d_delta);
-  cudaFree(f->d_vis);
-  cudaFree(f->d_scratch);
-  cudaFree(f->d_jobs);
-  cudaFree(f->d_block_start);
-  if (f->own_stream && f->stream) cudaStreamDestroy(f->stream);
+  if (f->pool) {
+    PoolFree(f, f->d_depth);
+    PoolFree(f, f->d_code);
+    PoolFree(f, f->d_refined);
+    PoolFree(f, f->d_delta);
+    PoolFree(f, f->d_vis);
+    PoolFree(f, f->d_scratch);
+    PoolFree(f, f->d_jobs);
+    PoolFree(f, f->d_blocks);
+  }
+  if (f->own_stream && f->stream) {
+    cudaStreamSynchronize(f->stream);
+    cudaStreamDestroy(f->stream);
+  }
 }
 
 CfConsts MakeConsts(const smvs_options& o) {
@@ -409,7 +464,8 @@ CfConsts MakeConsts(const smvs_options& o) {
 }
 
 // InitTransforms (:1320-1407) for one problem: the reference K, its inverse
-// and the source pose records (no source scaling in the cross filter).
+// and the sources' P, P^-1 and R from the 43-float pose records (no source
+// scaling in the cross filter).
 void FillJob(const smvs_cross_filter* f, int p, CfJob* j) {
   memset(j, 0, sizeof(*j));
   const smvs_filter_view& rv = f->views[f->refs[p]];
@@ -430,67 +486,72 @@ void FillJob(const smvs_cross_filter* f, int p, CfJob* j) {
     const smvs_filter_view& sv = f->views[f->srcs[p][i]];
     memcpy(src.K, sv.K, sizeof(src.K)); memcpy(src.R, sv.R, sizeof(src.R)); memcpy(src.T, sv.T, sizeof(src.T));
     src.scale = 1.0f;
-    smvs_internal_pose_record(&ref, &src, j->pose[i]);
+    float pose[SMVS_POSE_FLOATS];
+    smvs_internal_pose_record(&ref, &src, pose);
+    memcpy(j->rec[i], pose + 19, 12 * sizeof(float));       // P
+    memcpy(j->rec[i] + 12, pose + 31, 12 * sizeof(float));  // P^-1
+    memcpy(j->rec[i] + 24, pose + 4, 9 * sizeof(float));    // R
     j->src[i].width = sv.width;
     j->src[i].height = sv.height;
     j->src[i].ref_flag = sv.ref_flag ? 1 : 0;
   }
 }
 
-int Blocks(const CfJob& j) { return j.blocks_x * ((j.height + kBlockY - 1) / kBlockY); }
-
-int EnsureJobs(smvs_cross_filter* f, size_t jobs, size_t prefix) {
-  if (jobs <= f->job_capacity && prefix <= f->prefix_capacity) return SMVS_OK;
-  CF_CUDA(cudaStreamSynchronize(f->stream));
-  cudaFree(f->d_jobs);
-  cudaFree(f->d_block_start);
-  f->d_jobs = nullptr;
-  f->d_block_start = nullptr;
-  f->job_capacity = f->prefix_capacity = 0;
-  CF_CUDA(cudaMalloc(&f->d_jobs, std::max<size_t>(jobs, 1) * sizeof(CfJob)));
-  CF_CUDA(cudaMalloc(&f->d_block_start, std::max<size_t>(prefix, 1) * sizeof(int)));
+int EnsureJobs(smvs_cross_filter* f, size_t jobs, size_t blocks) {
+  if (jobs <= f->job_capacity && blocks <= f->block_capacity) return SMVS_OK;
+  PoolFree(f, f->d_jobs);  // stream-ordered: earlier launches still read the old arrays
+  PoolFree(f, f->d_blocks);
+  f->job_capacity = f->block_capacity = 0;
+  int st = PoolAlloc(f, &f->d_jobs, std::max<size_t>(jobs, 1) * sizeof(CfJob));
+  if (!st) st = PoolAlloc(f, &f->d_blocks, std::max<size_t>(blocks, 1) * sizeof(int2));
+  if (st) return st;
   f->job_capacity = jobs;
-  f->prefix_capacity = prefix;
+  f->block_capacity = blocks;
   return SMVS_OK;
 }
 
 // Uploads f->h_jobs once and launches `kernel` once per segment, segment k
-// being jobs [bounds[k], bounds[k + 1]), in stream order. Each segment gets its
-// own block prefix (n + 1 entries) in one device array.
+// being jobs [bounds[k], bounds[k + 1]), in stream order. A segment's blocks
+// are listed (problem, tile) in row-band-major order: band 0 of every problem,
+// then band 1, and so on. The host arrays may be rebuilt as soon as this
+// returns: copies from pageable memory are staged before cudaMemcpyAsync
+// returns.
 template <typename Kernel>
 int LaunchSegments(smvs_cross_filter* f, const std::vector<size_t>& bounds, Kernel kernel, int kind,
                    const CfConsts& c) {
   const size_t nseg = bounds.size() - 1, njobs = f->h_jobs.size();
-  f->h_block_start.clear();
-  std::vector<long long> totals(nseg, 0);
+  f->h_blocks.clear();
+  std::vector<size_t> seg_start(nseg + 1, 0);
   for (size_t k = 0; k < nseg; ++k) {
-    long long total = 0;
-    for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) {
-      f->h_block_start.push_back((int)total);
-      total += Blocks(f->h_jobs[i]);
-      if (total > 0x7fffffffLL) return Fail(SMVS_EINVAL, "cross filter: too many pixel blocks in one launch");
-    }
-    f->h_block_start.push_back((int)total);
-    totals[k] = total;
+    seg_start[k] = f->h_blocks.size();
+    int bands = 0;
+    for (size_t i = bounds[k]; i < bounds[k + 1]; ++i)
+      bands = std::max(bands, (f->h_jobs[i].height + kBlockY - 1) / kBlockY);
+    for (int by = 0; by < bands; ++by)
+      for (size_t i = bounds[k]; i < bounds[k + 1]; ++i) {
+        const CfJob& j = f->h_jobs[i];
+        if (by >= (j.height + kBlockY - 1) / kBlockY) continue;
+        for (int bx = 0; bx < j.blocks_x; ++bx) f->h_blocks.push_back(make_int2((int)(i - bounds[k]), by * j.blocks_x + bx));
+      }
+    if (f->h_blocks.size() - seg_start[k] > 0x7fffffffu)
+      return Fail(SMVS_EINVAL, "cross filter: too many pixel blocks in one launch");
   }
-  int st = EnsureJobs(f, njobs, f->h_block_start.size());
-  if (st) return st;
+  seg_start[nseg] = f->h_blocks.size();
   if (njobs == 0) return SMVS_OK;
+  int st = EnsureJobs(f, njobs, f->h_blocks.size());
+  if (st) return st;
   CF_CUDA(cudaMemcpyAsync(f->d_jobs, f->h_jobs.data(), njobs * sizeof(CfJob), cudaMemcpyHostToDevice, f->stream));
-  CF_CUDA(cudaMemcpyAsync(f->d_block_start, f->h_block_start.data(), f->h_block_start.size() * sizeof(int),
-                          cudaMemcpyHostToDevice, f->stream));
+  CF_CUDA(cudaMemcpyAsync(f->d_blocks, f->h_blocks.data(), f->h_blocks.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                          f->stream));
   (void)cudaGetLastError();
   for (size_t k = 0; k < nseg; ++k) {
-    if (totals[k] == 0) continue;
-    // Segment k's prefix starts after the k terminal entries of earlier segments.
+    const size_t nb = seg_start[k + 1] - seg_start[k];
+    if (nb == 0) continue;
     ProfScope prof(f, kind);
-    kernel<<<(unsigned)totals[k], kThreads, 0, f->stream>>>(f->d_jobs + bounds[k], f->d_block_start + bounds[k] + k,
-                                                             (int)(bounds[k + 1] - bounds[k]), c);
+    kernel<<<(unsigned)nb, kThreads, 0, f->stream>>>(f->d_jobs + bounds[k], f->d_blocks + seg_start[k], c);
     CF_CUDA(cudaGetLastError());
     ++f->launches;
   }
-  // The host job arrays are rebuilt by the next call: let the copies finish.
-  CF_CUDA(cudaStreamSynchronize(f->stream));
   return SMVS_OK;
 }
 
@@ -506,7 +567,19 @@ int CheckView(const smvs_cross_filter* f, int view) {
   return SMVS_OK;
 }
 
+// The zero-filled refined buffer (allocated on first use).
+int EnsureRefined(smvs_cross_filter* f) {
+  if (f->d_refined) return SMVS_OK;
+  int st = PoolAlloc(f, &f->d_refined, f->total * 4);
+  if (st) return st;
+  CF_CUDA(cudaMemsetAsync(f->d_refined, 0, f->total * 4, f->stream));
+  return SMVS_OK;
+}
+
 }  // namespace
+
+// The pool above, for the other units that allocate per call.
+cudaMemPool_t smvs_internal_device_pool(int device) { return DevicePool(device); }
 
 extern "C" {
 
@@ -523,7 +596,8 @@ int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* vi
   bool any_normal = false;
   for (int v = 0; v < num_views; ++v) {
     const smvs_filter_view& fv = views[v];
-    if (fv.width < 1 || fv.height < 1 || fv.width > 65536 || fv.height > 65536)
+    // Pixel indices are 32-bit inside the kernels.
+    if (fv.width < 1 || fv.height < 1 || (size_t)fv.width * fv.height >= ((size_t)1 << 31))
       return Fail(SMVS_EINVAL, "cross filter: view %d has bad size %dx%d", v, fv.width, fv.height);
     if (!fv.depth) return Fail(SMVS_EINVAL, "cross filter: view %d has no depth map", v);
     any_normal |= fv.normal != nullptr;
@@ -544,9 +618,7 @@ int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* vi
   }
   auto* f = new smvs_cross_filter();
   f->opt = *opt;
-  f->ref_of_view = ref_of;
   f->views.assign(views, views + num_views);
-  f->has_normals = any_normal;
   f->has_normal.resize(num_views);
   for (int v = 0; v < num_views; ++v) f->has_normal[v] = views[v].normal != nullptr;
   for (int p = 0; p < num_problems; ++p) {
@@ -576,19 +648,12 @@ int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* vi
     if (err != cudaSuccess) return fail(Fail(SMVS_ECUDA, "cudaStreamCreate: %s", cudaGetErrorString(err)));
     f->own_stream = true;
   }
-  const size_t bytes = f->total * 4;
-  auto alloc = [&](void** p) -> int {
-    cudaError_t err = cudaMalloc(p, bytes);
-    if (err != cudaSuccess) return Fail(SMVS_ENOMEM, "cross filter: cudaMalloc(%zu): %s", bytes, cudaGetErrorString(err));
-    return SMVS_OK;
-  };
+  f->pool = DevicePool(f->device);
+  if (!f->pool) return fail(Fail(SMVS_ECUDA, "cross filter: no memory pool on device %d", f->device));
   int st;
-  if ((st = alloc((void**)&f->d_depth))) return fail(st);
-  if (any_normal && (st = alloc((void**)&f->d_code))) return fail(st);
-  {
-    cudaError_t err = cudaMalloc(&f->d_scratch, std::max<size_t>(max_wh, 1) * 3 * sizeof(float));
-    if (err != cudaSuccess) return fail(Fail(SMVS_ENOMEM, "cross filter: scratch: %s", cudaGetErrorString(err)));
-  }
+  if ((st = PoolAlloc(f, &f->d_depth, f->total * 4))) return fail(st);
+  if (any_normal && (st = PoolAlloc(f, &f->d_code, f->total * sizeof(uint32_t)))) return fail(st);
+  if ((st = PoolAlloc(f, &f->d_scratch, max_wh * 3 * sizeof(float)))) return fail(st);
   // InitDepthMaps / InitNormalMaps (:1139-1258): one dense region per view.
   const cudaMemcpyKind kind = memory == SMVS_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   for (int v = 0; v < num_views; ++v) {
@@ -604,15 +669,17 @@ int smvs_cross_filter_create(const smvs_options* opt, const smvs_filter_view* vi
         n = f->d_scratch;
       }
       (void)cudaGetLastError();
-      EncodeNormalsKernel<<<GridFor(wh), 256, 0, f->stream>>>(n, wh, f->d_code + f->off[v]);
+      EncodeKernel<<<GridFor(wh), 256, 0, f->stream>>>(n, wh, f->d_code + f->off[v]);
       err = cudaGetLastError();
-      if (err != cudaSuccess) return fail(Fail(SMVS_ECUDA, "cross filter: encode: %s", cudaGetErrorString(err)));
+      if (err != cudaSuccess) return fail(Fail(SMVS_ECUDA, "cross filter: normals: %s", cudaGetErrorString(err)));
       ++f->launches;
     }
     f->views[v].depth = nullptr;
     f->views[v].normal = nullptr;
   }
-  {
+  if (memory == SMVS_MEM_HOST) {
+    // Host maps may be pinned (copied asynchronously): they are free to reuse
+    // once this call returns, as with the reference's synchronous upload.
     cudaError_t err = cudaStreamSynchronize(f->stream);
     if (err != cudaSuccess) return fail(Fail(SMVS_ECUDA, "cross filter: upload: %s", cudaGetErrorString(err)));
   }
@@ -630,10 +697,8 @@ int smvs_cross_filter_run(smvs_cross_filter* f) {
     for (int s : f->srcs[p])
       if (!f->has_normal[s]) return Fail(SMVS_EINVAL, "cross filter: view %d has no normal map", s);
   }
-  if (!f->d_refined) {
-    CF_CUDA(cudaMalloc(&f->d_refined, f->total * 4));
-    CF_CUDA(cudaMemsetAsync(f->d_refined, 0, f->total * 4, f->stream));
-  }
+  int st = EnsureRefined(f);
+  if (st) return st;
   f->h_jobs.clear();
   for (int p = 0; p < np; ++p) {
     if (f->srcs[p].empty()) continue;  // :1504-1506
@@ -650,11 +715,10 @@ int smvs_cross_filter_run(smvs_cross_filter* f) {
     }
     f->h_jobs.push_back(j);
   }
-  int st = LaunchSegments(f, {0, f->h_jobs.size()}, CrossFilterRunKernel, SMVS_CF_KERNEL_RUN, MakeConsts(f->opt));
+  st = LaunchSegments(f, {0, f->h_jobs.size()}, CrossFilterRunKernel, SMVS_CF_KERNEL_RUN, MakeConsts(f->opt));
   if (st) return st;
   for (int p = 0; p < np; ++p)
     if (!f->srcs[p].empty()) f->refined[f->refs[p]] = 1;
-  f->ran = true;
   return SMVS_OK;
 }
 
@@ -664,14 +728,12 @@ int smvs_cross_filter_dedup_run(smvs_cross_filter* f) {
     return Fail(SMVS_EINVAL, "dedup needs filter_min_num_consistent >= 1 (the reference reads an unset entry otherwise)");
   cudaSetDevice(f->device);
   const int nv = (int)f->views.size(), np = (int)f->refs.size();
-  if (!f->d_vis) CF_CUDA(cudaMalloc(&f->d_vis, f->total * 4));
-  if (!f->d_delta) CF_CUDA(cudaMalloc(&f->d_delta, f->total * 4));
+  int st;
+  if (!f->d_vis && (st = PoolAlloc(f, &f->d_vis, f->total * 4))) return st;
+  if (!f->d_delta && (st = PoolAlloc(f, &f->d_delta, f->total * 4))) return st;
   bool any_flag = false;
   for (int v = 0; v < nv; ++v) any_flag |= f->views[v].ref_flag != 0;
-  if (any_flag && !f->d_refined) {
-    CF_CUDA(cudaMalloc(&f->d_refined, f->total * 4));
-    CF_CUDA(cudaMemsetAsync(f->d_refined, 0, f->total * 4, f->stream));
-  }
+  if (any_flag && (st = EnsureRefined(f))) return st;
   // ResetDepthMaps (:1260-1318): ref_flag views read their refined map; one
   // that no problem refined reads zeros (its region was zero-filled).
   auto input = [&](int v) -> const float* {
@@ -720,14 +782,13 @@ int smvs_cross_filter_dedup_run(smvs_cross_filter* f) {
     bounds.push_back(f->h_jobs.size());
   }
   // One launch per level on one stream: level lv sees every write of level lv - 1.
-  int st = LaunchSegments(f, bounds, DedupKernel, SMVS_CF_KERNEL_DEDUP, MakeConsts(f->opt));
+  st = LaunchSegments(f, bounds, DedupKernel, SMVS_CF_KERNEL_DEDUP, MakeConsts(f->opt));
   if (st) return st;
   std::fill(f->dedup_ref.begin(), f->dedup_ref.end(), 0);
   for (int p = 0; p < np; ++p)
     if (!f->srcs[p].empty()) f->dedup_ref[f->refs[p]] = 1;
   f->dedup_levels = levels;
   f->deduped = true;
-  CF_CUDA(cudaStreamSynchronize(f->stream));
   return SMVS_OK;
 }
 
@@ -815,9 +876,18 @@ int smvs_cross_filter_synchronize(smvs_cross_filter* f) {
 void smvs_cross_filter_destroy(smvs_cross_filter* f) {
   if (!f) return;
   cudaSetDevice(f->device);
-  if (f->stream) cudaStreamSynchronize(f->stream);
   FreeAll(f);
   delete f;
+}
+
+int smvs_cross_filter_release_cache(int gpu_index) {
+  int dev = gpu_index;
+  if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) return Fail(SMVS_ECUDA, "no current device");
+  cudaMemPool_t pool = DevicePool(dev);
+  if (!pool) return Fail(SMVS_ECUDA, "no memory pool on device %d", dev);
+  CF_CUDA(cudaDeviceSynchronize());
+  CF_CUDA(cudaMemPoolTrimTo(pool, 0));
+  return SMVS_OK;
 }
 
 }  // extern "C"

@@ -340,3 +340,90 @@ def noisy_maps(scene: Scene, seed: int = 0, rel_noise: float = 0.002, outlier_fr
         n /= np.maximum(np.linalg.norm(n, axis=0, keepdims=True), 1e-12)
         out.append((d.astype(np.float32), n.astype(np.float32)))
     return out
+
+
+def _backproject(v: SceneView, ys: np.ndarray, xs: np.ndarray, fy=None, fx=None) -> np.ndarray:
+    """World points of pixels (ys, xs) of a view at their ground-truth depth,
+    optionally at sub-pixel positions (ys + fy, xs + fx)."""
+    d = v.depth_gt[ys, xs].astype(np.float64)
+    Ki = np.linalg.inv(v.K)
+    px = xs.astype(np.float64) + (0 if fx is None else fx)
+    py = ys.astype(np.float64) + (0 if fy is None else fy)
+    pc = np.stack([px, py, np.ones_like(px)], -1) @ Ki.T * d[:, None]
+    return (pc - v.T) @ v.R  # R^T (x_cam - T)
+
+
+def sparse_points(scene: Scene, view: int, count: int = 2000, seed: int = 0, noise: float = 0.002) -> np.ndarray:
+    """Stand-in for the SfM points a view observes: surface points at random
+    sub-pixel positions (away from pixel borders) at the ground-truth depth
+    along the view's ray, with relative depth noise (n x 3 float32)."""
+    gen = np.random.default_rng(seed)
+    v = scene.views[view]
+    H, W = v.depth_gt.shape
+    ys, xs = gen.integers(0, H, count), gen.integers(0, W, count)
+    ok = v.depth_gt[ys, xs] > 0
+    ys, xs = ys[ok], xs[ok]
+    fy, fx = gen.uniform(0.2, 0.8, len(ys)), gen.uniform(0.2, 0.8, len(ys))
+    C = -v.R.T @ v.T
+    X = _backproject(v, ys, xs, fy, fx)
+    X = C + (X - C) * (1.0 + noise * gen.standard_normal(len(X)))[:, None]
+    return X.astype(np.float32)
+
+
+def grid_mesh(scene: Scene, view: int, step: int = 8, duplicate_frac: float = 0.0, seed: int = 0):
+    """Stand-in for a prior TriangleMesh: the view's ground-truth surface on a
+    grid of `step` pixels, two triangles per cell, wound so that they are front
+    facing; face normals point to the camera. Returns (vertices n x 3 float64,
+    faces m x 3 int32, face_normals m x 3 float64). A fraction of faces is
+    repeated (shared-depth ties)."""
+    gen = np.random.default_rng(seed)
+    v = scene.views[view]
+    H, W = v.depth_gt.shape
+    gy, gx = np.meshgrid(np.arange(0, H, step), np.arange(0, W, step), indexing="ij")
+    ny, nx = gy.shape
+    X = _backproject(v, gy.ravel(), gx.ravel())
+    valid = (v.depth_gt[gy, gx] > 0).ravel()
+    idx = np.arange(ny * nx).reshape(ny, nx)
+    a, b, c, d = idx[:-1, :-1].ravel(), idx[:-1, 1:].ravel(), idx[1:, :-1].ravel(), idx[1:, 1:].ravel()
+    # Model2Depth draws a triangle when the pixel is right of all three edges
+    # (m1, m2, m3 < 0, patch_match_controller.cc:598-601): (a, c, b), (b, c, d).
+    faces = np.concatenate([np.stack([a, c, b], 1), np.stack([b, c, d], 1)])
+    faces = faces[valid[faces].all(1)]
+    C = -v.R.T @ v.T
+    p0, p1, p2 = X[faces[:, 0]], X[faces[:, 1]], X[faces[:, 2]]
+    n = np.cross(p1 - p0, p2 - p0)
+    n /= np.maximum(np.linalg.norm(n, axis=1, keepdims=True), 1e-300)
+    flip = np.einsum("ij,ij->i", (p0 + p1 + p2) / 3 - C, n) > 0
+    n[flip] *= -1
+    if duplicate_frac > 0:
+        rep = gen.random(len(faces)) < duplicate_frac
+        faces = np.concatenate([faces, faces[rep]])
+        n = np.concatenate([n, n[rep]])
+        order = gen.permutation(len(faces))
+        faces, n = faces[order], n[order]
+    return X, faces.astype(np.int32), n
+
+
+def dense_points(scene: Scene, view: int, step: int = 3, seed: int = 0, duplicate_frac: float = 0.0):
+    """Stand-in for a fused point cloud (PlyPoint x/y/z, nx/ny/nz): ground-truth
+    surface points of a view on a grid with world-frame normals facing the
+    camera. A fraction of points is repeated with depths moved by 1e-9
+    relative (ties in float, not in double)."""
+    gen = np.random.default_rng(seed)
+    v = scene.views[view]
+    H, W = v.depth_gt.shape
+    gy, gx = np.meshgrid(np.arange(1, H, step), np.arange(1, W, step), indexing="ij")
+    gy, gx = gy.ravel(), gx.ravel()
+    ok = v.depth_gt[gy, gx] > 0
+    gy, gx = gy[ok], gx[ok]
+    X = _backproject(v, gy, gx)
+    n_cam = v.normal_gt[:, gy, gx].T.astype(np.float64)
+    n_w = n_cam @ v.R  # R^T n
+    if duplicate_frac > 0:
+        rep = gen.random(len(X)) < duplicate_frac
+        C = -v.R.T @ v.T
+        X = np.concatenate([X, C + (X[rep] - C) * (1 + 1e-9 * gen.standard_normal(int(rep.sum())))[:, None]])
+        n_w = np.concatenate([n_w, n_w[rep]])
+        order = gen.permutation(len(X))
+        X, n_w = X[order], n_w[order]
+    return X.astype(np.float32), n_w.astype(np.float32)

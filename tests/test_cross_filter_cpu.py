@@ -127,3 +127,16 @@ def test_cross_filter_abi_declared():
     assert b"share reference view" in lib.smvs_last_error()
     p[0].num_src = 32
     assert lib.smvs_cross_filter_create(C.byref(o), v, 2, p, 1, N.MEM_HOST, None, C.byref(h)) == N.SMVS_EINVAL
+
+
+def test_decode_short_form_is_exact_for_every_code():
+    """The CUDA filter decodes normal codes with (float)((double)iq * (1/32767))
+    and 1 - 2s in float; both equal the reference's expressions
+    ((float)iq / 32767.f and (float)(1.0 - 2.0 * s)) for every input it sees."""
+    iq = np.arange(65536, dtype=np.float32)
+    assert np.array_equal(iq / np.float32(32767), (iq.astype(np.float64) * (1.0 / 32767.0)).astype(np.float32))
+    q = (iq / np.float32(32767) - np.float32(1)).astype(np.float32)
+    rng = np.random.default_rng(0)
+    q1, q2 = rng.choice(q, 2_000_000), rng.choice(q, 2_000_000)
+    s = (q1 * q1 + q2 * q2).astype(np.float32)  # any float s in [0, 2]
+    assert np.array_equal((1.0 - 2.0 * s.astype(np.float64)).astype(np.float32), np.float32(1) - np.float32(2) * s)

@@ -189,3 +189,19 @@ def test_cross_filter_vs_reference_kernels():
         if not keep.any():  # e.g. the first problem: every consistent pixel is still kept by a later view
             continue
         assert np.mean(np.abs(ref_delta[r][keep] - delta[r][keep]) <= 1e-4 + 1e-4 * np.abs(delta[r][keep])) > 0.99
+
+
+def test_cross_filter_pool_reuse_and_release():
+    """Filters allocate from a stream-ordered pool: a second filter on the same
+    set reuses the freed blocks and gives the same maps; the cache can be
+    returned to the device."""
+    scene, views, problems = filter_set(seed=13, n_views=4)
+    opt = PatchMatchOptions()
+    a = _gpu_run(opt, views, problems)
+    b = _gpu_run(opt, views, problems)
+    for r in a["refined"]:
+        assert np.array_equal(a["refined"][r], b["refined"][r])
+    assert N.lib().smvs_cross_filter_release_cache(-1) == N.SMVS_OK
+    c = _gpu_run(opt, views, problems)
+    for k in range(len(views)):
+        assert np.array_equal(a["vis"][k], c["vis"][k])
