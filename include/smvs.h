@@ -435,6 +435,36 @@ int smvs_init_depth_from_dense_points(const smvs_view* view, const float* xyz, c
                                       size_t num_points, int level, int memory, float* depth, float* normal,
                                       float* depth_range, void* stream);
 
+/* ---- view selection and depth ranges from the sparse model (host) -------- */
+/* One image of mvs::Model (src/mvs/model.h): the world-to-camera pose and
+ * Image::IsRig. */
+typedef struct smvs_model_image {
+  float R[9];
+  float T[3];
+  int is_rig;
+} smvs_model_image;
+
+/* Model::GetMaxOverlappingImages (src/mvs/model.cc:701-935): for every image in
+ * `candidates` (the reference's unique_image_idxs), the source views sharing the
+ * most sparse points whose 75th-percentile triangulation angle reaches
+ * min_triangulation_angle (degrees), best first (a shared point counts 1.5x
+ * between images of the same rig kind); an image that observes no point falls
+ * back to spatial neighbours (distance and viewing-angle score). Points are
+ * Model::Point x/y/z (n x 3 float) with their tracks in CSR form
+ * (track_offsets[n + 1], track_images). Output in CSR form: out_offsets
+ * [num_images + 1] and out_images (capacity num_images * max_num_images); images
+ * outside `candidates` get no list. Ties keep ascending image order (the
+ * reference leaves their order unspecified). Host only; all host threads. */
+int smvs_select_views(const smvs_model_image* images, int num_images, const float* points, size_t num_points,
+                      const int32_t* track_offsets, const int32_t* track_images, const int32_t* candidates,
+                      int num_candidates, int max_num_images, double min_triangulation_angle,
+                      int32_t* out_offsets, int32_t* out_images);
+/* Model::ComputeDepthRanges (:941-959): per image the depth range of the
+ * model's bounding box corners (lt, rb as BoundingBox), first clamped to
+ * >= 1e-6. ranges is num_images x 2. Host only. */
+int smvs_compute_depth_ranges(const smvs_model_image* images, int num_images, const float bbox_lt[3],
+                              const float bbox_rb[3], float* ranges);
+
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);
 

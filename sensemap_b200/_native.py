@@ -116,6 +116,10 @@ class smvs_filter_problem(C.Structure):
     _fields_ = [("ref", C.c_int), ("src", C.POINTER(C.c_int)), ("num_src", C.c_int)]
 
 
+class smvs_model_image(C.Structure):
+    _fields_ = [("R", C.c_float * 9), ("T", C.c_float * 3), ("is_rig", C.c_int)]
+
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "smvs_options_default": (C.c_int, [C.POINTER(smvs_options)]),
@@ -170,6 +174,10 @@ _SIGNATURES = {
                                             C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_init_depth_from_dense_points": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
                                                     C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_select_views": (C.c_int, [C.POINTER(smvs_model_image), C.c_int, C.c_void_p, C.c_size_t, C.c_void_p,
+                                    C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
+    "smvs_compute_depth_ranges": (C.c_int, [C.POINTER(smvs_model_image), C.c_int, C.c_void_p, C.c_void_p,
+                                            C.c_void_p]),
     "smvs_pool_options_default": (C.c_int, [C.POINTER(smvs_pool_options)]),
     "smvs_pool_create": (C.c_int, [C.POINTER(smvs_pool_options), C.c_void_p, C.POINTER(C.c_void_p)]),
     "smvs_pool_add_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(smvs_view), C.c_int]),

@@ -427,3 +427,38 @@ def dense_points(scene: Scene, view: int, step: int = 3, seed: int = 0, duplicat
         order = gen.permutation(len(X))
         X, n_w = X[order], n_w[order]
     return X.astype(np.float32), n_w.astype(np.float32)
+
+
+def ring_model(num_cameras: int = 40, num_points: int = 3000, radius: float = 20.0, width: int = 1600,
+               height: int = 1200, focal: float = 1200.0, seed: int = 0, drop: float = 0.2):
+    """Stand-in for a sparse SfM model around a ring of cameras (config 3's
+    200-camera ring, radius 20 m, heights 2-6 m): cameras look at the scene
+    centre; points lie on a seeded terrain inside the ring; a point's track is
+    the cameras it projects into, each observation dropped with probability
+    `drop`. Returns (Rs, Ts, K, points n x 3 float32, tracks, is_rig)."""
+    gen = np.random.default_rng(seed)
+    K = intrinsics(focal, width, height)
+    Rs, Ts = [], []
+    for i in range(num_cameras):
+        a = 2 * math.pi * i / num_cameras + gen.uniform(-0.02, 0.02)
+        pos = np.array([radius * math.cos(a), radius * math.sin(a), gen.uniform(2.0, 6.0)])
+        R, T = look_at(pos, (0.0, 0.0, 0.0))
+        Rs.append(R)
+        Ts.append(T)
+    r = 12.0 * np.sqrt(gen.random(num_points))
+    th = 2 * math.pi * gen.random(num_points)
+    x, y = r * np.cos(th), r * np.sin(th)
+    z = 0.8 * np.sin(0.4 * x) * np.cos(0.3 * y) + gen.uniform(0, 3.0, num_points) * (gen.random(num_points) < 0.2)
+    P = np.stack([x, y, z], 1)
+    tracks = [[] for _ in range(num_points)]
+    for c in range(num_cameras):
+        Xc = P @ Rs[c].T + Ts[c]
+        uv = Xc @ K.T
+        ok = Xc[:, 2] > 0.1
+        u = uv[:, 0] / np.where(ok, uv[:, 2], 1)
+        v = uv[:, 1] / np.where(ok, uv[:, 2], 1)
+        ok &= (u >= 0) & (u < width) & (v >= 0) & (v < height) & (gen.random(num_points) >= drop)
+        for i in np.nonzero(ok)[0]:
+            tracks[i].append(c)
+    is_rig = (np.arange(num_cameras) % 3 == 0)
+    return Rs, Ts, K, P.astype(np.float32), tracks, is_rig
