@@ -253,9 +253,10 @@ class PoolWorkload:
     """The same scene step through the batched pool: every view resident once,
     11 photometric jobs in one batch, then 11 geometric jobs in one batch."""
 
-    def __init__(self, wl: Workload, block_x: int = 32):
+    def __init__(self, wl: Workload, block_x: int = 32, ref_tile_tma: bool = True):
         self.wl = wl
         self.block_x = block_x
+        self.ref_tile_tma = ref_tile_tma
 
     def _run(self, pool, images):
         from sensemap_b200.patch_match import View
@@ -282,7 +283,7 @@ class PoolWorkload:
     def new_pool(self, stream):
         from sensemap_b200.pool import DepthMapPool
         return DepthMapPool(memory_budget_bytes=64 << 30, max_active_jobs=self.wl.V, image_storage=self.wl.storage,
-                            sweep_block_x=self.block_x, stream=stream)
+                            sweep_block_x=self.block_x, stream=stream, ref_tile_tma=self.ref_tile_tma)
 
     def step_device(self, stream):
         pool = self.new_pool(stream)
@@ -404,7 +405,13 @@ def main():
         run_single(args, wl, sptr)
         return
 
-    pw = PoolWorkload(wl)
+    # Launch shape from the autotuner (one iteration of view 0's photometric
+    # pass per candidate, before the timed region; maps do not depend on it).
+    from sensemap_b200.patch_match import autotune
+    tune = autotune(make_options(scene, storage, False), wl.problem(0, wl.views(dev_imgs)), stream=sptr, repeats=2)
+    log(f"autotune: block_x={tune['sweep_block_x']} tma={tune['ref_tile_tma']} "
+        f"({', '.join(f'{c['sweep_block_x']}/{int(c['ref_tile_tma'])}: {c['ms_per_sweep']:.2f} ms' for c in tune['candidates'])})")
+    pw = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"])
     import sensemap_b200._native as NN
 
     def device_step():
@@ -454,6 +461,7 @@ def main():
     prof_keep = []
     views = wl.views(dev_imgs)
     pm = PatchMatchACMMCuda(make_options(scene, storage, False), wl.problem(0, views), stream=sptr)
+    pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"])
     pm.SetProfiling(True)
     pm.Run()
     prof = pm.Profile()
@@ -513,7 +521,7 @@ def main():
                            "global_batch": wl.V * world, "parallelism": f"views sharded, {world} replica(s)",
                            "l2": "inputs larger than L2 (11 x 1600x1200 images + maps per step)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "serving": serving,
-                "clocks": clock_info,
+                "clocks": clock_info, "autotune": tune,
                 "accuracy": {"within_1pct_gt_mean": float(np.mean(acc)), "per_view": [round(a, 4) for a in acc]}}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -218,8 +218,22 @@ typedef enum smvs_kernel_kind {
  * them). No counterpart in the reference. */
 typedef struct smvs_tuning {
   int sweep_block_x; /* threads per block in x: 8, 16, 32 (default) or 64; 256 / x in y */
+  int ref_tile_tma;  /* 1 (default): stage the reference tile with a TMA load where the image
+                        qualifies (rows a multiple of 16 bytes, image at least one tile);
+                        0: plain loads */
 } smvs_tuning;
 int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
+/* The launch shape in use and whether the last smvs_run staged its reference
+ * tiles with TMA (ref_tile_tma = 1) or with plain loads (0). */
+int smvs_get_tuning(const smvs_engine* eng, smvs_tuning* tuning);
+/* Launch-shape autotuner: on a scratch engine for (opt, prob), times one
+ * iteration's checkerboard sweep for every launch shape (sweep_block_x 8, 16,
+ * 32, 64; reference tiles by TMA where the image qualifies, and by plain
+ * loads), best of `repeats` (<= 0: 3), and writes the fastest to `best`. The
+ * candidates and their ms per sweep launch go to tried/ms (up to `capacity`),
+ * their number to num_tried. Maps do not depend on the choice. */
+int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* stream, int repeats, smvs_tuning* best,
+                  smvs_tuning* tried, double* ms, int capacity, int* num_tried);
 /* Record CUDA events around every subsequent launch of this engine. */
 int smvs_set_profiling(smvs_engine* eng, int enable);
 /* Number of timed launches of `kind` and their summed device time (ms); synchronises. */
@@ -245,6 +259,7 @@ typedef struct smvs_pool_options {
   int sweep_block_x;          /* launch shape (smvs_tuning) */
   int use_graphs;             /* capture each batch's iteration in a CUDA graph */
   int gpu_index;              /* -1 = current device */
+  int ref_tile_tma;           /* stage reference tiles with TMA where a view qualifies (smvs_tuning) */
 } smvs_pool_options;
 
 typedef struct smvs_pool_stats {

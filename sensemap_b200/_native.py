@@ -82,12 +82,13 @@ class smvs_problem(C.Structure):
 
 
 class smvs_tuning(C.Structure):
-    _fields_ = [("sweep_block_x", C.c_int)]
+    _fields_ = [("sweep_block_x", C.c_int), ("ref_tile_tma", C.c_int)]
 
 
 class smvs_pool_options(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_active_jobs", C.c_int), ("image_storage", C.c_int),
-                ("sweep_block_x", C.c_int), ("use_graphs", C.c_int), ("gpu_index", C.c_int)]
+                ("sweep_block_x", C.c_int), ("use_graphs", C.c_int), ("gpu_index", C.c_int),
+                ("ref_tile_tma", C.c_int)]
 
 
 class smvs_pool_stats(C.Structure):
@@ -139,6 +140,10 @@ _SIGNATURES = {
     "smvs_launch_count": (C.c_int64, [C.c_void_p]),
     "smvs_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "smvs_set_tuning": (C.c_int, [C.c_void_p, C.POINTER(smvs_tuning)]),
+    "smvs_get_tuning": (C.c_int, [C.c_void_p, C.POINTER(smvs_tuning)]),
+    "smvs_autotune": (C.c_int, [C.POINTER(smvs_options), C.POINTER(smvs_problem), C.c_void_p, C.c_int,
+                                C.POINTER(smvs_tuning), C.POINTER(smvs_tuning), C.POINTER(C.c_double), C.c_int,
+                                C.POINTER(C.c_int)]),
     "smvs_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
     "smvs_destroy": (None, [C.c_void_p]),
     "smvs_last_error": (C.c_char_p, []),

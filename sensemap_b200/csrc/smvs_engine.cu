@@ -155,6 +155,10 @@ struct smvs_engine {
   uint16_t* d_curv = nullptr;   // 2*W*H (est_curvature && geom_consistency)
   // One-job batch for the checkerboard kernels: [JobParams | iters | prefix | conf prefix].
   void* d_batch = nullptr;
+  CUtensorMap* d_tmap = nullptr;  // the reference image's TMA descriptor
+  int* d_status = nullptr;        // bounded waits of the kernels that gave up
+  bool use_tma = true;
+  bool tma_active = false;        // the last run staged reference tiles with TMA
   float* d_ggrad = nullptr;     // W*H (median_filter)
   bool has_init = false;
   bool has_src_depth = false;
@@ -491,6 +495,12 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   if (prob->ref_mask) TRY(StageIn(e, prob->ref_mask, WH, prob->memory, (void**)&e->d_mask));
   if (opt->est_curvature && opt->geom_consistency) TRY(e->Alloc((void**)&e->d_curv, 2 * WH * sizeof(uint16_t)));
   TRY(e->Alloc(&e->d_batch, sizeof(smvs::JobParams) + 8 * sizeof(int)));
+  TRY(e->Alloc((void**)&e->d_tmap, sizeof(CUtensorMap)));
+  TRY(e->Alloc((void**)&e->d_status, sizeof(int)));
+  {
+    cudaError_t err = cudaMemsetAsync(e->d_status, 0, sizeof(int), e->stream);
+    if (err != cudaSuccess) { delete e; return Fail(SMVS_ECUDA, "status: %s", cudaGetErrorString(err)); }
+  }
   if (opt->median_filter) TRY(e->Alloc((void**)&e->d_ggrad, WH * sizeof(float)));
   // Source pixels/depths staged from host memory must stay valid until the
   // copies complete; the caller's buffers are only guaranteed during this call.
@@ -500,6 +510,28 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   }
 #undef TRY
   *out = e;
+  return SMVS_OK;
+}
+
+// The reference image's TMA descriptor for the job's launch shape, or
+// tma_box_w = 0 (plain loads) when the image does not qualify.
+static int UploadRefMap(smvs_engine* e, smvs::JobParams* p) {
+  p->tma_box_w = p->tma_box_h = 0;
+  CUtensorMap map;
+  if (!e->use_tma || !smvs::EncodeRefMap(&map, p->ref, p->W, p->H, p->block_x, p->R)) return SMVS_OK;
+  // The host descriptor dies at return: copy it before returning.
+  SMVS_CUDA(cudaMemcpyAsync(e->d_tmap, &map, sizeof(map), cudaMemcpyHostToDevice, e->stream));
+  SMVS_CUDA(cudaStreamSynchronize(e->stream));
+  p->tma_box_w = smvs::RefTileW(p->block_x, p->R);
+  p->tma_box_h = smvs::RefTileH(p->block_x, p->R);
+  return SMVS_OK;
+}
+
+// Reports a kernel wait that gave up (the stream has been synchronised).
+static int CheckStatus(smvs_engine* e) {
+  int status = 0;
+  SMVS_CUDA(cudaMemcpy(&status, e->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+  if (status) return Fail(SMVS_ETIMEDOUT, "a reference-tile copy did not complete; maps of this run are incomplete");
   return SMVS_OK;
 }
 
@@ -521,6 +553,8 @@ int smvs_run(smvs_engine* e) {
   if (st) return st;
   smvs::Batch b;
   if ((st = smvs_internal_prepare_job(&p, &o))) return st;
+  if ((st = UploadRefMap(e, &p))) return st;
+  e->tma_active = p.tma_box_w > 0;
   {
     // The checkerboard kernels run as a batch of one job.
     char host[sizeof(smvs::JobParams) + 8 * sizeof(int)];
@@ -544,6 +578,8 @@ int smvs_run(smvs_engine* e) {
     b.total_conf_blocks = ncb;
     b.block_x = p.block_x;
     b.R = p.R; b.S = p.S; b.NB = smvs::ViewBucket(p.N);
+    b.ref_maps = e->d_tmap;
+    b.status = e->d_status;
   }
   if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(b, e->stream); }))) return st;
   int* iters = const_cast<int*>(b.iters);
@@ -606,7 +642,7 @@ static int CopyOut(smvs_engine* e, void* dst, const void* src, size_t bytes, boo
   if (!need_run && !e->ran && !e->filtered) return Fail(SMVS_ESTATE, "call smvs_run or smvs_run_filter first");
   SMVS_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, e->stream));
   SMVS_CUDA(cudaStreamSynchronize(e->stream));
-  return SMVS_OK;
+  return CheckStatus(e);
 }
 
 int smvs_get_depth_map(smvs_engine* e, float* out) {
@@ -650,7 +686,7 @@ int smvs_get_device_maps(const smvs_engine* e, smvs_device_maps* m) {
 int smvs_synchronize(smvs_engine* e) {
   if (!e) return Fail(SMVS_EINVAL, "null engine");
   SMVS_CUDA(cudaStreamSynchronize(e->stream));
-  return SMVS_OK;
+  return CheckStatus(e);
 }
 int64_t smvs_launch_count(const smvs_engine* e) { return e ? e->launches : -1; }
 
@@ -659,6 +695,14 @@ int smvs_set_tuning(smvs_engine* e, const smvs_tuning* t) {
   const int bx = t->sweep_block_x;
   if (bx != 8 && bx != 16 && bx != 32 && bx != 64) return Fail(SMVS_EINVAL, "sweep_block_x must be 8, 16, 32 or 64");
   e->jp.block_x = bx;
+  e->use_tma = t->ref_tile_tma != 0;
+  return SMVS_OK;
+}
+
+int smvs_get_tuning(const smvs_engine* e, smvs_tuning* t) {
+  if (!e || !t) return Fail(SMVS_EINVAL, "null argument");
+  t->sweep_block_x = e->jp.block_x;
+  t->ref_tile_tma = e->tma_active ? 1 : 0;
   return SMVS_OK;
 }
 
@@ -685,5 +729,55 @@ int smvs_get_profile(smvs_engine* e, int kind, int* count, double* total_ms) {
   return SMVS_OK;
 }
 void smvs_destroy(smvs_engine* e) { delete e; }
+
+// Launch-shape autotuner: times the checkerboard sweep of one iteration of
+// `prob` for every candidate launch shape (threads per block in x, reference
+// tiles by TMA or by plain loads) on a scratch engine, best of `repeats`, and
+// returns the fastest. Results do not depend on the launch shape, so the
+// choice only affects speed.
+int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* stream, int repeats, smvs_tuning* best,
+                  smvs_tuning* tried, double* ms, int capacity, int* num_tried) {
+  if (!opt || !prob || !best) return Fail(SMVS_EINVAL, "null argument");
+  smvs_options o = *opt;
+  o.num_iterations = 1;  // init, InitConf and both colours of one sweep
+  smvs_engine* e = nullptr;
+  int st = smvs_create(&o, prob, stream, &e);
+  if (st) return st;
+  const int xs[4] = {8, 16, 32, 64};
+  double best_ms = 0;
+  int n = 0;
+  for (int k = 0; k < 4 && st == SMVS_OK; ++k)
+    for (int tma = 1; tma >= 0 && st == SMVS_OK; --tma) {
+      smvs_tuning t{xs[k], tma};
+      if ((st = smvs_set_tuning(e, &t))) break;
+      double t_best = 0;
+      for (int r = 0; r < (repeats > 0 ? repeats : 3) && st == SMVS_OK; ++r) {
+        if ((st = smvs_synchronize(e))) break;
+        for (auto& ev : e->timed) { cudaEventDestroy(ev.start); cudaEventDestroy(ev.stop); }
+        e->timed.clear();
+        if ((st = smvs_set_profiling(e, 1)) || (st = smvs_run(e))) break;
+        int cnt = 0;
+        double tot = 0;
+        if ((st = smvs_get_profile(e, SMVS_KERNEL_SWEEP, &cnt, &tot))) break;
+        if (cnt > 0 && (r == 0 || tot / cnt < t_best)) t_best = tot / cnt;
+      }
+      if (st) break;
+      smvs_tuning used;
+      smvs_get_tuning(e, &used);
+      if (tma && !used.ref_tile_tma) continue;  // the image does not qualify: same as the plain candidate
+      if (tried && ms && n < capacity) {
+        tried[n] = used;
+        ms[n] = t_best;
+      }
+      ++n;
+      if (n == 1 || t_best < best_ms) {
+        best_ms = t_best;
+        *best = used;
+      }
+    }
+  if (num_tried) *num_tried = n;
+  smvs_destroy(e);
+  return st;
+}
 
 }  // extern "C"

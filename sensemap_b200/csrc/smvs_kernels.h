@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>  // CUtensorMap (type only; the encoder is reached through the runtime)
 #include <cuda_runtime.h>
 
 #include "../../include/smvs.h"
@@ -31,6 +32,7 @@ struct alignas(16) JobParams {
   int local_opt;
   int blocks_x;                     // batched launches: this job's checkerboard blocks per row
   int conf_blocks_x;                // batched InitConf launches: blocks per row
+  int tma_box_w, tma_box_h;         // box of this job's reference tensor map; 0 = stage with loads
   float th_tab[kMaxIterations];     // th_mc of each iteration (patch_match_cuda.cu:778-779)
   // State maps (dense row-major; normal and cost planar).
   float* depth;
@@ -61,7 +63,24 @@ struct Batch {
   int total_conf_blocks;        // full tiling
   int block_x;                  // shared launch shape of the batch
   int R, S, NB;                 // shared window and view bucket of the batch
+  const CUtensorMap* ref_maps;  // per job: reference image for TMA tile loads (jobs with tma_box_w > 0)
+  int* status;                  // set to 1 when a bounded wait of a kernel gave up
 };
+
+// Reference tile of the checkerboard kernels (block bx x 256/bx threads, two
+// columns per thread): rows [row0 - R, row0 + by + R), columns starting at
+// col0 - R - RefTileShift(R), so that the first column is a multiple of 4
+// floats (col0 is a multiple of 2 bx >= 16): a TMA box may only start on a
+// 16-byte boundary. The tile's row stride is RefTileW.
+__host__ __device__ inline int RefTileShift(int R) { return (4 - (R & 3)) & 3; }
+__host__ __device__ inline int RefTileW(int bx, int R) { return (2 * bx + 2 * R + RefTileShift(R) + 3) & ~3; }
+__host__ __device__ inline int RefTileH(int bx, int R) { return 256 / bx + 2 * R; }
+
+// Encodes the TMA descriptor of a dense W x H FP32 reference image for the
+// checkerboard tile of launch shape bx and window R. Returns false (use plain
+// loads) when the image rows are not a multiple of 16 bytes, the image is
+// smaller than the box, or the driver does not provide the encoder.
+bool EncodeRefMap(CUtensorMap* map, const float* ref, int W, int H, int bx, int R);
 
 // All launchers enqueue on `stream` and return the launch status.
 cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, int w, int h, void* out,

@@ -150,6 +150,7 @@ struct PoolJob {
   int state = kQueued;
   int iter = 0;
   smvs::JobParams p;
+  CUtensorMap map;         // the reference view's TMA descriptor (p.tma_box_w > 0)
   void* block = nullptr;   // one allocation for every per-job buffer
   size_t block_bytes = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
@@ -188,6 +189,9 @@ struct smvs_pool {
   int* d_ints = nullptr;   // [iters (cap) | prefix (cap+32) | conf prefix (cap+32)]
   smvs::JobParams* h_jobs = nullptr;
   int* h_ints = nullptr;
+  CUtensorMap* d_maps = nullptr;  // per job, as d_jobs
+  CUtensorMap* h_maps = nullptr;
+  int* d_status = nullptr;        // bounded waits of the kernels that gave up
   int capacity = 0;
   // Graph of the current batch's step (valid while the batch is unchanged).
   cudaGraphExec_t graph = nullptr;
@@ -207,8 +211,11 @@ struct smvs_pool {
     arena.Trim();
     cudaFree(d_jobs);
     cudaFree(d_ints);
+    cudaFree(d_maps);
+    cudaFree(d_status);
     cudaFreeHost(h_jobs);
     cudaFreeHost(h_ints);
+    cudaFreeHost(h_maps);
     if (own_stream && stream) cudaStreamDestroy(stream);
   }
   void ReleaseView(PoolView& v) {
@@ -266,13 +273,18 @@ int EnsureCapacity(smvs_pool* P, int n) {
   cudaStreamSynchronize(P->stream);
   cudaFree(P->d_jobs);
   cudaFree(P->d_ints);
+  cudaFree(P->d_maps);
   cudaFreeHost(P->h_jobs);
   cudaFreeHost(P->h_ints);
+  cudaFreeHost(P->h_maps);
   P->d_jobs = nullptr; P->d_ints = nullptr; P->h_jobs = nullptr; P->h_ints = nullptr;
+  P->d_maps = nullptr; P->h_maps = nullptr;
   POOL_CUDA(cudaMalloc(&P->d_jobs, sizeof(smvs::JobParams) * cap));
   POOL_CUDA(cudaMalloc(&P->d_ints, sizeof(int) * IntsSize(cap)));
+  POOL_CUDA(cudaMalloc(&P->d_maps, sizeof(CUtensorMap) * cap));
   POOL_CUDA(cudaMallocHost(&P->h_jobs, sizeof(smvs::JobParams) * cap));
   POOL_CUDA(cudaMallocHost(&P->h_ints, sizeof(int) * IntsSize(cap)));
+  POOL_CUDA(cudaMallocHost(&P->h_maps, sizeof(CUtensorMap) * cap));
   P->capacity = cap;
   P->batch_dirty = true;
   return SMVS_OK;
@@ -290,6 +302,7 @@ int smvs_pool_options_default(smvs_pool_options* o) {
   o->image_storage = SMVS_STORE_U8;
   o->sweep_block_x = 32;
   o->use_graphs = 1;
+  o->ref_tile_tma = 1;
   o->gpu_index = -1;
   return SMVS_OK;
 }
@@ -319,6 +332,11 @@ int smvs_pool_create(const smvs_pool_options* o, void* stream, smvs_pool** out) 
   }
   int st = EnsureCapacity(P, o->max_active_jobs);
   if (st) { delete P; return st; }
+  if (cudaMalloc(&P->d_status, sizeof(int)) != cudaSuccess ||
+      cudaMemsetAsync(P->d_status, 0, sizeof(int), P->stream) != cudaSuccess) {
+    delete P;
+    return Fail(SMVS_ENOMEM, "pool status word");
+  }
   *out = P;
   return SMVS_OK;
 }
@@ -495,6 +513,12 @@ int Admit(smvs_pool* P, PoolJob& J) {
   p.refiK[3] = -p.refK[3] / p.refK[2];
   p.block_x = P->opt.sweep_block_x;
   p.ref = rv.ref;
+  p.tma_box_w = p.tma_box_h = 0;
+  memset(&J.map, 0, sizeof(J.map));
+  if (P->opt.ref_tile_tma && smvs::EncodeRefMap(&J.map, p.ref, W, H, p.block_x, p.R)) {
+    p.tma_box_w = smvs::RefTileW(p.block_x, p.R);
+    p.tma_box_h = smvs::RefTileH(p.block_x, p.R);
+  }
   for (int i = 0; i < N; ++i) {
     PoolView& sv = P->views[J.srcs[i]];
     p.src_tex[i] = sv.tex;
@@ -566,6 +590,7 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
     for (int k = 0; k < n; ++k) {
       PoolJob& J = P->jobs[list[k]];
       P->h_jobs[base + k] = J.p;
+      P->h_maps[base + k] = J.map;
       iters[base + k] = J.iter;
       prefix[pos + k] = tot;
       cprefix[pos + k] = ctot;
@@ -575,6 +600,8 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
     prefix[pos + n] = tot;
     cprefix[pos + n] = ctot;
     b.jobs = P->d_jobs + base;
+    b.ref_maps = P->d_maps + base;
+    b.status = P->d_status;
     b.iters = P->d_ints + base;
     b.block_start = P->d_ints + cap + pos;
     b.conf_block_start = P->d_ints + 2 * cap + kMaxGroups + pos;
@@ -591,6 +618,7 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
 
 int Upload(smvs_pool* P, int njobs) {
   POOL_CUDA(cudaMemcpyAsync(P->d_jobs, P->h_jobs, sizeof(smvs::JobParams) * njobs, cudaMemcpyHostToDevice, P->stream));
+  POOL_CUDA(cudaMemcpyAsync(P->d_maps, P->h_maps, sizeof(CUtensorMap) * njobs, cudaMemcpyHostToDevice, P->stream));
   POOL_CUDA(cudaMemcpyAsync(P->d_ints, P->h_ints, sizeof(int) * IntsSize(P->capacity), cudaMemcpyHostToDevice,
                             P->stream));
   return SMVS_OK;
@@ -675,6 +703,11 @@ int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
   }
   P->steps++;
   POOL_CUDA(cudaStreamSynchronize(P->stream));
+  {
+    int status = 0;
+    POOL_CUDA(cudaMemcpy(&status, P->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+    if (status) return Fail(SMVS_ETIMEDOUT, "a reference-tile copy did not complete; active jobs' maps are incomplete");
+  }
   // 4. Retire jobs that finished their iterations.
   const double now = NowSeconds();
   std::vector<int64_t> still;

@@ -17,8 +17,15 @@ namespace detail {
 namespace {  // internal linkage: every window translation unit gets its own copy
 
 constexpr int kThreads = 256;  // threads per block; the block's x/y split is a tuning knob (JobParams)
+// Resident blocks per SM the register allocation of the sweep kernels must
+// allow; 0 leaves the register budget to the compiler.
 #ifndef SMVS_SWEEP_MIN_BLOCKS
-#define SMVS_SWEEP_MIN_BLOCKS 1  // resident blocks per SM the register allocation must allow
+#define SMVS_SWEEP_MIN_BLOCKS 0
+#endif
+#if SMVS_SWEEP_MIN_BLOCKS > 0
+#define SMVS_SWEEP_BOUNDS __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS)
+#else
+#define SMVS_SWEEP_BOUNDS __launch_bounds__(kThreads)
 #endif
 
 __constant__ float kMWeights[5] = {0.f, 1.f, 2.01f, 3.03f, 4.06f};  // kernel_functions.cu:22
@@ -48,6 +55,84 @@ __device__ __forceinline__ void StageShared(const JobParams& p, float* tile, int
     tile[i] = RefAt(p.ref, p.W, p.H, row0 + r, col0 + c);
   }
   for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += nthr) poses[i] = __ldg(p.poses + i);
+}
+
+// Bounded waits (mbarrier polls) before a kernel gives up on a TMA copy.
+constexpr uint32_t kTmaWaitPolls = 1u << 22;
+
+__device__ __forceinline__ float* Align128(float* p) {
+  return reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(p) + 127) & ~static_cast<uintptr_t>(127));
+}
+
+__device__ __forceinline__ uint32_t SmemAddr(const void* ptr) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(ptr));
+}
+
+__device__ __forceinline__ bool MbarPoll(uint32_t bar, uint32_t parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity) {
+  for (uint32_t i = 0; i < kTmaWaitPolls; ++i) {
+    if (MbarPoll(bar, parity)) return true;
+    if (i >= 32) __nanosleep(64);
+  }
+  return false;
+}
+
+// The block's reference tile as one TMA load: box (RefTileW x RefTileH) of
+// `map` at column x (a multiple of 4) and row y into `tile` (128-byte aligned
+// shared memory); rows and columns outside the image read as zero (the
+// border of the reference's texture). Every thread waits on the mbarrier with
+// a bounded wait. Returns false after setting *status if the copy did not
+// land; the caller then leaves the block's pixels unchanged.
+__device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile, int x, int y, uint32_t bytes,
+                                             uint64_t* mbar, int* status) {
+  const uint32_t bar = SmemAddr(mbar);
+  const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
+  if (leader) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  __syncthreads();
+  if (leader) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(SmemAddr(tile)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+  }
+  const bool landed = MbarWait(bar, 0);
+  if (!__syncthreads_or(!landed)) return true;  // block-uniform outcome
+  if (leader) atomicExch(status, 1);
+  MbarWait(bar, 0);  // let a late copy land before the block's shared memory is released
+  return false;
+}
+
+// Stage the reference tile (TMA when the job has a descriptor for this launch
+// shape, else plain loads) and the pose records. `tile` holds RefTileH rows of
+// RefTileW floats starting at (row0 - R, col0 - R - RefTileShift(R)).
+template <int R>
+__device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobParams& p, float* tile, int row0,
+                                             int col0, float* poses, uint64_t* mbar) {
+  const int bx = blockDim.x;
+  const int tw = RefTileW(bx, R), th = RefTileH(bx, R);
+  const int x0 = col0 - R - RefTileShift(R), y0 = row0 - R;
+  const bool tma = b.ref_maps != nullptr && p.tma_box_w == tw && p.tma_box_h == th;
+  if (!tma) {
+    StageShared(p, tile, y0, x0, th, tw, poses);
+    return true;
+  }
+  const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+  for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += blockDim.x * blockDim.y) poses[i] = __ldg(p.poses + i);
+  return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, b.status);
 }
 
 // Batched launches: find this block's job (binary search over the block
@@ -209,9 +294,10 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
 // propagate_depth): one checkerboard colour, one thread per pixel.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) SweepKernel(const Batch b, int colour) {
+__global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
+  __shared__ uint64_t mbar;
   int job, blk, iter;
   DecodeBlock(b, b.block_start, sp, job, blk, iter);
   const JobParams& p = sp;
@@ -219,11 +305,11 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) SweepKernel(c
   const float th_mc = p.th_tab[iter];
   const uint64_t skey = StageKey(p.seed, StageSweep(iter, colour));
   const int kBX = blockDim.x, kBY = blockDim.y;
-  const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
-  float* tile = smem;
-  float* poses = smem + tw * th;
+  const int tw = RefTileW(kBX, R), th = RefTileH(kBX, R);
+  float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
+  float* poses = tile + tw * th;
   const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, poses, &mbar)) return;  // block-uniform
   __syncthreads();
   const int row = row0 + threadIdx.y;
   const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
@@ -303,7 +389,7 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) SweepKernel(c
   pr.rsum = p.ref_sum[pix];
   pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
   pr.ws = tw;
-  pr.win = tile + threadIdx.y * tw + (col - col0);
+  pr.win = tile + threadIdx.y * tw + (col - col0) + RefTileShift(R);
   float M[kMaxHyp][NB];
   for (int v = 0; v < N; ++v) M[0][v] = p.cost[(size_t)v * WH + pix];
   float vw[NB];
@@ -413,9 +499,10 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) SweepKernel(c
 
 // LocalOptimization, kernel_functions.cu:2736-2931.
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) LocalOptKernel(const Batch b, int colour) {
+__global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
+  __shared__ uint64_t mbar;
   int job, blk, iter;
   DecodeBlock(b, b.block_start, sp, job, blk, iter);
   const JobParams& p = sp;
@@ -423,11 +510,11 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) LocalOptKerne
   if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
   const uint64_t skey = StageKey(p.seed, StageLocal(iter, colour));
   const int kBX = blockDim.x, kBY = blockDim.y;
-  const int tw = 2 * kBX + 2 * R, th = kBY + 2 * R;
-  float* tile = smem;
-  float* poses = smem + tw * th;
+  const int tw = RefTileW(kBX, R), th = RefTileH(kBX, R);
+  float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
+  float* poses = tile + tw * th;
   const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, poses, &mbar)) return;  // block-uniform
   __syncthreads();
   const int row = row0 + threadIdx.y;
   const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
@@ -462,7 +549,7 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) LocalOptKerne
   pr.rsum = p.ref_sum[pix];
   pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
   pr.ws = tw;
-  pr.win = tile + threadIdx.y * tw + (col - col0);
+  pr.win = tile + threadIdx.y * tw + (col - col0) + RefTileShift(R);
   float M[5][NB];
   float hyp[5][4];
   int mi = -1;
@@ -515,7 +602,8 @@ __global__ void __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS) LocalOptKerne
 
 template <int R, int S>
 size_t SweepSmem(int NB, int bx, int by) {
-  return sizeof(float) * ((2 * bx + 2 * R) * (by + 2 * R) + NB * SMVS_POSE_FLOATS);
+  (void)by;
+  return 128 + sizeof(float) * (RefTileW(bx, R) * RefTileH(bx, R) + NB * SMVS_POSE_FLOATS);  // + alignment slack
 }
 
 template <int R, int S, int NB>

@@ -145,6 +145,65 @@ def _addr(x):
     return x.ctypes.data, x, False
 
 
+def _problem_struct(problem: Problem):
+    """(smvs_problem, objects that must stay alive) for a Problem."""
+    keep = []
+    memories = set()
+
+    def fill_view(cv: N.smvs_view, v: View, scale: float) -> None:
+        img = v.image
+        if _is_cuda_tensor(img):
+            fmt = N.PIX_U8 if str(img.dtype) in ("torch.uint8", "uint8") else N.PIX_F32
+            if fmt == N.PIX_F32 and str(img.dtype) not in ("torch.float32", "float32"):
+                img = img.float()
+        else:
+            img = np.asarray(img)
+            if img.dtype == np.uint8:
+                fmt = N.PIX_U8
+            else:
+                img = img.astype(np.float32, copy=False)
+                fmt = N.PIX_F32
+        ptr, obj, dev = _addr(img)
+        keep.append(obj)
+        memories.add(dev)
+        cv.width, cv.height, cv.pixel_format, cv.row_stride = v.width, v.height, fmt, 0
+        cv.pixels = ptr
+        cv.K[:] = [float(a) for a in np.asarray(v.K, dtype=np.float64).reshape(9)]
+        cv.R[:] = [float(a) for a in np.asarray(v.R, dtype=np.float64).reshape(9)]
+        cv.T[:] = [float(a) for a in np.asarray(v.T, dtype=np.float64).reshape(3)]
+        cv.scale = float(scale)
+        for name in ("depth", "normal"):
+            arr = getattr(v, name)
+            if arr is None:
+                setattr(cv, name, None)
+                continue
+            if not _is_cuda_tensor(arr):
+                arr = np.asarray(arr, dtype=np.float32)
+            p, o, d = _addr(arr)
+            keep.append(o)
+            memories.add(d)
+            setattr(cv, name, p)
+
+    prob = N.smvs_problem()
+    fill_view(prob.ref, problem.images[problem.ref_image_idx], 1.0)
+    srcs = (N.smvs_view * len(problem.src_image_idxs))()
+    scales = list(problem.src_image_scales) or [1.0] * len(problem.src_image_idxs)
+    for i, idx in enumerate(problem.src_image_idxs):
+        fill_view(srcs[i], problem.images[idx], scales[i])
+    prob.src = srcs
+    prob.num_src = len(problem.src_image_idxs)
+    if problem.mask is not None:
+        m = problem.mask if _is_cuda_tensor(problem.mask) else np.asarray(problem.mask, dtype=np.uint8)
+        p, o, d = _addr(m)
+        keep.append(o)
+        memories.add(d)
+        prob.ref_mask = p
+    if len(memories) > 1:
+        raise N.SmvsError(N.SMVS_EINVAL, "all images and maps must live in the same memory (host or device)")
+    prob.memory = N.MEM_DEVICE if memories == {True} else N.MEM_HOST
+    return prob, keep
+
+
 class PatchMatchACMMCuda:
     """Drop-in for sensemap::mvs::PatchMatchACMMCuda (patch_match_cuda.h:154-203)."""
 
@@ -152,60 +211,7 @@ class PatchMatchACMMCuda:
         self.options = options
         self.problem = problem
         lib = N.lib()
-        keep = []
-        memories = set()
-
-        def fill_view(cv: N.smvs_view, v: View, scale: float) -> None:
-            img = v.image
-            if _is_cuda_tensor(img):
-                fmt = N.PIX_U8 if str(img.dtype) in ("torch.uint8", "uint8") else N.PIX_F32
-                if fmt == N.PIX_F32 and str(img.dtype) not in ("torch.float32", "float32"):
-                    img = img.float()
-            else:
-                img = np.asarray(img)
-                if img.dtype == np.uint8:
-                    fmt = N.PIX_U8
-                else:
-                    img = img.astype(np.float32, copy=False)
-                    fmt = N.PIX_F32
-            ptr, obj, dev = _addr(img)
-            keep.append(obj)
-            memories.add(dev)
-            cv.width, cv.height, cv.pixel_format, cv.row_stride = v.width, v.height, fmt, 0
-            cv.pixels = ptr
-            cv.K[:] = [float(a) for a in np.asarray(v.K, dtype=np.float64).reshape(9)]
-            cv.R[:] = [float(a) for a in np.asarray(v.R, dtype=np.float64).reshape(9)]
-            cv.T[:] = [float(a) for a in np.asarray(v.T, dtype=np.float64).reshape(3)]
-            cv.scale = float(scale)
-            for name in ("depth", "normal"):
-                arr = getattr(v, name)
-                if arr is None:
-                    setattr(cv, name, None)
-                    continue
-                if not _is_cuda_tensor(arr):
-                    arr = np.asarray(arr, dtype=np.float32)
-                p, o, d = _addr(arr)
-                keep.append(o)
-                memories.add(d)
-                setattr(cv, name, p)
-
-        prob = N.smvs_problem()
-        fill_view(prob.ref, problem.images[problem.ref_image_idx], 1.0)
-        srcs = (N.smvs_view * len(problem.src_image_idxs))()
-        scales = list(problem.src_image_scales) or [1.0] * len(problem.src_image_idxs)
-        for i, idx in enumerate(problem.src_image_idxs):
-            fill_view(srcs[i], problem.images[idx], scales[i])
-        prob.src = srcs
-        prob.num_src = len(problem.src_image_idxs)
-        if problem.mask is not None:
-            m = problem.mask if _is_cuda_tensor(problem.mask) else np.asarray(problem.mask, dtype=np.uint8)
-            p, o, d = _addr(m)
-            keep.append(o)
-            memories.add(d)
-            prob.ref_mask = p
-        if len(memories) > 1:
-            raise N.SmvsError(N.SMVS_EINVAL, "all images and maps must live in the same memory (host or device)")
-        prob.memory = N.MEM_DEVICE if memories == {True} else N.MEM_HOST
+        prob, keep = _problem_struct(problem)
         handle = C.c_void_p()
         stream_ptr = C.c_void_p(int(stream)) if stream is not None else None
         N.check(lib.smvs_create(C.byref(options.to_c()), C.byref(prob), stream_ptr, C.byref(handle)))
@@ -269,9 +275,15 @@ class PatchMatchACMMCuda:
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_launch_count(self._h))
 
-    def SetTuning(self, sweep_block_x: int) -> None:
-        t = N.smvs_tuning(sweep_block_x=sweep_block_x)
+    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True) -> None:
+        t = N.smvs_tuning(sweep_block_x=sweep_block_x, ref_tile_tma=int(ref_tile_tma))
         N.check(N.lib().smvs_set_tuning(self._h, C.byref(t)))
+
+    def Tuning(self) -> dict:
+        """Launch shape in use and whether the last Run staged reference tiles with TMA."""
+        t = N.smvs_tuning()
+        N.check(N.lib().smvs_get_tuning(self._h, C.byref(t)))
+        return {"sweep_block_x": t.sweep_block_x, "ref_tile_tma": bool(t.ref_tile_tma)}
 
     def SetProfiling(self, enable: bool = True) -> None:
         N.check(N.lib().smvs_set_profiling(self._h, int(enable)))
@@ -302,3 +314,19 @@ class PatchMatchACMMCuda:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def autotune(options: PatchMatchOptions, problem: Problem, stream=None, repeats: int = 3) -> dict:
+    """Launch-shape autotuner (smvs_autotune): the fastest sweep launch shape for
+    this problem, with every candidate's ms per sweep launch."""
+    prob, keep = _problem_struct(problem)
+    best = N.smvs_tuning()
+    tried = (N.smvs_tuning * 16)()
+    ms = (C.c_double * 16)()
+    n = C.c_int()
+    stream_ptr = C.c_void_p(int(stream)) if stream is not None else None
+    N.check(N.lib().smvs_autotune(C.byref(options.to_c()), C.byref(prob), stream_ptr, int(repeats), C.byref(best),
+                                  tried, ms, 16, C.byref(n)))
+    return {"sweep_block_x": best.sweep_block_x, "ref_tile_tma": bool(best.ref_tile_tma),
+            "candidates": [{"sweep_block_x": tried[i].sweep_block_x, "ref_tile_tma": bool(tried[i].ref_tile_tma),
+                            "ms_per_sweep": ms[i]} for i in range(min(n.value, 16))]}
