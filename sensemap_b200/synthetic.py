@@ -231,25 +231,12 @@ def _height(X, Y, g):
     return h, hx, hy
 
 
-def heightfield_scene(seed: int = 0, width: int = 1600, height: int = 1200, focal: float = 1200.0,
-                      num_src: int = 10, gain_range=(0.8, 1.2), noise_sigma: float = 2.0, distance: float = 7.0,
-                      elevation_deg: float = 45.0, ring_radius: float = 0.8, device: str = "cpu",
-                      chunk: int = 1 << 20) -> Scene:
-    gen = np.random.default_rng(seed)
-    g = _gaussians(gen)
-    hmax = float(np.sum(g[2])) + 0.01
-    target = np.array([0.0, 0.0, 0.0])
-    el = math.radians(elevation_deg)
-    ref_pos = target + distance * np.array([0.0, -math.cos(el), math.sin(el)])
-    R0, _ = look_at(ref_pos, target)
-    positions = [ref_pos]
-    for k in range(num_src):
-        a = 2 * math.pi * k / num_src
-        positions.append(ref_pos + ring_radius * (math.cos(a) * R0[0] + math.sin(a) * R0[1]))
-    K = intrinsics(focal, width, height)
-    tex_salt = int(gen.integers(1, 1 << 30))
+def _render_heightfield(cams, target, g, hmax, tex_salt, gen, gain_range, noise_sigma, device, chunk):
+    """Ray-march the heightfield for cameras (position, width, height, focal),
+    each looking at `target`; returns SceneViews."""
     views = []
-    for pos in positions:
+    for pos, width, height, focal in cams:
+        K = intrinsics(focal, width, height)
         R, T = look_at(pos, target)
         origin, d, pc = _pixel_rays(K, R, T, width, height, device)
         dflat = d.reshape(-1, 3)
@@ -298,6 +285,27 @@ def heightfield_scene(seed: int = 0, width: int = 1600, height: int = 1200, foca
         img = _finish_image(albedo.reshape(height, width), gen, gain_range, noise_sigma)
         views.append(SceneView(img, K.copy(), R, T, depth.to(torch.float32).cpu().numpy(),
                                normal.permute(2, 0, 1).to(torch.float32).cpu().numpy()))
+    return views
+
+
+def heightfield_scene(seed: int = 0, width: int = 1600, height: int = 1200, focal: float = 1200.0,
+                      num_src: int = 10, gain_range=(0.8, 1.2), noise_sigma: float = 2.0, distance: float = 7.0,
+                      elevation_deg: float = 45.0, ring_radius: float = 0.8, device: str = "cpu",
+                      chunk: int = 1 << 20) -> Scene:
+    gen = np.random.default_rng(seed)
+    g = _gaussians(gen)
+    hmax = float(np.sum(g[2])) + 0.01
+    target = np.array([0.0, 0.0, 0.0])
+    el = math.radians(elevation_deg)
+    ref_pos = target + distance * np.array([0.0, -math.cos(el), math.sin(el)])
+    R0, _ = look_at(ref_pos, target)
+    positions = [ref_pos]
+    for k in range(num_src):
+        a = 2 * math.pi * k / num_src
+        positions.append(ref_pos + ring_radius * (math.cos(a) * R0[0] + math.sin(a) * R0[1]))
+    tex_salt = int(gen.integers(1, 1 << 30))
+    cams = [(pos, width, height, focal) for pos in positions]
+    views = _render_heightfield(cams, target, g, hmax, tex_salt, gen, gain_range, noise_sigma, device, chunk)
     d_ref = views[0].depth_gt
     valid = d_ref[d_ref > 0]
     return Scene(views, 0, list(range(1, num_src + 1)), float(valid.min()) * 0.9, float(valid.max()) * 1.1,
@@ -462,3 +470,39 @@ def ring_model(num_cameras: int = 40, num_points: int = 3000, radius: float = 20
             tracks[i].append(c)
     is_rig = (np.arange(num_cameras) % 3 == 0)
     return Rs, Ts, K, P.astype(np.float32), tracks, is_rig
+
+
+def ring_scene(seed: int = 0, num_cameras: int = 24, scale: float = 0.125, radius: float = 20.0,
+               num_refs: int = 8, min_src: int = 5, max_src: int = 20, device: str = "cpu",
+               gain_range=(0.8, 1.2), noise_sigma: float = 2.0):
+    """Stand-in for the batched configuration: cameras on a ring (radius 20 m,
+    heights 2-6 m) around the seeded heightfield, all looking at its centre,
+    each of one of three sizes (800x600, 1600x1200, 3000x2000, times `scale`,
+    focal 0.75 x width). `num_refs` reference views each take their k nearest
+    cameras on the ring as sources, k drawn from [min_src, max_src]. Returns
+    (Scene with every camera, [(ref, [src...]), ...])."""
+    gen = np.random.default_rng(seed)
+    g = _gaussians(gen)
+    hmax = float(np.sum(g[2])) + 0.01
+    target = np.array([0.0, 0.0, 0.0])
+    sizes = [(800, 600), (1600, 1200), (3000, 2000)]
+    cams = []
+    for i in range(num_cameras):
+        a = 2 * math.pi * i / num_cameras
+        pos = np.array([radius * math.cos(a), radius * math.sin(a), float(gen.uniform(2.0, 6.0))])
+        w, h = sizes[int(gen.integers(0, len(sizes)))]
+        w, h = max(16, int(round(w * scale))), max(16, int(round(h * scale)))
+        cams.append((pos, w, h, 0.75 * w))
+    tex_salt = int(gen.integers(1, 1 << 30))
+    views = _render_heightfield(cams, target, g, hmax, tex_salt, gen, gain_range, noise_sigma, device, 1 << 20)
+    refs = sorted(gen.choice(num_cameras, size=min(num_refs, num_cameras), replace=False).tolist())
+    jobs = []
+    for r in refs:
+        k = int(gen.integers(min_src, max_src + 1))
+        k = min(k, num_cameras - 1)
+        order = sorted((i for i in range(num_cameras) if i != r),
+                       key=lambda i: (min(abs(i - r), num_cameras - abs(i - r)), i))
+        jobs.append((r, order[:k]))
+    depths = np.concatenate([v.depth_gt[v.depth_gt > 0] for v in views])
+    return Scene(views, refs[0], jobs[0][1], float(depths.min()) * 0.9, float(depths.max()) * 1.1,
+                 name=f"ring(seed={seed},{num_cameras} cameras,scale={scale})", meta={"jobs": jobs}), jobs

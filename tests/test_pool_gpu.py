@@ -107,3 +107,22 @@ def test_budget_evicts_unreferenced_views_and_rejects_oversized_jobs(scenes):
             pool.step()
         assert ei.value.status == N.SMVS_ENOMEM
         pool.release(jid)
+
+
+def test_ring_of_uneven_views_batched():
+    """The batched configuration in small: a ring of cameras of three sizes
+    around the heightfield, reference views with 3-12 nearest sources, all
+    jobs admitted into one pool (one launch per kernel per window/view bucket)
+    and each result identical to the single-job engine."""
+    sc, jobs = syn.ring_scene(seed=2, num_cameras=20, scale=0.1, num_refs=6, min_src=3, max_src=12, device="cuda")
+    assert len({v.image.shape for v in sc.views}) > 1
+    assert len({len(s) for _, s in jobs}) > 1
+    results = []
+    with DepthMapPool(max_active_jobs=len(jobs)) as pool:
+        add_scene(pool, sc, 0)
+        for k, (r, srcs) in enumerate(jobs):
+            opt = photometric_options(sc, iters=4, random_seed=300 + k)
+            results.append((pool.submit(opt, r, srcs), r, srcs, opt))
+        pool.run_until_done([j[0] for j in results])
+        for jid, r, srcs, opt in results:
+            assert_same(pool.maps(jid), engine_maps(opt, problem_from_scene(sc, ref=r, src=srcs)))
