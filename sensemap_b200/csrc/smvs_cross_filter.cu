@@ -183,6 +183,13 @@ __device__ __forceinline__ float BackProject(const float4* rec, const float refK
   return bz;
 }
 
+// The reference compares float depths with double constants (depth < 1e-6,
+// src_depth < 1e-4); for a float x, (double)x < 1e-6 is x <= 1e-6f and
+// (double)x < 1e-4 is x <= 1e-4f (no float lies between each constant and
+// its float rounding, which is below it), so the tests stay in float.
+__device__ __forceinline__ bool BelowDepthEps(float x) { return x <= 1e-6f; }
+__device__ __forceinline__ bool BelowSrcEps(float x) { return x <= 1e-4f; }
+
 // BubbleSort (src/mvs/utils.h:205-221).
 __device__ __forceinline__ void BubbleSort(float* v, int n) {
   for (int i = 0; i < n - 1; ++i)
@@ -224,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) CrossFilterRunKernel(const CfJob* __
   const int W = sj.width, H = sj.height;
   const size_t pix = (size_t)row * W + col;
   const float depth = sj.depth[pix];
-  if ((double)depth < 1e-6 || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.out[pix] = 0.0f; return; }
+  if (BelowDepthEps(depth) || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.out[pix] = 0.0f; return; }
   float rn[3];
   Decode(__ldg(sj.code + pix), rn);
   float vr[3] = {fmaf(sj.refiK[0], (float)col, sj.refiK[1]), fmaf(sj.refiK[2], (float)row, sj.refiK[3]), 1.0f};
@@ -243,7 +250,7 @@ __global__ void __launch_bounds__(kThreads) CrossFilterRunKernel(const CfJob* __
     int q;
     if (!Texel(scol, srow, s.width, s.height, &q)) continue;  // border: depth 0 < 1e-4
     const float sd = __ldg(s.depth + q);
-    if ((double)sd < 1e-4) continue;
+    if (BelowSrcEps(sd)) continue;
     float err;
     const float bz = BackProject(rec, sj.refK, scol, srow, sd, col, row, &err);
     const float dd = depth - bz;
@@ -278,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) DedupKernel(const CfJob* __restrict_
   const int W = sj.width, H = sj.height;
   const size_t pix = (size_t)row * W + col;
   const float depth = sj.depth[pix];
-  if ((double)depth < 1e-6 || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.vis[pix] = 0u; return; }
+  if (BelowDepthEps(depth) || col < 3 || col > W - 3 || row < 3 || row > H - 3) { sj.vis[pix] = 0u; return; }
   const uint32_t vis0 = sj.vis[pix];
   if (!(vis0 >> 3)) { sj.vis[pix] = 0u; return; }  // [quirk] :3803 shifts by sizeof(uint32_t) - 1
   const float X[3] = {depth * fmaf(sj.refiK[0], (float)col, sj.refiK[1]),

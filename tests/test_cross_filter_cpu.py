@@ -140,3 +140,14 @@ def test_decode_short_form_is_exact_for_every_code():
     q1, q2 = rng.choice(q, 2_000_000), rng.choice(q, 2_000_000)
     s = (q1 * q1 + q2 * q2).astype(np.float32)  # any float s in [0, 2]
     assert np.array_equal((1.0 - 2.0 * s.astype(np.float64)).astype(np.float32), np.float32(1) - np.float32(2) * s)
+
+
+def test_float_forms_of_the_double_thresholds():
+    """The CUDA filter tests depth <= 1e-6f and src_depth <= 1e-4f where the
+    reference writes depth < 1e-6 and src_depth < 1e-4 with double constants:
+    the same answer for every float around the thresholds and the specials."""
+    for thr in (1e-4, 1e-6):
+        lo, hi = np.float32(thr / 2).view(np.int32), np.float32(thr * 2).view(np.int32)
+        xs = np.arange(lo, hi, dtype=np.int32).view(np.float32)
+        xs = np.concatenate([xs, -xs, np.array([0, -0.0, np.inf, -np.inf, np.nan, 1.0, 3e-38], np.float32)])
+        assert np.array_equal(xs.astype(np.float64) < thr, xs <= np.float32(thr))
