@@ -71,12 +71,13 @@ def parse():
     ap.add_argument("--serving-rate", type=float, default=2.0, help="job arrivals per second")
     ap.add_argument("--single", action="store_true",
                     help="profiling mode: run one photometric pass of view 0 per step (for ncu captures)")
-    ap.add_argument("--workload", default="patchmatch", choices=["patchmatch", "cross-filter"],
+    ap.add_argument("--workload", default="patchmatch", choices=["patchmatch", "cross-filter", "fusion"],
                     help="patchmatch: the depth-map stage (default); cross-filter: CrossFilterCuda::Run + "
-                         "DedupRun over the views' depth/normal maps")
+                         "DedupRun over the views' depth/normal maps; fusion: StereoFusion of the views' maps "
+                         "into a point cloud")
     args = ap.parse_args()
     if args.steps is None:
-        args.steps = 200 if args.workload == "cross-filter" else 3
+        args.steps = {"cross-filter": 200, "fusion": 10}.get(args.workload, 3)
     return args
 
 
@@ -379,6 +380,12 @@ def main():
             run_cross_filter_reference(args)
         else:
             run_cross_filter(args)
+        return
+    if args.workload == "fusion":
+        if args.impl == "reference":
+            run_fusion_reference(args)
+        else:
+            run_fusion(args)
         return
     if args.impl == "reference":
         run_reference(args)
@@ -772,6 +779,169 @@ def run_cross_filter(args):
                            "l2": f"inputs larger than L2 ({V} x {args.width}x{args.height} depth + normal maps)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clock_info,
                 "filter": {"refined_kept_fraction": kept, "kept_within_1pct_gt": acc}}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+FU_METRIC = "fused depth maps/s (1.6MP, 11 views)"
+
+
+def fusion_set(args, rank, device):
+    """The bench scene's views with noisy ground-truth depth/normal maps (what
+    the PatchMatch passes hand over), an RGB bitmap per view and, as each
+    view's overlapping images, every other view nearest first."""
+    from sensemap_b200 import synthetic as syn
+    scene = syn.heightfield_scene(seed=rank, width=args.width, height=args.height, num_src=args.views - 1,
+                                  device=device)
+    ims, ov = syn.fusion_inputs(scene, seed=200 + rank)
+    return scene, ims, ov
+
+
+def cpu_fusion(ims, ov) -> dict:
+    """The oracle (the reference's fusion loop, seed after seed, one thread)
+    over the whole set: fused depth maps/s."""
+    import oracle.oracle as orc
+    from sensemap_b200.fusion import FusionOptions
+    t = time.perf_counter()
+    out = orc.fusion_run(FusionOptions(), ims, ov, masks=False)
+    dt = time.perf_counter() - t
+    return {"value": len(out["order"]) / dt, "unit": "depth maps/s", "cores": 1, "kind": "port",
+            "sample": f"oracle fusion of the whole {len(ims)}-view set, one pass, {dt:.2f} s, "
+                      f"{len(out['points'])} points"}
+
+
+def run_fusion_reference(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    import torch
+    from oracle import build as oracle_build
+    oracle_build.build()
+    _, ims, ov = fusion_set(args, 0, "cuda" if torch.cuda.is_available() else "cpu")
+    samples, cb = [], None
+    steps = min(args.steps, 2)  # each step is a full CPU pass (several seconds)
+    for i in range(min(args.warmup, 1) + steps):
+        cb = cpu_fusion(ims, ov)
+        if i >= min(args.warmup, 1):
+            samples.append(cb["value"])
+    value = statistics.median(samples)
+    line = {"metric": FU_METRIC, "value": value, "unit": "depth maps/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * len(ims) / value, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": {"workload": f"fusion (StereoFusion image loop), {args.views} views {args.width}x{args.height}",
+                       "global_batch": len(ims), "parallelism": "cpu, one thread"},
+            "cpu_baseline": {**cb, "value": value, "sample": cb["sample"] + f"; median of {steps} timed passes"},
+            "e2e": {"value": value, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_fusion(args):
+    import torch
+    world, rank, local = dist_setup()
+    from sensemap_b200 import build as engine_build
+    from sensemap_b200.fusion import FusionImage, FusionOptions, StereoFusion
+    engine_build.build()
+    scene, ims, ov = fusion_set(args, rank, "cuda")
+    V = len(ims)
+
+    def placed(fn):
+        return [FusionImage(K=i.K, R=i.R, T=i.T, depth=fn(i.depth), normal=fn(i.normal), color=fn(i.color),
+                            is_rig=i.is_rig) for i in ims]
+
+    dev = placed(lambda a: torch.from_numpy(a).cuda())
+    host = placed(lambda a: torch.from_numpy(a).pin_memory())
+    opts = FusionOptions()
+    stream = torch.cuda.current_stream()
+    sptr = stream.cuda_stream
+
+    def step(images, fetch, profile=False):
+        f = StereoFusion(opts, images, ov, stream=sptr)
+        if profile:
+            f.SetProfiling(True)
+        f.Run()
+        out = None
+        if fetch:
+            pts = f.GetFusedPoints()
+            off, vis = f.VisibilityCSR()
+            out = (pts, off, vis)
+        return f, out
+
+    for _ in range(args.warmup):
+        f, _ = step(dev, False)
+        f.close()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    barrier(world)
+    torch.cuda.synchronize()
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    ev0.record(stream)
+    for _ in range(args.steps):
+        f, _ = step(dev, False)
+        launches += f.LaunchCount()
+        f.close()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop()
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    value = args.steps * V * world / (ms / 1000.0)
+
+    f, out = step(dev, True, profile=True)
+    prof = f.Profile()
+    npts = len(out[0])
+    f.close()
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    px = sum(int(i.depth.shape[0]) * int(i.depth.shape[1]) for i in ims)
+    # Closure launches read each traversable image's depth, point and normal
+    # maps and masks (29 B/px); summed over the images in fusion order, the
+    # k-th image's launch can reach the V - k images not fused yet.
+    clo_n, clo_ms = prof.get("closure", (1, float("nan")))
+    clo_bytes = sum(29 * px * (V - k) // V for k in range(V))
+    clo_gbs = clo_bytes / (clo_ms / 1000.0) / 1e9
+    roof = {"bound": "hbm", "achieved": clo_gbs, "peak": hbm, "unit": "GB/s", "frac": clo_gbs / hbm,
+            "traffic": None, "kernel": "ClosureKernel", "bytes_per_launch": clo_bytes / max(clo_n, 1),
+            "avg_launch_ms": clo_ms / max(clo_n, 1),
+            "bytes_model": "per image fused: depth + point + normal maps and masks of every image not fused yet "
+                           "read once (29 B/px)",
+            "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else "fallback 6650 GB/s",
+            "kernel_ms": {k: round(v[1], 3) for k, v in prof.items()},
+            "kernel_launches": {k: v[0] for k, v in prof.items()}}
+    e2e = None
+    if not args.no_e2e:
+        f, _ = step(host, True)
+        f.close()
+        torch.cuda.synchronize()
+        barrier(world)
+        e2e_steps = min(args.steps, 5)
+        t = time.perf_counter()
+        for _ in range(e2e_steps):
+            f, o = step(host, True)
+            f.close()
+        torch.cuda.synchronize()
+        el = max_over_ranks(time.perf_counter() - t, world)
+        h2d = sum(i.depth.numel() * 4 + i.normal.numel() * 4 + i.color.numel() for i in host)
+        d2h = sum(a.nbytes for a in o)
+        e2e = {"value": e2e_steps * V * world / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_fusion(ims, ov)
+    if rank == 0:
+        line = {"metric": FU_METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": f"fusion (StereoFusion image loop, default options), {V} views "
+                                       f"{args.width}x{args.height}, every other view overlapping; noisy "
+                                       f"ground-truth depth/normal maps of the heightfield scene",
+                           "global_batch": V * world, "parallelism": f"view sets sharded, {world} replica(s)",
+                           "l2": f"inputs larger than L2 ({V} x {args.width}x{args.height} depth, normal and "
+                                 f"color maps)"},
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clock_info,
+                "fusion": {"points": npts}}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -480,6 +480,94 @@ int smvs_select_views(const smvs_model_image* images, int num_images, const floa
 int smvs_compute_depth_ranges(const smvs_model_image* images, int num_images, const float bbox_lt[3],
                               const float bbox_rb[3], float* ranges);
 
+/* ---- fusion of depth maps into a point cloud ----------------------------- */
+/* StereoFusion (src/mvs/fusion.h:43-280, fusion.cc:648-2182): the image loop of
+ * Run (:1160-1215), FuseImage (:1730-1792) and Fuse (:1794-2182). Images are
+ * fused one after another in FindNextImage order (:697-727); in each image every
+ * seed pixel that is not yet fused starts a depth-first traversal over the
+ * overlapping images' pixels that agree with it in reprojection, depth and
+ * normal, and a cluster with enough pixels and images becomes one point (the
+ * medians of its pixels). Results are those of the reference run with one
+ * fusion thread per image slice taking its seeds in order (num_slices slices,
+ * one after another); the reference's concurrent slices race on the shared
+ * pixel masks and have no single result. */
+typedef struct smvs_fusion_options {
+  int step_size;               /* seed stride in rows and columns (1) */
+  int min_num_pixels;          /* >= 2 (5) */
+  int max_num_pixels;          /* (10000) */
+  int min_num_visible_images;  /* (3) */
+  int max_traversal_depth;     /* > 0 (100) */
+  double max_reproj_error;     /* pixels (2) */
+  double max_depth_error;      /* relative (0.01f) */
+  double max_normal_error;     /* degrees (10) */
+  int with_normal;             /* (1) */
+  int num_slices;              /* FuseImage's row slices, taken in order (1) */
+  int gpu_index;               /* (0) */
+} smvs_fusion_options;
+
+/* One image: size, K/R/T (mvs::Image) and its maps. A view without a depth
+ * map is not used (Run's Init, fusion.cc:979-990). */
+typedef struct smvs_fusion_view {
+  int width;
+  int height;
+  float K[9];
+  float R[9];
+  float T[3];
+  const float* depth;    /* W*H; NULL = image not used */
+  const float* normal;   /* 3*W*H planar (world normals are R^T n); needed with with_normal */
+  const uint8_t* color;  /* W*H*3 interleaved RGB (Bitmap::GetPixel); NULL reads black */
+  int is_rig;            /* Image::IsRig: FindNextImage prefers other images */
+} smvs_fusion_view;
+
+/* PlyPoint x/y/z, nx/ny/nz, r/g/b plus the point's score (fused_points_score_). */
+typedef struct smvs_fused_point {
+  float x, y, z;
+  float nx, ny, nz;   /* 0 without with_normal */
+  uint8_t r, g, b, pad;
+  float score;
+} smvs_fused_point;
+
+typedef struct smvs_fusion smvs_fusion;
+
+int smvs_fusion_options_default(smvs_fusion_options* opt);
+/* StereoFusion(options, ...) with the maps and the overlapping image lists
+ * (overlapping_images_, from Model::GetMaxOverlappingImages; CSR form
+ * overlap_offsets[num_views + 1], overlap_images) given directly. `memory` says
+ * where depth/normal/color live; host maps are copied before the call returns.
+ * The views together hold fewer than 2^31 pixels. */
+int smvs_fusion_create(const smvs_fusion_options* opt, const smvs_fusion_view* views, int num_views,
+                       const int32_t* overlap_offsets, const int32_t* overlap_images, int memory, void* stream,
+                       smvs_fusion** out);
+/* Fuses every used image (Run :1160-1215). Enqueues the work on the stream
+ * and waits for it. May be called once. */
+int smvs_fusion_run(smvs_fusion* f);
+/* Number of fused points and of visibility entries. */
+int smvs_fusion_get_sizes(smvs_fusion* f, size_t* num_points, size_t* num_visibility);
+/* GetFusedPoints / GetFusedPointsVisibility (:665-672) in the order the points
+ * were fused: points[num_points], visibility offsets[num_points + 1] and image
+ * indices, each point's images in ascending order (the reference lists them in
+ * std::unordered_set order). Any output may be NULL. */
+int smvs_fusion_get_points(smvs_fusion* f, smvs_fused_point* points, uint64_t* vis_offsets,
+                           uint32_t* vis_images);
+/* Device addresses of the same arrays (valid until destroy). */
+int smvs_fusion_get_device_points(smvs_fusion* f, const smvs_fused_point** points, const uint64_t** vis_offsets,
+                                  const uint32_t** vis_images);
+/* The images in the order they were fused (count <= num_views). */
+int smvs_fusion_get_image_order(smvs_fusion* f, int* order, int* count);
+/* fused_pixel_masks_ of a view after run: W*H bytes, 1 = fused. */
+int smvs_fusion_get_mask(smvs_fusion* f, int view, uint8_t* out);
+/* Kernel kinds of smvs_fusion_get_profile. */
+typedef enum smvs_fusion_kernel {
+  SMVS_FUSION_KERNEL_CLOSURE = 0,  /* candidate clusters of every seed of an image */
+  SMVS_FUSION_KERNEL_ORDER = 1,    /* claim lists, predecessors and the replay order */
+  SMVS_FUSION_KERNEL_REPLAY = 2,   /* the seeds' traversals in dependency order */
+  SMVS_FUSION_KERNEL_OTHER = 3     /* point maps, output compaction */
+} smvs_fusion_kernel;
+int smvs_fusion_set_profiling(smvs_fusion* f, int enable);
+int smvs_fusion_get_profile(smvs_fusion* f, int kind, int* count, double* total_ms);
+int64_t smvs_fusion_launch_count(smvs_fusion* f);
+void smvs_fusion_destroy(smvs_fusion* f);
+
 /* Thread-local message describing the last failure on this thread. */
 const char* smvs_last_error(void);
 

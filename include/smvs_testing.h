@@ -26,6 +26,13 @@ int smvs_test_sample_texture(const float* image, int w, int h, int storage, cons
  * `seconds`; synchronous. */
 int smvs_test_calibrate(int kind, double seconds, double* rate);
 
+/* Fusion capacities for the next smvs_fusion_create calls on this thread
+ * (0 restores the defaults): records of more than closure_cap pixels go
+ * through the overflow closure pass, and records of more than replay_cap
+ * pixels or replay_stack stack entries replay from global scratch instead of
+ * shared memory. Results do not change; the paths taken do. */
+int smvs_test_fusion_caps(int closure_cap, int replay_cap, int replay_stack);
+
 #ifdef __cplusplus
 }
 #endif

@@ -59,6 +59,17 @@ def lib():
                                          C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_init_from_dense_points.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
                                                  C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_fusion_run.restype = C.c_void_p
+        h.orc_fusion_run.argtypes = [C.POINTER(N.smvs_fusion_options), C.POINTER(N.smvs_fusion_view), C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_int]
+        h.orc_fusion_sizes.restype = C.c_int
+        h.orc_fusion_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
+        h.orc_fusion_copy.restype = C.c_int
+        h.orc_fusion_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_fusion_mask.restype = C.c_int
+        h.orc_fusion_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        h.orc_fusion_free.restype = None
+        h.orc_fusion_free.argtypes = [C.c_void_p]
         h.orc_cross_filter_poses.restype = C.c_int
         h.orc_cross_filter_poses.argtypes = [vp, C.c_int, pp, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = h
@@ -296,3 +307,37 @@ def init_from_dense_points(width, height, K, R, T, xyz, normals, level=2):
                                         len(x), int(level), d.ctypes.data, n.ctypes.data, r.ctypes.data):
         raise RuntimeError("orc_init_from_dense_points failed")
     return d, n, (r[0], r[1])
+
+
+def fusion_run(options, images, overlapping_images, max_images: int = 0, masks: bool = True) -> dict:
+    """StereoFusion's image loop on the CPU (smvs_oracle_fusion.c) with the
+    arguments of sensemap_b200.fusion.StereoFusion: points (structured array),
+    visibility CSR (vis_offsets, vis_images), the image order and each image's
+    fused-pixel mask."""
+    from sensemap_b200.fusion import fusion_structs
+    views, off, flat, memory, keep = fusion_structs(images, overlapping_images)
+    if memory != N.MEM_HOST:
+        raise ValueError("the oracle reads host arrays")
+    h = lib().orc_fusion_run(C.byref(options.to_c()), views, len(images), off.ctypes.data, flat.ctypes.data,
+                             int(max_images))
+    if not h:
+        raise ValueError("orc_fusion_run rejected its arguments")
+    try:
+        npts, nvis, nord = C.c_size_t(), C.c_size_t(), C.c_int()
+        lib().orc_fusion_sizes(h, C.byref(npts), C.byref(nvis), C.byref(nord))
+        pts = np.zeros(npts.value, dtype=N.FUSED_POINT_DTYPE)
+        voff = np.zeros(npts.value + 1, dtype=np.uint64)
+        vis = np.zeros(max(nvis.value, 1), dtype=np.uint32)
+        order = np.zeros(max(nord.value, 1), dtype=np.int32)
+        lib().orc_fusion_copy(h, pts.ctypes.data, voff.ctypes.data, vis.ctypes.data, order.ctypes.data)
+        out = {"points": pts, "vis_offsets": voff, "vis_images": vis[:nvis.value],
+               "order": [int(i) for i in order[:nord.value]]}
+        if masks:
+            out["masks"] = []
+            for k, v in enumerate(views):
+                m = np.zeros((v.height, v.width), dtype=np.uint8)
+                lib().orc_fusion_mask(h, k, v.width, v.height, m.ctypes.data)
+                out["masks"].append(m)
+        return out
+    finally:
+        lib().orc_fusion_free(h)

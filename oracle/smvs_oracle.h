@@ -94,6 +94,16 @@ int orc_init_from_mesh(const smvs_view* view, const double* vertices, size_t num
 int orc_init_from_dense_points(const smvs_view* view, const float* xyz, const float* normals, size_t n, int level,
                                float* depth, float* normal, float* range);
 
+/* ---- fusion (smvs_oracle_fusion.c) ---- */
+/* StereoFusion::Run for one cluster of every image; max_images > 0 stops after
+ * that many images. Returns a result handle, NULL on bad arguments or no memory. */
+void* orc_fusion_run(const smvs_fusion_options* opt, const smvs_fusion_view* views, int num_views,
+                     const int32_t* overlap_offsets, const int32_t* overlap_images, int max_images);
+int orc_fusion_sizes(void* h, size_t* num_points, size_t* num_vis, int* order_count);
+int orc_fusion_copy(void* h, smvs_fused_point* points, uint64_t* vis_offsets, uint32_t* vis_images, int* order);
+int orc_fusion_mask(void* h, int view, int width, int height, uint8_t* out);
+void orc_fusion_free(void* h);
+
 /* The generator shared with the engine: uniform in (0, 1]. */
 float orc_uniform(uint64_t seed, uint32_t stage, uint32_t pixel, uint32_t draw);
 

@@ -25,6 +25,8 @@ JOB_QUEUED, JOB_ACTIVE, JOB_DONE, JOB_FAILED = range(4)
 MAP_DEPTH, MAP_NORMAL, MAP_CONF, MAP_COST, MAP_VIEW_SEL = range(5)
 CF_KERNEL_RUN, CF_KERNEL_DEDUP, CF_KERNEL_OTHER = range(3)
 CF_KERNEL_NAMES = ["cross_filter", "dedup", "other"]
+FUSION_KERNEL_CLOSURE, FUSION_KERNEL_ORDER, FUSION_KERNEL_REPLAY, FUSION_KERNEL_OTHER = range(4)
+FUSION_KERNEL_NAMES = ["closure", "order", "replay", "other"]
 
 STATUS_NAMES = {0: "SMVS_OK", 1: "SMVS_EINVAL", 2: "SMVS_ENOMEM", 3: "SMVS_ECUDA", 4: "SMVS_ESTATE",
                 5: "SMVS_EIO", 6: "SMVS_ETIMEDOUT", 7: "SMVS_ECANCELED"}
@@ -121,6 +123,37 @@ class smvs_model_image(C.Structure):
     _fields_ = [("R", C.c_float * 9), ("T", C.c_float * 3), ("is_rig", C.c_int)]
 
 
+class smvs_fusion_options(C.Structure):
+    _fields_ = [
+        ("step_size", C.c_int), ("min_num_pixels", C.c_int), ("max_num_pixels", C.c_int),
+        ("min_num_visible_images", C.c_int), ("max_traversal_depth", C.c_int),
+        ("max_reproj_error", C.c_double), ("max_depth_error", C.c_double), ("max_normal_error", C.c_double),
+        ("with_normal", C.c_int), ("num_slices", C.c_int), ("gpu_index", C.c_int),
+    ]
+
+
+class smvs_fusion_view(C.Structure):
+    _fields_ = [
+        ("width", C.c_int), ("height", C.c_int),
+        ("K", C.c_float * 9), ("R", C.c_float * 9), ("T", C.c_float * 3),
+        ("depth", C.c_void_p), ("normal", C.c_void_p), ("color", C.c_void_p), ("is_rig", C.c_int),
+    ]
+
+
+class smvs_fused_point(C.Structure):
+    _fields_ = [
+        ("x", C.c_float), ("y", C.c_float), ("z", C.c_float),
+        ("nx", C.c_float), ("ny", C.c_float), ("nz", C.c_float),
+        ("r", C.c_uint8), ("g", C.c_uint8), ("b", C.c_uint8), ("pad", C.c_uint8),
+        ("score", C.c_float),
+    ]
+
+
+# numpy view of smvs_fused_point
+FUSED_POINT_DTYPE = [("x", "<f4"), ("y", "<f4"), ("z", "<f4"), ("nx", "<f4"), ("ny", "<f4"), ("nz", "<f4"),
+                     ("r", "u1"), ("g", "u1"), ("b", "u1"), ("pad", "u1"), ("score", "<f4")]
+
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "smvs_options_default": (C.c_int, [C.POINTER(smvs_options)]),
@@ -183,6 +216,20 @@ _SIGNATURES = {
                                     C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_void_p]),
     "smvs_compute_depth_ranges": (C.c_int, [C.POINTER(smvs_model_image), C.c_int, C.c_void_p, C.c_void_p,
                                             C.c_void_p]),
+    "smvs_fusion_options_default": (C.c_int, [C.POINTER(smvs_fusion_options)]),
+    "smvs_fusion_create": (C.c_int, [C.POINTER(smvs_fusion_options), C.POINTER(smvs_fusion_view), C.c_int,
+                                     C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_void_p)]),
+    "smvs_fusion_run": (C.c_int, [C.c_void_p]),
+    "smvs_fusion_get_sizes": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "smvs_fusion_get_points": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_fusion_get_device_points": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
+                                                C.POINTER(C.c_void_p)]),
+    "smvs_fusion_get_image_order": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "smvs_fusion_get_mask": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
+    "smvs_fusion_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
+    "smvs_fusion_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "smvs_fusion_launch_count": (C.c_int64, [C.c_void_p]),
+    "smvs_fusion_destroy": (None, [C.c_void_p]),
     "smvs_pool_options_default": (C.c_int, [C.POINTER(smvs_pool_options)]),
     "smvs_pool_create": (C.c_int, [C.POINTER(smvs_pool_options), C.c_void_p, C.POINTER(C.c_void_p)]),
     "smvs_pool_add_view": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(smvs_view), C.c_int]),
@@ -203,6 +250,7 @@ _SIGNATURES = {
     "smvs_test_sample_texture": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int,
                                            C.c_void_p]),
     "smvs_test_calibrate": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_double)]),
+    "smvs_test_fusion_caps": (C.c_int, [C.c_int, C.c_int, C.c_int]),
 }
 
 _LIB = None

@@ -24,9 +24,9 @@ NVCC_FLAGS = COMMON_FLAGS + ["--use_fast_math"]
 # Units whose kernels must reproduce IEEE single-precision results exactly
 # (no contraction into FMA, correctly rounded division and square root, no
 # flush to zero): the cross-view filter's decisions and medians, and the
-# depth tests of the initial maps.
+# depth tests of the initial maps, the fusion's consistency tests and medians.
 EXACT_FLAGS = COMMON_FLAGS + ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-EXACT_UNITS = {"smvs_cross_filter.cu", "smvs_init_maps.cu"}
+EXACT_UNITS = {"smvs_cross_filter.cu", "smvs_init_maps.cu", "smvs_fusion.cu"}
 
 
 def _nvcc() -> str:

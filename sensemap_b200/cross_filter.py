@@ -19,7 +19,7 @@ from typing import Sequence
 import numpy as np
 
 from . import _native as N
-from .patch_match import PatchMatchOptions, Problem, _addr, _is_cuda_tensor
+from .patch_match import PatchMatchOptions, Problem, _addr, _is_cuda_tensor, _sync_producers
 
 
 class CrossFilterCuda:
@@ -74,6 +74,7 @@ class CrossFilterCuda:
             n_used += 1
         handle = C.c_void_p()
         memory = N.MEM_DEVICE if memories == {True} else N.MEM_HOST
+        _sync_producers(keep, stream)
         stream_ptr = C.c_void_p(int(stream)) if stream is not None else None
         N.check(N.lib().smvs_cross_filter_create(C.byref(options.to_c()), views, len(self.whole_ids), probs, n_used,
                                                  memory, stream_ptr, C.byref(handle)))

@@ -1,0 +1,1614 @@
+// smvs_fusion.cu — fusion of depth maps into a point cloud (StereoFusion).
+//
+// StereoFusion's image loop (SenseMap src/mvs/fusion.cc:1160-1215), FuseImage
+// (:1730-1792) and Fuse (:1794-2182) on the GPU, with the results of the
+// reference run seed after seed (its fusion threads' row slices taken one
+// after another). Compiled with -fmad=false -prec-div=true -prec-sqrt=true
+// -ftz=false: the same IEEE single-precision operations, in the same order, as
+// the reference's Eigen expressions (see the float helpers below).
+//
+// Each image is fused in five steps, all in stream order:
+//   1. closure: every seed pixel (one thread each) collects the pixels its
+//      traversal could ever accept — those that pass its reprojection, depth
+//      and normal tests, are not fused yet and are reachable from it through
+//      such pixels — with the push lists between them (the seed's record);
+//   2. claims: for every pixel the seeds whose records hold it, sorted; each
+//      seed's predecessor on each of its pixels is the previous claimant;
+//   3. order: a ticket order in which every predecessor comes first (the seed
+//      grid sheared so that key = column + K x row grows along every
+//      predecessor pair);
+//   4. replay: warps take tickets, wait for their predecessors, read the masks
+//      of their record's pixels, replay the reference's depth-first traversal
+//      (explicit stack, limits) on the record, mark the accepted pixels, and
+//      release their successors; then they compute the fused point (medians);
+//   5. compaction of the points in seed order.
+// A traversal only reads or writes the masks of pixels that pass its tests
+// (a pixel that fails them is skipped whether or not it is fused), so two
+// seeds whose records share no pixel commute, and waiting for every earlier
+// claimant of each pixel reproduces the sequential order exactly.
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/smvs.h"
+#include "../../include/smvs_testing.h"
+
+extern "C" void smvs_internal_set_error(const char* msg);
+cudaMemPool_t smvs_internal_device_pool(int device);
+
+namespace {
+
+constexpr int kBlank = 3;              // blank_size (fusion.cc:1757, :1831)
+constexpr int kCap = 256;              // record capacity of the closure pass (pixels)
+constexpr int kBigCap = 65535;         // record capacity of the overflow pass (u16 indices)
+constexpr int kBigBatch = 256;         // overflow seeds per launch
+// Scratch bytes of one overflow thread: gid (u32) | derr (f32) | vid (u16),
+// rounded to 16 so every thread's arrays stay aligned.
+constexpr size_t kBigStride = ((size_t)kBigCap * 10u + 15u) & ~(size_t)15u;
+constexpr uint32_t kEmpty = 0xffffffffu;
+constexpr uint32_t kOver = 0xfffffffeu;
+constexpr int kReplayWarps = 8;        // warps per replay block
+constexpr int kStackSh = 512;          // replay stack entries kept in shared memory per warp
+constexpr int kScanItems = 4096;       // items per scan block (256 threads x 16)
+constexpr unsigned long long kWaitLimitNs = 20ull * 1000 * 1000 * 1000;  // bounded waits: 20 s
+
+// Status bits written by the kernels.
+constexpr uint32_t kStTimeout = 1u, kStPool = 2u, kStBad = 4u;
+
+int Fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  smvs_internal_set_error(buf);
+  return code;
+}
+
+#define FU_CUDA(call)                                                                                      \
+  do {                                                                                                     \
+    cudaError_t e_ = (call);                                                                               \
+    if (e_ != cudaSuccess) return Fail(SMVS_ECUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+// One image as the kernels see it.
+struct FView {
+  float P[12];   // K [R | T], ComposeProjectionMatrix (src/mvs/utils.cc:35-42)
+  float iP[12];  // top rows of [P; 0 0 0 1]^-1 (double inverse rounded once)
+  int W, H;
+  uint32_t base;  // first pixel of the image in the concatenated arrays
+  int ov_begin, ov_end;
+  int pad;
+};
+
+// Per-pixel arrays of all images, concatenated.
+struct FMaps {
+  const FView* views;
+  const int* ov;          // overlapping_images_, concatenated
+  const uint8_t* trav;    // per image: used and not yet fused
+  const float* D;         // depth
+  const float* X;         // inv_P * (col d, row d, d, 1) (fusion.cc:1953-1955)
+  const float* Y;
+  const float* Z;
+  const float* NX;        // inv_R * normal (:1939-1941)
+  const float* NY;
+  const float* NZ;
+  const float* G;         // red-channel gradient (:2007-2021)
+  const uint8_t* rgb;     // W*H*3 per image
+  uint8_t* mask;          // fused_pixel_masks_
+};
+
+struct FConsts {
+  float max_sq_reproj;  // max_squared_reproj_error_ (float)
+  float min_cos;        // min_cos_normal_error_ (float)
+  float derr_thr;       // largest float <= max_depth_error: x > derr_thr <=> (double)x > max_depth_error
+  double max_depth_error;
+  int with_normal, min_pix, max_pix, max_depth, min_vis;
+};
+
+struct FImage {
+  int view;
+  int cap;  // closure capacity of the fast pass (<= kCap)
+  int Rs, Cs, step;
+  uint32_t nseeds;
+  const int* rows;  // Rs image rows of the seed grid
+};
+
+// Record pool of one image. A record (u32 words): cnt, nE, gid[cnt], derr[cnt],
+// pred[cnt], eoff[cnt + 1], vid[cnt] (u16), edges[nE bound] (u16).
+struct FRecs {
+  uint32_t* pool;
+  unsigned long long pool_words;
+  unsigned long long* used;   // bump cursor (words)
+  uint32_t* rec_off;          // per seed: word offset, kEmpty or kOver
+  uint32_t* over_list;        // seeds over kCap
+  uint32_t* n_over;
+  uint32_t* stats;            // [0] max cnt, [1] max nE, [2] status
+};
+
+__host__ __device__ inline uint32_t RecWords(uint32_t cnt, uint32_t ebound) {
+  return 2u + 3u * cnt + (cnt + 1u) + (cnt + 1u) / 2u + (ebound + 1u) / 2u;
+}
+
+// Bytes of one replay warp's scratch region: stack (u32) | vals (f32) | ids (u32)
+// | acc (u16) | flags (u8), rounded to 16.
+__host__ __device__ inline size_t ScratchPer(uint32_t cnt, uint32_t stack) {
+  return ((size_t)stack * 4u + (size_t)cnt * 11u + 31u) & ~(size_t)15u;
+}
+
+// ---- float helpers: the reference's Eigen evaluation order ----------------
+// A 3x4 row-major matrix times a Vector4f: one SSE packet product reduced as
+// (p0 + p2) + (p1 + p3) (Eigen's predux).
+__device__ __forceinline__ float Dot4p(const float* a, float x, float y, float z, float w) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a[0], x), __fmul_rn(a[2], z)), __fadd_rn(__fmul_rn(a[1], y), __fmul_rn(a[3], w)));
+}
+// P * xyz.homogeneous(): the 3x3 block product plus the last column.
+__device__ __forceinline__ float Dot3h(const float* a, float x, float y, float z) {
+  return __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(a[0], x), __fmul_rn(a[1], y)), __fmul_rn(a[2], z)), a[3]);
+}
+// Vector3f dot product / 3x3 times Vector3f row.
+__device__ __forceinline__ float Dot3(float a0, float a1, float a2, float x, float y, float z) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a0, x), __fmul_rn(a1, y)), __fmul_rn(a2, z));
+}
+__device__ __forceinline__ bool ValidDepth(float d) { return d > 0.0f && isfinite(d); }
+// Total order of floats (sign first): the order the medians use.
+__device__ __forceinline__ uint32_t FKey(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// Rounded projection of a point into image u (fusion.cc:2080-2091); false if
+// it falls outside the blank border.
+__device__ __forceinline__ bool ProjectPixel(const FView& fu, float x, float y, float z, int* row, int* col) {
+  const float q0 = Dot3h(fu.P, x, y, z), q1 = Dot3h(fu.P + 4, x, y, z), q2 = Dot3h(fu.P + 8, x, y, z);
+  const float uc = roundf(__fdiv_rn(q0, q2)), ur = roundf(__fdiv_rn(q1, q2));
+  if (!(uc >= (float)kBlank && ur >= (float)kBlank && uc < (float)(fu.W - kBlank) && ur < (float)(fu.H - kBlank)))
+    return false;
+  *col = (int)uc;
+  *row = (int)ur;
+  return true;
+}
+
+// ---- point maps -------------------------------------------------------------
+__global__ void PointMapKernel(FView v, float R0, float R1, float R2, float R3, float R4, float R5, float R6,
+                               float R7, float R8, const float* __restrict__ normal_in, int with_normal,
+                               int has_color, float* D, float* X, float* Y, float* Z, float* NX, float* NY,
+                               float* NZ, float* G, const uint8_t* __restrict__ rgb) {
+  const uint32_t plane = (uint32_t)v.W * (uint32_t)v.H;
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < plane; p += gridDim.x * blockDim.x) {
+    const int row = (int)(p / (uint32_t)v.W), col = (int)(p - (uint32_t)row * (uint32_t)v.W);
+    const uint32_t g = v.base + p;
+    const float d = D[g];
+    const float cd = __fmul_rn((float)col, d), rd = __fmul_rn((float)row, d);
+    X[g] = Dot4p(v.iP, cd, rd, d, 1.0f);
+    Y[g] = Dot4p(v.iP + 4, cd, rd, d, 1.0f);
+    Z[g] = Dot4p(v.iP + 8, cd, rd, d, 1.0f);
+    if (with_normal) {
+      const float n0 = normal_in[p], n1 = normal_in[plane + p], n2 = normal_in[2 * plane + p];
+      // inv_R = R^T: row i of inv_R is column i of R.
+      NX[g] = Dot3(R0, R3, R6, n0, n1, n2);
+      NY[g] = Dot3(R1, R4, R7, n0, n1, n2);
+      NZ[g] = Dot3(R2, R5, R8, n0, n1, n2);
+    }
+    float grad = 0.0f;
+    if (has_color && col > 1 && col < v.W - 1 && row > 1 && row < v.H - 1) {
+      const uint8_t* px = rgb + 3ull * g;
+      const float gx = __fdiv_rn((float)((int)px[-3] - (int)px[3]), 255.0f);
+      const float gy = __fdiv_rn((float)((int)px[-3 * v.W] - (int)px[3 * v.W]), 255.0f);
+      grad = __fsqrt_rn(__fadd_rn(__fmul_rn(gx, gx), __fmul_rn(gy, gy)));
+    }
+    G[g] = grad;
+  }
+}
+
+// ---- closure ---------------------------------------------------------------
+// The pixels the seed's traversal can accept (see the file comment) into
+// gid/vid/derr; returns their count, 0 when the seed itself is fused or has no
+// valid depth, -1 when there are more than `cap`.
+__device__ __forceinline__ int BuildClosure(const FMaps& m, const FConsts& c, uint32_t sg, int sv, uint32_t* gid,
+                                            uint16_t* vid, float* derr, int cap) {
+  if (m.mask[sg]) return 0;
+  if (!ValidDepth(m.D[sg])) return 0;
+  const float sx = m.X[sg], sy = m.Y[sg], sz = m.Z[sg];
+  float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+  if (c.with_normal) {
+    s0 = m.NX[sg];
+    s1 = m.NY[sg];
+    s2 = m.NZ[sg];
+  }
+  gid[0] = sg;
+  vid[0] = (uint16_t)sv;
+  derr[0] = 0.0f;
+  int cnt = 1;
+  for (int i = 0; i < cnt; ++i) {
+    const uint32_t g = gid[i];
+    const FView& fv = m.views[vid[i]];
+    const float x = m.X[g], y = m.Y[g], z = m.Z[g];
+    for (int k = fv.ov_begin; k < fv.ov_end; ++k) {
+      const int u = m.ov[k];
+      if (!m.trav[u]) continue;
+      const FView& fu = m.views[u];
+      int row, col;
+      if (!ProjectPixel(fu, x, y, z, &row, &col)) continue;
+      const uint32_t q = fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col;
+      if (m.mask[q]) continue;
+      bool seen = false;
+      for (int j = 0; j < cnt; ++j)
+        if (gid[j] == q) {
+          seen = true;
+          break;
+        }
+      if (seen) continue;
+      const float dq = m.D[q];
+      if (!ValidDepth(dq)) continue;
+      // Reprojection and depth error of the seed point in image u (:1893-1912).
+      const float p0 = Dot4p(fu.P, sx, sy, sz, 1.0f), p1 = Dot4p(fu.P + 4, sx, sy, sz, 1.0f),
+                  p2 = Dot4p(fu.P + 8, sx, sy, sz, 1.0f);
+      const float cdiff = __fsub_rn(__fdiv_rn(p0, p2), (float)col);
+      const float rdiff = __fsub_rn(__fdiv_rn(p1, p2), (float)row);
+      const float sq = __fadd_rn(__fmul_rn(cdiff, cdiff), __fmul_rn(rdiff, rdiff));
+      if (sq > c.max_sq_reproj) continue;
+      const float de = __fdiv_rn(fabsf(__fsub_rn(p2, dq)), dq);
+      if (de > c.derr_thr) continue;
+      if (c.with_normal && Dot3(s0, s1, s2, m.NX[q], m.NY[q], m.NZ[q]) < c.min_cos) continue;  // :1944-1948
+      if (cnt == cap) return -1;
+      gid[cnt] = q;
+      vid[cnt] = (uint16_t)u;
+      derr[cnt] = de;
+      ++cnt;
+    }
+  }
+  return cnt;
+}
+
+// Writes the record of a closure; false when the pool is full.
+__device__ bool WriteRecord(const FMaps& m, const FRecs& r, uint32_t seed, const uint32_t* gid, const uint16_t* vid,
+                            const float* derr, int cnt) {
+  uint32_t ebound = 0;
+  for (int i = 0; i < cnt; ++i) {
+    const FView& fv = m.views[vid[i]];
+    ebound += (uint32_t)(fv.ov_end - fv.ov_begin);
+  }
+  const uint32_t words = RecWords((uint32_t)cnt, ebound);
+  const unsigned long long off = atomicAdd(r.used, (unsigned long long)words);
+  if (off + words > r.pool_words || off + words > 0xfffffff0ull) {
+    atomicOr(&r.stats[2], kStPool);
+    r.rec_off[seed] = kEmpty;
+    return false;
+  }
+  uint32_t* rec = r.pool + off;
+  uint32_t* rg = rec + 2;
+  float* rd = reinterpret_cast<float*>(rg + cnt);
+  int32_t* rp = reinterpret_cast<int32_t*>(rd + cnt);
+  uint32_t* eoff = reinterpret_cast<uint32_t*>(rp + cnt);
+  uint16_t* rv = reinterpret_cast<uint16_t*>(eoff + cnt + 1);
+  uint16_t* edges = rv + 2 * ((cnt + 1) / 2);
+  for (int i = 0; i < cnt; ++i) {
+    rg[i] = gid[i];
+    rd[i] = derr[i];
+    rp[i] = -1;
+    rv[i] = vid[i];
+  }
+  // Push lists between record pixels, in the reference's push order
+  // (overlapping_images_ of the pixel's image, :2073-2092).
+  uint32_t e = 0;
+  for (int i = 0; i < cnt; ++i) {
+    eoff[i] = e;
+    const uint32_t g = gid[i];
+    const FView& fv = m.views[vid[i]];
+    const float x = m.X[g], y = m.Y[g], z = m.Z[g];
+    for (int k = fv.ov_begin; k < fv.ov_end; ++k) {
+      const int u = m.ov[k];
+      if (!m.trav[u]) continue;
+      const FView& fu = m.views[u];
+      int row, col;
+      if (!ProjectPixel(fu, x, y, z, &row, &col)) continue;
+      const uint32_t q = fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col;
+      for (int j = 0; j < cnt; ++j)
+        if (gid[j] == q) {
+          if (e < ebound) edges[e] = (uint16_t)j;
+          ++e;
+          break;
+        }
+    }
+  }
+  eoff[cnt] = e;
+  rec[0] = (uint32_t)cnt;
+  rec[1] = e;
+  if (e > ebound) atomicOr(&r.stats[2], kStBad);
+  r.rec_off[seed] = (uint32_t)off;
+  atomicMax(&r.stats[0], (uint32_t)cnt);
+  atomicMax(&r.stats[1], e);
+  return true;
+}
+
+__device__ __forceinline__ uint32_t SeedPixel(const FMaps& m, const FImage& im, uint32_t s) {
+  const uint32_t i = s / (uint32_t)im.Cs, j = s - i * (uint32_t)im.Cs;
+  const FView& fv = m.views[im.view];
+  const uint32_t row = (uint32_t)im.rows[i], col = (uint32_t)(kBlank + (int)j * im.step);
+  return fv.base + row * (uint32_t)fv.W + col;
+}
+
+__global__ void __launch_bounds__(128) ClosureKernel(FMaps m, FConsts c, FImage im, FRecs r) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= im.nseeds) return;
+  uint32_t gid[kCap];
+  uint16_t vid[kCap];
+  float derr[kCap];
+  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, im.cap);
+  if (cnt == 0) {
+    r.rec_off[s] = kEmpty;
+    return;
+  }
+  if (cnt < 0) {
+    r.rec_off[s] = kOver;
+    const uint32_t k = atomicAdd(r.n_over, 1u);
+    r.over_list[k] = s;
+    return;
+  }
+  WriteRecord(m, r, s, gid, vid, derr, cnt);
+}
+
+// Seeds over kCap, with their scratch in global memory.
+__global__ void __launch_bounds__(64) ClosureBigKernel(FMaps m, FConsts c, FImage im, FRecs r, uint32_t first,
+                                                       uint32_t count, uint8_t* scratch) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const uint32_t s = r.over_list[first + t];
+  uint8_t* base = scratch + (size_t)t * kBigStride;
+  uint32_t* gid = reinterpret_cast<uint32_t*>(base);
+  float* derr = reinterpret_cast<float*>(base + (size_t)kBigCap * 4u);
+  uint16_t* vid = reinterpret_cast<uint16_t*>(base + (size_t)kBigCap * 8u);
+  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, kBigCap);
+  if (cnt <= 0) {  // cannot be empty here; over kBigCap is reported
+    if (cnt < 0) atomicOr(&r.stats[2], kStBad);
+    r.rec_off[s] = kEmpty;
+    return;
+  }
+  WriteRecord(m, r, s, gid, vid, derr, cnt);
+}
+
+// ---- claims and predecessors ------------------------------------------------
+struct RecView {
+  uint32_t cnt, ne;
+  const uint32_t* gid;
+  const float* derr;
+  int32_t* pred;
+  const uint32_t* eoff;
+  const uint16_t* vid;
+  const uint16_t* edges;
+};
+
+__device__ __forceinline__ RecView OpenRecord(uint32_t* pool, uint32_t off) {
+  RecView v;
+  uint32_t* rec = pool + off;
+  v.cnt = rec[0];
+  v.ne = rec[1];
+  v.gid = rec + 2;
+  v.derr = reinterpret_cast<const float*>(v.gid + v.cnt);
+  v.pred = reinterpret_cast<int32_t*>(rec + 2 + 2 * v.cnt);
+  v.eoff = rec + 2 + 3 * v.cnt;
+  v.vid = reinterpret_cast<const uint16_t*>(v.eoff + v.cnt + 1);
+  v.edges = v.vid + 2 * ((v.cnt + 1) / 2);
+  return v;
+}
+
+__global__ void ClaimCountKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseeds) return;
+  const uint32_t off = r.rec_off[s];
+  if (off >= kOver) return;
+  const RecView v = OpenRecord(r.pool, off);
+  for (uint32_t k = 0; k < v.cnt; ++k) atomicAdd(&claim_cnt[v.gid[k]], 1u);
+}
+
+__global__ void ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt, const uint32_t* claim_off,
+                                uint32_t* claim_list) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseeds) return;
+  const uint32_t off = r.rec_off[s];
+  if (off >= kOver) return;
+  const RecView v = OpenRecord(r.pool, off);
+  for (uint32_t k = 0; k < v.cnt; ++k) {
+    const uint32_t g = v.gid[k];
+    const uint32_t slot = atomicSub(&claim_cnt[g], 1u) - 1u;  // leaves claim_cnt at zero
+    claim_list[claim_off[g] + slot] = s;
+  }
+}
+
+__global__ void ClaimSortKernel(const uint32_t* claim_off, uint32_t total, uint32_t* claim_list) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+    const uint32_t a = claim_off[g], b = claim_off[g + 1];
+    for (uint32_t i = a + 1; i < b; ++i) {
+      const uint32_t x = claim_list[i];
+      uint32_t j = i;
+      while (j > a && claim_list[j - 1] > x) {
+        claim_list[j] = claim_list[j - 1];
+        --j;
+      }
+      claim_list[j] = x;
+    }
+  }
+}
+
+// Predecessor of each (seed, pixel) and the shear K of the ticket order:
+// key(p) < key(s) for every predecessor p of s needs K (i_s - i_p) > j_p - j_s.
+__global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* claim_off, const uint32_t* claim_list,
+                           int* shear) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseeds) return;
+  const uint32_t off = r.rec_off[s];
+  if (off >= kOver) return;
+  RecView v = OpenRecord(r.pool, off);
+  const int is = (int)(s / (uint32_t)Cs), js = (int)(s - (uint32_t)is * (uint32_t)Cs);
+  int need = 1;
+  for (uint32_t k = 0; k < v.cnt; ++k) {
+    const uint32_t g = v.gid[k];
+    uint32_t lo = claim_off[g], hi = claim_off[g + 1];
+    const uint32_t a = lo;
+    while (lo < hi) {  // first entry >= s
+      const uint32_t mid = (lo + hi) >> 1;
+      if (claim_list[mid] < s) lo = mid + 1; else hi = mid;
+    }
+    if (lo >= claim_off[g + 1] || claim_list[lo] != s) {
+      atomicOr(&r.stats[2], kStBad);
+      v.pred[k] = -1;
+      continue;
+    }
+    if (lo == a) {
+      v.pred[k] = -1;
+      continue;
+    }
+    const uint32_t p = claim_list[lo - 1];
+    v.pred[k] = (int32_t)p;
+    const int ip = (int)(p / (uint32_t)Cs), jp = (int)(p - (uint32_t)ip * (uint32_t)Cs);
+    if (ip < is) {
+      const int num = jp - js, den = is - ip;
+      const int fl = num >= 0 ? num / den : -((-num + den - 1) / den);
+      need = max(need, fl + 1);
+    }
+  }
+  if (need > 1) atomicMax(shear, min(need, Cs));
+}
+
+// ---- ticket order ------------------------------------------------------------
+__device__ __forceinline__ int KeyRowMin(long long k, int Cs, int K) {
+  const long long num = k - Cs + 1;
+  return num <= 0 ? 0 : (int)((num + K - 1) / K);
+}
+
+__global__ void KeyCountKernel(uint32_t nkeys_cap, int Rs, int Cs, const int* shear, uint32_t* keycnt) {
+  const int K = *shear;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < nkeys_cap; k += gridDim.x * blockDim.x) {
+    const int imin = KeyRowMin(k, Cs, K);
+    const int imax = min(Rs - 1, (int)(k / (uint32_t)K));
+    keycnt[k] = imax >= imin ? (uint32_t)(imax - imin + 1) : 0u;
+  }
+}
+
+__global__ void SeqKernel(uint32_t nseeds, int Cs, const int* shear, const uint32_t* keyoff, uint32_t* seq) {
+  const int K = *shear;
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseeds) return;
+  const int i = (int)(s / (uint32_t)Cs), j = (int)(s - (uint32_t)i * (uint32_t)Cs);
+  const long long k = (long long)j + (long long)K * i;
+  seq[keyoff[k] + (uint32_t)(i - KeyRowMin(k, Cs, K))] = s;
+}
+
+// ---- replay -----------------------------------------------------------------
+struct FReplay {
+  const uint32_t* seq;
+  uint32_t nseeds;
+  uint32_t* done;
+  unsigned int* ticket;
+  smvs_fused_point* slot_pts;
+  uint32_t* slot_has;
+  uint32_t* slot_nvis;
+  uint32_t* slot_visoff;
+  uint32_t* vis_pool;
+  unsigned long long* vis_cursor;
+  uint8_t* scratch;           // per-warp scratch for records over the shared budget
+  uint32_t scratch_cnt;       // node capacity of a scratch region
+  uint32_t scratch_stack;     // stack capacity of a scratch region
+  int shared_cnt;             // records up to this many pixels ...
+  int shared_stack;           // ... and stack entries replay in shared memory
+};
+
+struct WarpShared {
+  uint32_t stack[kStackSh];
+  float vals[kCap];
+  uint32_t ids[kCap];
+  uint16_t acc[kCap];
+  uint8_t flags[kCap];
+  float med[2];
+  int nacc;
+};
+
+__device__ __forceinline__ uint32_t LoadAcquire(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void StoreRelease(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long GlobalTimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Median over vals[0..n) (internal::Median, fusion.cc:47-60) in the total
+// order of FKey; ties between equal keys are broken by position.
+__device__ float WarpMedian(const float* vals, int n, float* med, int lane) {
+  const int mid = n / 2;
+  for (int i = lane; i < n; i += 32) {
+    const uint32_t ki = FKey(vals[i]);
+    int rank = 0;
+    for (int j = 0; j < n; ++j) {
+      const uint32_t kj = FKey(vals[j]);
+      rank += (kj < ki || (kj == ki && j < i)) ? 1 : 0;
+    }
+    if (rank == mid) med[0] = vals[i];
+    if ((n & 1) == 0 && rank == mid - 1) med[1] = vals[i];
+  }
+  __syncwarp();
+  const float r = (n & 1) ? med[0] : __fdiv_rn(__fadd_rn(med[0], med[1]), 2.0f);
+  __syncwarp();
+  return r;
+}
+
+__global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FConsts c, FRecs r, FReplay rp) {
+  __shared__ WarpShared shm[kReplayWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  WarpShared& sh = shm[w];
+  const size_t gw = (size_t)blockIdx.x * kReplayWarps + w;
+  for (;;) {
+    uint32_t t = 0;
+    if (lane == 0) t = atomicAdd(rp.ticket, 1u);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= rp.nseeds) break;
+    const uint32_t s = rp.seq[t];
+    const uint32_t off = r.rec_off[s];
+    if (off >= kOver) continue;  // no record: nothing to fuse, nobody waits for it
+    const RecView v = OpenRecord(r.pool, off);
+    const int cnt = (int)v.cnt;
+    // Storage: shared memory, or this warp's scratch for large records.
+    uint8_t* flags;
+    uint16_t* acc;
+    uint32_t* stack;
+    float* vals;
+    uint32_t* ids;
+    if (cnt <= rp.shared_cnt && v.ne + 1 <= (uint32_t)rp.shared_stack) {
+      flags = sh.flags;
+      acc = sh.acc;
+      stack = sh.stack;
+      vals = sh.vals;
+      ids = sh.ids;
+    } else {
+      if ((uint32_t)cnt > rp.scratch_cnt || v.ne + 1 > rp.scratch_stack || !rp.scratch) {
+        if (lane == 0) {
+          atomicOr(&r.stats[2], kStBad);
+          StoreRelease(&rp.done[s], 1u);
+        }
+        continue;
+      }
+      uint8_t* base = rp.scratch + gw * ScratchPer(rp.scratch_cnt, rp.scratch_stack);
+      stack = reinterpret_cast<uint32_t*>(base);
+      vals = reinterpret_cast<float*>(base + (size_t)rp.scratch_stack * 4u);
+      ids = reinterpret_cast<uint32_t*>(base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 4u);
+      acc = reinterpret_cast<uint16_t*>(base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 8u);
+      flags = base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 10u;
+    }
+    // Wait for the predecessors (every earlier seed that may touch these pixels).
+    for (int k = lane; k < cnt; k += 32) {
+      const int32_t p = v.pred[k];
+      if (p < 0) continue;
+      const unsigned long long t0 = GlobalTimer();
+      unsigned ns = 32;
+      while (LoadAcquire(&rp.done[p]) == 0u) {
+        __nanosleep(ns);
+        ns = ns < 256 ? ns * 2 : 256;
+        if (GlobalTimer() - t0 > kWaitLimitNs) {
+          atomicOr(&r.stats[2], kStTimeout);
+          break;
+        }
+      }
+    }
+    __syncwarp();
+    __threadfence();
+    for (int k = lane; k < cnt; k += 32) flags[k] = *(volatile const uint8_t*)(m.mask + v.gid[k]);
+    __syncwarp();
+    // The reference's traversal (:1836-2094) on the record: LIFO stack of
+    // (pixel, traversal depth); a pushed pixel that is already fused would be
+    // skipped when popped, so it is not pushed.
+    if (lane == 0) {
+      int nacc = 0, top = 0;
+      if (!flags[0]) stack[top++] = 0u;
+      while (top > 0) {
+        const uint32_t e = stack[--top];
+        const uint32_t k = e & 0xffffu, d = e >> 16;
+        if (flags[k]) continue;
+        flags[k] = 1;
+        acc[nacc++] = (uint16_t)k;
+        if (nacc >= c.max_pix) break;
+        if ((int)d + 1 >= c.max_depth) continue;
+        const uint32_t nd = d + 1 < 0xffffu ? d + 1 : 0xffffu;
+        for (uint32_t q = v.eoff[k]; q < v.eoff[k + 1]; ++q) {
+          const uint32_t j = v.edges[q];
+          if (!flags[j]) stack[top++] = j | (nd << 16);
+        }
+      }
+      sh.nacc = nacc;
+    }
+    __syncwarp();
+    const int n = sh.nacc;
+    for (int i = lane; i < n; i += 32) *(volatile uint8_t*)(m.mask + v.gid[acc[i]]) = 1;
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) StoreRelease(&rp.done[s], 1u);
+    // The fused point (:2098-2180).
+    if (n < c.min_pix) continue;
+    // Images of the cluster, ascending.
+    for (int i = lane; i < n; i += 32) ids[i] = v.vid[acc[i]];
+    __syncwarp();
+    int nvis = 0;
+    for (int i0 = 0; i0 < n; i0 += 32) {
+      const int i = i0 + lane;
+      bool first = false;
+      if (i < n) {
+        first = true;
+        for (int j = 0; j < i; ++j)
+          if (ids[j] == ids[i]) {
+            first = false;
+            break;
+          }
+      }
+      nvis += __popc(__ballot_sync(0xffffffffu, first));
+    }
+    if (nvis < c.min_vis) continue;
+    smvs_fused_point pt;
+    memset(&pt, 0, sizeof(pt));
+    const float* maps[3] = {m.X, m.Y, m.Z};
+    float xyz[3];
+    for (int a = 0; a < 3; ++a) {
+      for (int i = lane; i < n; i += 32) vals[i] = maps[a][v.gid[acc[i]]];
+      __syncwarp();
+      xyz[a] = WarpMedian(vals, n, sh.med, lane);
+    }
+    if (!isfinite(xyz[0]) || !isfinite(xyz[1]) || !isfinite(xyz[2])) continue;
+    pt.x = xyz[0];
+    pt.y = xyz[1];
+    pt.z = xyz[2];
+    if (c.with_normal) {
+      const float* nmaps[3] = {m.NX, m.NY, m.NZ};
+      float fn[3];
+      for (int a = 0; a < 3; ++a) {
+        for (int i = lane; i < n; i += 32) vals[i] = nmaps[a][v.gid[acc[i]]];
+        __syncwarp();
+        fn[a] = WarpMedian(vals, n, sh.med, lane);
+      }
+      const float norm =
+          __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(fn[0], fn[0]), __fmul_rn(fn[1], fn[1])), __fmul_rn(fn[2], fn[2])));
+      if (norm < 1.1920928955078125e-07f) continue;  // FLT_EPSILON
+      pt.nx = __fdiv_rn(fn[0], norm);
+      pt.ny = __fdiv_rn(fn[1], norm);
+      pt.nz = __fdiv_rn(fn[2], norm);
+    }
+    uint8_t rgb[3];
+    for (int ch = 0; ch < 3; ++ch) {
+      for (int i = lane; i < n; i += 32) vals[i] = (float)m.rgb[3ull * v.gid[acc[i]] + ch];
+      __syncwarp();
+      float med = roundf(WarpMedian(vals, n, sh.med, lane));
+      med = med < 255.0f ? med : 255.0f;  // TruncateCast<float, uint8_t>
+      med = med > 0.0f ? med : 0.0f;
+      rgb[ch] = (uint8_t)med;
+    }
+    pt.r = rgb[0];
+    pt.g = rgb[1];
+    pt.b = rgb[2];
+    // Mean gradient in traversal order, then the score (:2157-2166).
+    for (int i = lane; i < n; i += 32) vals[i] = m.G[v.gid[acc[i]]];
+    __syncwarp();
+    float m_conf = 0.0f;
+    if (lane == 0) {
+      for (int i = 0; i < n; ++i) m_conf = __fadd_rn(m_conf, vals[i]);
+      m_conf = __fdiv_rn(m_conf, (float)n);
+    }
+    m_conf = __shfl_sync(0xffffffffu, m_conf, 0);
+    if (nvis >= 3) m_conf = 1.0f;
+    m_conf = __fsub_rn(1.0f, m_conf);
+    __syncwarp();
+    for (int i = lane + 1; i < n; i += 32) vals[i - 1] = v.derr[acc[i]];
+    __syncwarp();
+    const float med_err = WarpMedian(vals, n - 1, sh.med, lane);
+    float score = (float)((double)med_err / c.max_depth_error);
+    const float mixed = __fadd_rn(__fmul_rn(0.6f, score), __fmul_rn(0.4f, m_conf));
+    score = (1.0f < mixed) ? 1.0f : mixed;
+    if (!isfinite(score)) continue;
+    pt.score = score;
+    // Output slot of this seed: the point and its images, ascending.
+    uint32_t vbase = 0;
+    if (lane == 0) vbase = (uint32_t)atomicAdd(rp.vis_cursor, (unsigned long long)nvis);
+    vbase = __shfl_sync(0xffffffffu, vbase, 0);
+    for (int i = lane; i < n; i += 32) {
+      bool first = true;
+      for (int j = 0; j < i; ++j)
+        if (ids[j] == ids[i]) {
+          first = false;
+          break;
+        }
+      if (!first) continue;
+      int rank = 0;  // distinct images below this one
+      for (int j = 0; j < n; ++j) {
+        if (ids[j] >= ids[i]) continue;
+        bool fj = true;
+        for (int q = 0; q < j; ++q)
+          if (ids[q] == ids[j]) {
+            fj = false;
+            break;
+          }
+        rank += fj ? 1 : 0;
+      }
+      rp.vis_pool[vbase + rank] = ids[i];
+    }
+    if (lane == 0) {
+      rp.slot_pts[s] = pt;
+      rp.slot_nvis[s] = (uint32_t)nvis;
+      rp.slot_visoff[s] = vbase;
+      rp.slot_has[s] = 1u;
+    }
+    __syncwarp();
+  }
+}
+
+// ---- scan (exclusive, out[n] = total) ---------------------------------------
+__global__ void __launch_bounds__(256) ScanReduceKernel(const uint32_t* in, uint32_t n, uint32_t* sums) {
+  __shared__ uint32_t red[256];
+  const uint32_t b0 = blockIdx.x * (uint32_t)kScanItems;
+  uint32_t acc = 0;
+  for (int k = 0; k < kScanItems / 256; ++k) {
+    const uint32_t i = b0 + (uint32_t)k * 256u + threadIdx.x;
+    if (i < n) acc += in[i];
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int sft = 128; sft > 0; sft >>= 1) {
+    if ((int)threadIdx.x < sft) red[threadIdx.x] += red[threadIdx.x + sft];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sums[blockIdx.x] = red[0];
+}
+
+__global__ void __launch_bounds__(1024) ScanSumsKernel(uint32_t* sums, uint32_t nb) {
+  __shared__ uint32_t buf[1024];
+  uint32_t carry = 0;
+  for (uint32_t b0 = 0; b0 < nb; b0 += 1024) {
+    const uint32_t i = b0 + threadIdx.x;
+    const uint32_t x = i < nb ? sums[i] : 0u;
+    buf[threadIdx.x] = x;
+    __syncthreads();
+    for (int sft = 1; sft < 1024; sft <<= 1) {
+      const uint32_t y = (int)threadIdx.x >= sft ? buf[threadIdx.x - sft] : 0u;
+      __syncthreads();
+      buf[threadIdx.x] += y;
+      __syncthreads();
+    }
+    if (i < nb) sums[i] = carry + buf[threadIdx.x] - x;
+    const uint32_t tot = buf[1023];
+    __syncthreads();
+    carry += tot;
+  }
+  if (threadIdx.x == 0) sums[nb] = carry;
+}
+
+__global__ void __launch_bounds__(256) ScanBlockKernel(const uint32_t* in, uint32_t n, const uint32_t* sums,
+                                                       uint32_t nb, uint32_t* out) {
+  __shared__ uint32_t buf[256];
+  const uint32_t b0 = blockIdx.x * (uint32_t)kScanItems;
+  uint32_t carry = sums[blockIdx.x];
+  for (int k = 0; k < kScanItems / 256; ++k) {
+    const uint32_t i = b0 + (uint32_t)k * 256u + threadIdx.x;
+    const uint32_t x = i < n ? in[i] : 0u;
+    buf[threadIdx.x] = x;
+    __syncthreads();
+    for (int sft = 1; sft < 256; sft <<= 1) {
+      const uint32_t y = (int)threadIdx.x >= sft ? buf[threadIdx.x - sft] : 0u;
+      __syncthreads();
+      buf[threadIdx.x] += y;
+      __syncthreads();
+    }
+    if (i < n) out[i] = carry + buf[threadIdx.x] - x;
+    const uint32_t tot = buf[255];
+    __syncthreads();
+    carry += tot;
+  }
+  if (blockIdx.x == nb - 1 && threadIdx.x == 0) out[n] = sums[nb];
+}
+
+// ---- per-image bookkeeping and compaction ------------------------------------
+__global__ void ImageStartKernel(int* shear, unsigned int* ticket, unsigned long long* rec_used,
+                                 unsigned long long* vis_cursor, uint32_t* n_over, uint32_t* stats) {
+  *shear = 1;
+  *ticket = 0u;
+  *rec_used = 0ull;
+  *vis_cursor = 0ull;
+  *n_over = 0u;
+  stats[0] = 0u;
+  stats[1] = 0u;
+}
+
+__global__ void CompactKernel(uint32_t nseeds, const uint32_t* slot_has, const uint32_t* pt_idx,
+                              const uint32_t* vis_idx, const smvs_fused_point* slot_pts, const uint32_t* slot_nvis,
+                              const uint32_t* slot_visoff, const uint32_t* vis_pool,
+                              const unsigned long long* totals, smvs_fused_point* out_pts, uint64_t* out_visoff,
+                              uint32_t* out_vis) {
+  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nseeds || !slot_has[s]) return;
+  const unsigned long long bp = totals[0], bv = totals[1];
+  const unsigned long long dst = bp + pt_idx[s], vdst = bv + vis_idx[s];
+  out_pts[dst] = slot_pts[s];
+  out_visoff[dst] = vdst;
+  const uint32_t nv = slot_nvis[s], src = slot_visoff[s];
+  for (uint32_t i = 0; i < nv; ++i) out_vis[vdst + i] = vis_pool[src + i];
+}
+
+__global__ void AdvanceKernel(unsigned long long* totals, const uint32_t* pt_idx, const uint32_t* vis_idx,
+                              uint32_t nseeds, uint64_t* out_visoff) {
+  totals[0] += pt_idx[nseeds];
+  totals[1] += vis_idx[nseeds];
+  out_visoff[totals[0]] = totals[1];
+}
+
+}  // namespace
+
+// ---- host object ---------------------------------------------------------------
+struct smvs_fusion {
+  smvs_fusion_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  cudaMemPool_t pool = nullptr;
+  int num_views = 0;
+  std::vector<smvs_fusion_view> views;  // sizes and poses (map pointers are not kept)
+  std::vector<FView> h_views;
+  std::vector<uint8_t> used, fused;
+  std::vector<int32_t> ov_off, ov_img;
+  std::vector<int> order;
+  uint64_t total = 0;  // pixels of all images
+  FConsts consts{};
+  // Device arrays.
+  FView* d_views = nullptr;
+  int* d_ov = nullptr;
+  uint8_t* d_trav = nullptr;
+  float *d_D = nullptr, *d_X = nullptr, *d_Y = nullptr, *d_Z = nullptr, *d_NX = nullptr, *d_NY = nullptr,
+        *d_NZ = nullptr, *d_G = nullptr;
+  uint8_t* d_rgb = nullptr;
+  uint8_t* d_mask = nullptr;
+  uint32_t *d_claim_cnt = nullptr, *d_claim_off = nullptr, *d_claim_list = nullptr;
+  size_t claim_list_cap = 0;
+  uint32_t* d_pool = nullptr;
+  size_t pool_words = 0;
+  uint32_t *d_rec_off = nullptr, *d_over_list = nullptr, *d_seq = nullptr, *d_done = nullptr;
+  uint32_t *d_keycnt = nullptr, *d_keyoff = nullptr;
+  size_t key_cap = 0;
+  smvs_fused_point* d_slot_pts = nullptr;
+  uint32_t *d_slot_has = nullptr, *d_slot_nvis = nullptr, *d_slot_visoff = nullptr;
+  uint32_t *d_pt_idx = nullptr, *d_vis_idx = nullptr, *d_vis_pool = nullptr;
+  size_t seed_cap = 0;
+  uint32_t* d_scan_sums = nullptr;
+  size_t scan_sums_cap = 0;
+  int* d_rows = nullptr;
+  size_t rows_cap = 0;
+  uint8_t* d_big_scratch = nullptr;
+  uint8_t* d_replay_scratch = nullptr;
+  size_t replay_scratch_bytes = 0;
+  uint32_t replay_scratch_cnt = 0, replay_scratch_stack = 0;
+  // Small device scalars: shear, ticket, n_over, stats[3], counters.
+  int* d_shear = nullptr;
+  unsigned int* d_ticket = nullptr;
+  uint32_t* d_n_over = nullptr;
+  uint32_t* d_stats = nullptr;
+  unsigned long long* d_used = nullptr;
+  unsigned long long* d_vis_cursor = nullptr;
+  unsigned long long* d_totals = nullptr;  // [0] points, [1] visibility entries
+  // Outputs.
+  smvs_fused_point* d_out_pts = nullptr;
+  uint64_t* d_out_visoff = nullptr;
+  uint32_t* d_out_vis = nullptr;
+  uint64_t num_points = 0, num_vis = 0;
+  bool ran = false;
+  int replay_blocks = 0;
+  int cap_closure = kCap, cap_replay = kCap, cap_stack = kStackSh;
+  int64_t launches = 0;
+  std::vector<int> h_rows;
+  bool profiling = false;
+  struct Timed { int kind; cudaEvent_t a, b; };
+  std::vector<Timed> timed;
+  int prof_count[4] = {0, 0, 0, 0};
+  double prof_ms[4] = {0, 0, 0, 0};
+};
+
+namespace {
+
+struct ProfScope {
+  smvs_fusion* f;
+  int kind;
+  cudaEvent_t a = nullptr, b = nullptr;
+  ProfScope(smvs_fusion* f_, int kind_) : f(f_), kind(kind_) {
+    if (!f->profiling) return;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) { a = b = nullptr; return; }
+    cudaEventRecord(a, f->stream);
+  }
+  ~ProfScope() {
+    if (!a) return;
+    cudaEventRecord(b, f->stream);
+    f->timed.push_back({kind, a, b});
+  }
+};
+
+void Harvest(smvs_fusion* f) {
+  for (auto& t : f->timed) {
+    float ms = 0.f;
+    if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
+      f->prof_count[t.kind] += 1;
+      f->prof_ms[t.kind] += ms;
+    }
+    cudaEventDestroy(t.a);
+    cudaEventDestroy(t.b);
+  }
+  f->timed.clear();
+}
+
+template <typename T>
+int Alloc(smvs_fusion* f, T** p, size_t count) {
+  const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+  cudaError_t err = cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, f->pool, f->stream);
+  if (err != cudaSuccess) {
+    *p = nullptr;
+    return Fail(SMVS_ENOMEM, "fusion: device allocation of %zu bytes: %s", bytes, cudaGetErrorString(err));
+  }
+  return SMVS_OK;
+}
+
+template <typename T>
+void Free(smvs_fusion* f, T*& p) {
+  if (p) cudaFreeAsync(p, f->stream);
+  p = nullptr;
+}
+
+void FreeAll(smvs_fusion* f) {
+  Harvest(f);
+  if (f->pool) {
+    Free(f, f->d_views); Free(f, f->d_ov); Free(f, f->d_trav);
+    Free(f, f->d_D); Free(f, f->d_X); Free(f, f->d_Y); Free(f, f->d_Z);
+    Free(f, f->d_NX); Free(f, f->d_NY); Free(f, f->d_NZ); Free(f, f->d_G);
+    Free(f, f->d_rgb); Free(f, f->d_mask);
+    Free(f, f->d_claim_cnt); Free(f, f->d_claim_off); Free(f, f->d_claim_list);
+    Free(f, f->d_pool); Free(f, f->d_rec_off); Free(f, f->d_over_list); Free(f, f->d_seq); Free(f, f->d_done);
+    Free(f, f->d_keycnt); Free(f, f->d_keyoff);
+    Free(f, f->d_slot_pts); Free(f, f->d_slot_has); Free(f, f->d_slot_nvis); Free(f, f->d_slot_visoff);
+    Free(f, f->d_pt_idx); Free(f, f->d_vis_idx); Free(f, f->d_vis_pool);
+    Free(f, f->d_scan_sums); Free(f, f->d_rows); Free(f, f->d_big_scratch); Free(f, f->d_replay_scratch);
+    Free(f, f->d_shear); Free(f, f->d_ticket); Free(f, f->d_n_over); Free(f, f->d_stats);
+    Free(f, f->d_used); Free(f, f->d_vis_cursor); Free(f, f->d_totals);
+    Free(f, f->d_out_pts); Free(f, f->d_out_visoff); Free(f, f->d_out_vis);
+  }
+  if (f->stream) cudaStreamSynchronize(f->stream);
+  if (f->own_stream && f->stream) cudaStreamDestroy(f->stream);
+}
+
+// P = K [R | T] in float, Eigen's packet product of a 3x3 and a 3x4 matrix.
+void ComposeP(const float K[9], const float R[9], const float T[3], float P[12]) {
+  float M[12];
+  for (int r = 0; r < 3; ++r) {
+    M[4 * r] = R[3 * r];
+    M[4 * r + 1] = R[3 * r + 1];
+    M[4 * r + 2] = R[3 * r + 2];
+    M[4 * r + 3] = T[r];
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 4; ++j) {
+      volatile float a = K[3 * i] * M[j];
+      volatile float b = K[3 * i + 1] * M[4 + j];
+      volatile float ab = a + b;
+      volatile float c = K[3 * i + 2] * M[8 + j];
+      P[4 * i + j] = ab + c;
+    }
+}
+
+// [P; 0 0 0 1]^-1 in double (adjugate), rounded once.
+void ComposeInvP(const float P[12], float iP[12]) {
+  const double m0 = P[0], m1 = P[1], m2 = P[2], m3 = P[4], m4 = P[5], m5 = P[6], m6 = P[8], m7 = P[9], m8 = P[10];
+  const double c00 = m4 * m8 - m5 * m7, c01 = m2 * m7 - m1 * m8, c02 = m1 * m5 - m2 * m4;
+  const double c10 = m5 * m6 - m3 * m8, c11 = m0 * m8 - m2 * m6, c12 = m2 * m3 - m0 * m5;
+  const double c20 = m3 * m7 - m4 * m6, c21 = m1 * m6 - m0 * m7, c22 = m0 * m4 - m1 * m3;
+  const double det = m0 * c00 + m1 * c10 + m2 * c20;
+  const double inv[9] = {c00 / det, c01 / det, c02 / det, c10 / det, c11 / det,
+                         c12 / det, c20 / det, c21 / det, c22 / det};
+  const double p[3] = {P[3], P[7], P[11]};
+  for (int i = 0; i < 3; ++i) {
+    iP[4 * i] = (float)inv[3 * i];
+    iP[4 * i + 1] = (float)inv[3 * i + 1];
+    iP[4 * i + 2] = (float)inv[3 * i + 2];
+    iP[4 * i + 3] = (float)(-(inv[3 * i] * p[0] + inv[3 * i + 1] * p[1] + inv[3 * i + 2] * p[2]));
+  }
+}
+
+// FindNextImage (fusion.cc:697-727).
+int FindNextImage(const smvs_fusion* f, int prev) {
+  for (int pass = 0; pass < 2; ++pass)
+    for (int32_t k = f->ov_off[prev]; k < f->ov_off[prev + 1]; ++k) {
+      const int i = f->ov_img[k];
+      if (f->used[i] && !f->fused[i] && (pass == 1 || !f->views[i].is_rig)) return i;
+    }
+  for (int pass = 0; pass < 2; ++pass)
+    for (int i = 0; i < f->num_views; ++i)
+      if (f->used[i] && !f->fused[i] && (pass == 1 || !f->views[i].is_rig)) return i;
+  return -1;
+}
+
+uint32_t Blocks(uint64_t n, int threads) { return (uint32_t)std::max<uint64_t>(1, (n + threads - 1) / threads); }
+
+int EnsureScanSums(smvs_fusion* f, uint64_t n) {
+  const size_t nb = (size_t)((n + kScanItems - 1) / kScanItems);
+  if (nb + 1 <= f->scan_sums_cap) return SMVS_OK;
+  Free(f, f->d_scan_sums);
+  f->scan_sums_cap = nb + 1;
+  return Alloc(f, &f->d_scan_sums, f->scan_sums_cap);
+}
+
+// Exclusive scan of n values into out[0..n], out[n] = total.
+int Scan(smvs_fusion* f, const uint32_t* in, uint64_t n, uint32_t* out) {
+  if (n == 0) return Fail(SMVS_EINVAL, "fusion: empty scan");
+  int st = EnsureScanSums(f, n);
+  if (st) return st;
+  const uint32_t nb = (uint32_t)((n + kScanItems - 1) / kScanItems);
+  ScanReduceKernel<<<nb, 256, 0, f->stream>>>(in, (uint32_t)n, f->d_scan_sums);
+  ScanSumsKernel<<<1, 1024, 0, f->stream>>>(f->d_scan_sums, nb);
+  ScanBlockKernel<<<nb, 256, 0, f->stream>>>(in, (uint32_t)n, f->d_scan_sums, nb, out);
+  f->launches += 3;
+  FU_CUDA(cudaGetLastError());
+  return SMVS_OK;
+}
+
+FMaps Maps(const smvs_fusion* f) {
+  FMaps m;
+  m.views = f->d_views;
+  m.ov = f->d_ov;
+  m.trav = f->d_trav;
+  m.D = f->d_D;
+  m.X = f->d_X;
+  m.Y = f->d_Y;
+  m.Z = f->d_Z;
+  m.NX = f->d_NX;
+  m.NY = f->d_NY;
+  m.NZ = f->d_NZ;
+  m.G = f->d_G;
+  m.rgb = f->d_rgb;
+  m.mask = f->d_mask;
+  return m;
+}
+
+FRecs Recs(const smvs_fusion* f) {
+  FRecs r;
+  r.pool = f->d_pool;
+  r.pool_words = f->pool_words;
+  r.used = f->d_used;
+  r.rec_off = f->d_rec_off;
+  r.over_list = f->d_over_list;
+  r.n_over = f->d_n_over;
+  r.stats = f->d_stats;
+  return r;
+}
+
+// Per-seed arrays for an image of n seeds.
+int EnsureSeeds(smvs_fusion* f, uint64_t n, uint64_t nkeys) {
+  int st = SMVS_OK;
+  if (n > f->seed_cap) {
+    Free(f, f->d_rec_off); Free(f, f->d_over_list); Free(f, f->d_seq); Free(f, f->d_done);
+    Free(f, f->d_slot_pts); Free(f, f->d_slot_has); Free(f, f->d_slot_nvis); Free(f, f->d_slot_visoff);
+    Free(f, f->d_pt_idx); Free(f, f->d_vis_idx);
+    f->seed_cap = n;
+    if ((st = Alloc(f, &f->d_rec_off, n)) || (st = Alloc(f, &f->d_over_list, n)) || (st = Alloc(f, &f->d_seq, n)) ||
+        (st = Alloc(f, &f->d_done, n)) || (st = Alloc(f, &f->d_slot_pts, n)) || (st = Alloc(f, &f->d_slot_has, n)) ||
+        (st = Alloc(f, &f->d_slot_nvis, n)) || (st = Alloc(f, &f->d_slot_visoff, n)) ||
+        (st = Alloc(f, &f->d_pt_idx, n + 1)) || (st = Alloc(f, &f->d_vis_idx, n + 1))) {
+      f->seed_cap = 0;
+      return st;
+    }
+  }
+  if (nkeys > f->key_cap) {
+    Free(f, f->d_keycnt); Free(f, f->d_keyoff);
+    f->key_cap = nkeys;
+    if ((st = Alloc(f, &f->d_keycnt, nkeys)) || (st = Alloc(f, &f->d_keyoff, nkeys + 1))) {
+      f->key_cap = 0;
+      return st;
+    }
+  }
+  return SMVS_OK;
+}
+
+int ReadStats(smvs_fusion* f, uint32_t stats[3], uint32_t* n_over, unsigned long long* used) {
+  FU_CUDA(cudaMemcpyAsync(stats, f->d_stats, 3 * sizeof(uint32_t), cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaMemcpyAsync(n_over, f->d_n_over, sizeof(uint32_t), cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaMemcpyAsync(used, f->d_used, sizeof(unsigned long long), cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  return SMVS_OK;
+}
+
+int FuseImage(smvs_fusion* f, int image) {
+  const smvs_fusion_view& v = f->views[image];
+  const int W = v.width, H = v.height, T = f->opt.num_slices, step = f->opt.step_size;
+  // The seed rows of FuseImage's slices (fusion.cc:1733-1764), in order.
+  f->h_rows.clear();
+  const int hs = (H + T - 1) / T;
+  for (int t = 0; t < T; ++t) {
+    const int limit = std::min(hs * (t + 1), H);
+    const int row_end = std::min(limit, H - kBlank);
+    for (int row = std::max(hs * t, kBlank); row < row_end; row += step) f->h_rows.push_back(row);
+  }
+  const int Rs = (int)f->h_rows.size();
+  const int Cs = W - 2 * kBlank > 0 ? (W - 2 * kBlank + step - 1) / step : 0;
+  if (Rs == 0 || Cs == 0) return SMVS_OK;
+  const uint64_t nseeds = (uint64_t)Rs * (uint64_t)Cs;
+  const uint64_t nkeys = (uint64_t)Cs * (uint64_t)Rs + (uint64_t)Cs;
+  int st = EnsureSeeds(f, nseeds, nkeys);
+  if (st) return st;
+  if ((size_t)Rs > f->rows_cap) {
+    Free(f, f->d_rows);
+    f->rows_cap = (size_t)Rs;
+    if ((st = Alloc(f, &f->d_rows, (size_t)Rs))) { f->rows_cap = 0; return st; }
+  }
+  FU_CUDA(cudaMemcpyAsync(f->d_rows, f->h_rows.data(), (size_t)Rs * sizeof(int), cudaMemcpyHostToDevice, f->stream));
+  FImage im;
+  im.view = image;
+  im.cap = f->cap_closure;
+  im.Rs = Rs;
+  im.Cs = Cs;
+  im.step = step;
+  im.nseeds = (uint32_t)nseeds;
+  im.rows = f->d_rows;
+  const FMaps m = Maps(f);
+  // 1. Closure records (the pool grows until every record fits).
+  uint32_t stats[3] = {0, 0, 0}, n_over = 0;
+  unsigned long long used = 0;
+  for (int attempt = 0;; ++attempt) {
+    ImageStartKernel<<<1, 1, 0, f->stream>>>(f->d_shear, f->d_ticket, f->d_used, f->d_vis_cursor, f->d_n_over,
+                                             f->d_stats);
+    ++f->launches;
+    {
+      ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
+      ClosureKernel<<<Blocks(nseeds, 128), 128, 0, f->stream>>>(m, f->consts, im, Recs(f));
+      ++f->launches;
+    }
+    FU_CUDA(cudaGetLastError());
+    if ((st = ReadStats(f, stats, &n_over, &used))) return st;
+    if (!(stats[2] & kStPool) && n_over > 0) {
+      if (!f->d_big_scratch && (st = Alloc(f, &f->d_big_scratch, (size_t)kBigBatch * kBigStride))) return st;
+      for (uint32_t first = 0; first < n_over; first += kBigBatch) {
+        const uint32_t count = std::min<uint32_t>(kBigBatch, n_over - first);
+        ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
+        ClosureBigKernel<<<Blocks(count, 64), 64, 0, f->stream>>>(m, f->consts, im, Recs(f), first, count,
+                                                                  f->d_big_scratch);
+        ++f->launches;
+      }
+      FU_CUDA(cudaGetLastError());
+      if ((st = ReadStats(f, stats, &n_over, &used))) return st;
+    }
+    if (stats[2] & kStBad) return Fail(SMVS_ECUDA, "fusion: inconsistent cluster record (image %d)", image);
+    if (!(stats[2] & kStPool)) break;
+    if (attempt >= 8) return Fail(SMVS_ENOMEM, "fusion: record pool cannot grow further");
+    // Grow the pool to what this image asked for, plus a margin.
+    const size_t want = (size_t)std::min<unsigned long long>(used + used / 4 + (1ull << 20), 0xfffffff0ull);
+    if (want <= f->pool_words) return Fail(SMVS_ENOMEM, "fusion: record pool limit (16 GB) reached");
+    Free(f, f->d_pool);
+    f->pool_words = want;
+    if ((st = Alloc(f, &f->d_pool, f->pool_words))) return st;
+    const uint32_t zero = 0;
+    FU_CUDA(cudaMemcpyAsync(f->d_stats + 2, &zero, sizeof(zero), cudaMemcpyHostToDevice, f->stream));
+    FU_CUDA(cudaStreamSynchronize(f->stream));
+  }
+  const uint32_t max_cnt = stats[0], max_ne = stats[1];
+  // 2. Claims and predecessors.
+  {
+    ProfScope ps(f, SMVS_FUSION_KERNEL_ORDER);
+    const uint64_t claims = used / 4 + 1;  // a record of cnt pixels takes more than 4 cnt words
+    if (claims > f->claim_list_cap) {
+      Free(f, f->d_claim_list);
+      f->claim_list_cap = (size_t)claims + 1024;
+      if ((st = Alloc(f, &f->d_claim_list, f->claim_list_cap))) { f->claim_list_cap = 0; return st; }
+    }
+    ClaimCountKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt);
+    ++f->launches;
+    if ((st = Scan(f, f->d_claim_cnt, f->total, f->d_claim_off))) return st;
+    ClaimFillKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt,
+                                                                 f->d_claim_off, f->d_claim_list);
+    ClaimSortKernel<<<Blocks(f->total, 256), 256, 0, f->stream>>>(f->d_claim_off, (uint32_t)f->total,
+                                                                   f->d_claim_list);
+    PredKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, Cs, f->d_claim_off,
+                                                           f->d_claim_list, f->d_shear);
+    // 3. Ticket order.
+    KeyCountKernel<<<Blocks(nkeys, 256), 256, 0, f->stream>>>((uint32_t)nkeys, Rs, Cs, f->d_shear, f->d_keycnt);
+    f->launches += 4;
+    if ((st = Scan(f, f->d_keycnt, nkeys, f->d_keyoff))) return st;
+    SeqKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>((uint32_t)nseeds, Cs, f->d_shear, f->d_keyoff, f->d_seq);
+    ++f->launches;
+    FU_CUDA(cudaGetLastError());
+  }
+  // 4. Replay.
+  if (max_cnt > (uint32_t)f->cap_replay || max_ne + 1 > (uint32_t)f->cap_stack) {
+    const uint32_t cap_cnt = std::max<uint32_t>(max_cnt, 1), cap_stack = max_ne + 1;
+    const size_t per = ScratchPer(cap_cnt, cap_stack);
+    const size_t need = per * (size_t)f->replay_blocks * kReplayWarps;
+    if (need > f->replay_scratch_bytes || cap_cnt > f->replay_scratch_cnt || cap_stack > f->replay_scratch_stack) {
+      Free(f, f->d_replay_scratch);
+      f->replay_scratch_bytes = need;
+      if ((st = Alloc(f, &f->d_replay_scratch, need))) { f->replay_scratch_bytes = 0; return st; }
+    }
+    f->replay_scratch_cnt = cap_cnt;
+    f->replay_scratch_stack = cap_stack;
+  }
+  FU_CUDA(cudaMemsetAsync(f->d_done, 0, nseeds * sizeof(uint32_t), f->stream));
+  FU_CUDA(cudaMemsetAsync(f->d_slot_has, 0, nseeds * sizeof(uint32_t), f->stream));
+  FU_CUDA(cudaMemsetAsync(f->d_slot_nvis, 0, nseeds * sizeof(uint32_t), f->stream));
+  {
+    FReplay rp;
+    rp.seq = f->d_seq;
+    rp.nseeds = (uint32_t)nseeds;
+    rp.done = f->d_done;
+    rp.ticket = f->d_ticket;
+    rp.slot_pts = f->d_slot_pts;
+    rp.slot_has = f->d_slot_has;
+    rp.slot_nvis = f->d_slot_nvis;
+    rp.slot_visoff = f->d_slot_visoff;
+    rp.vis_pool = f->d_vis_pool;
+    rp.vis_cursor = f->d_vis_cursor;
+    rp.scratch = f->d_replay_scratch;
+    rp.scratch_cnt = f->d_replay_scratch ? f->replay_scratch_cnt : 0;
+    rp.scratch_stack = f->d_replay_scratch ? f->replay_scratch_stack : 0;
+    rp.shared_cnt = f->cap_replay;
+    rp.shared_stack = f->cap_stack;
+    ProfScope ps(f, SMVS_FUSION_KERNEL_REPLAY);
+    ReplayKernel<<<f->replay_blocks, 32 * kReplayWarps, 0, f->stream>>>(m, f->consts, Recs(f), rp);
+    ++f->launches;
+    FU_CUDA(cudaGetLastError());
+  }
+  // 5. Compaction in seed order.
+  {
+    ProfScope ps(f, SMVS_FUSION_KERNEL_OTHER);
+    if ((st = Scan(f, f->d_slot_has, nseeds, f->d_pt_idx))) return st;
+    if ((st = Scan(f, f->d_slot_nvis, nseeds, f->d_vis_idx))) return st;
+    CompactKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(
+        (uint32_t)nseeds, f->d_slot_has, f->d_pt_idx, f->d_vis_idx, f->d_slot_pts, f->d_slot_nvis,
+        f->d_slot_visoff, f->d_vis_pool, f->d_totals, f->d_out_pts, f->d_out_visoff, f->d_out_vis);
+    AdvanceKernel<<<1, 1, 0, f->stream>>>(f->d_totals, f->d_pt_idx, f->d_vis_idx, (uint32_t)nseeds,
+                                          f->d_out_visoff);
+    f->launches += 2;
+    FU_CUDA(cudaGetLastError());
+  }
+  // The image is fused: no later traversal enters it.
+  FU_CUDA(cudaMemsetAsync(f->d_trav + image, 0, 1, f->stream));
+  return SMVS_OK;
+}
+
+thread_local int t_cap_closure = 0, t_cap_replay = 0, t_cap_stack = 0;
+
+int CheckStatus(smvs_fusion* f) {
+  uint32_t stats[3];
+  FU_CUDA(cudaMemcpyAsync(stats, f->d_stats, sizeof(stats), cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  if (stats[2] & kStTimeout) return Fail(SMVS_ETIMEDOUT, "fusion: a replay wait gave up after 20 s");
+  if (stats[2] & kStBad) return Fail(SMVS_ECUDA, "fusion: inconsistent replay state");
+  return SMVS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int smvs_fusion_options_default(smvs_fusion_options* o) {
+  if (!o) return Fail(SMVS_EINVAL, "null options");
+  o->step_size = 1;
+  o->min_num_pixels = 5;
+  o->max_num_pixels = 10000;
+  o->min_num_visible_images = 3;
+  o->max_traversal_depth = 100;
+  o->max_reproj_error = 2.0;
+  o->max_depth_error = (double)0.01f;
+  o->max_normal_error = 10.0;
+  o->with_normal = 1;
+  o->num_slices = 1;
+  o->gpu_index = 0;
+  return SMVS_OK;
+}
+
+int smvs_fusion_create(const smvs_fusion_options* opt, const smvs_fusion_view* views, int num_views,
+                       const int32_t* overlap_offsets, const int32_t* overlap_images, int memory, void* stream,
+                       smvs_fusion** out) {
+  if (!opt || !views || num_views < 1 || !overlap_offsets || !out)
+    return Fail(SMVS_EINVAL, "fusion: null argument or no images");
+  *out = nullptr;
+  if (memory != SMVS_MEM_HOST && memory != SMVS_MEM_DEVICE) return Fail(SMVS_EINVAL, "fusion: bad memory kind");
+  if (opt->step_size < 1 || opt->min_num_pixels < 2 || opt->max_num_pixels < opt->min_num_pixels ||
+      opt->max_traversal_depth < 1 || opt->min_num_visible_images < 0 || opt->num_slices < 1 ||
+      !(opt->max_reproj_error >= 0) || !(opt->max_depth_error >= 0) || !(opt->max_normal_error >= 0))
+    return Fail(SMVS_EINVAL, "fusion: bad options (min_num_pixels >= 2, max_num_pixels >= min_num_pixels, "
+                             "max_traversal_depth > 0, step_size > 0, num_slices > 0, errors >= 0)");
+  if (num_views > 65535) return Fail(SMVS_EINVAL, "fusion: more than 65535 images");
+  if (overlap_offsets[0] != 0) return Fail(SMVS_EINVAL, "fusion: overlap_offsets[0] must be 0");
+  for (int v = 0; v < num_views; ++v) {
+    if (overlap_offsets[v + 1] < overlap_offsets[v]) return Fail(SMVS_EINVAL, "fusion: decreasing overlap offsets");
+    for (int32_t k = overlap_offsets[v]; k < overlap_offsets[v + 1]; ++k)
+      if (!overlap_images || overlap_images[k] < 0 || overlap_images[k] >= num_views)
+        return Fail(SMVS_EINVAL, "fusion: overlapping image index out of range");
+  }
+  uint64_t total = 0;
+  for (int v = 0; v < num_views; ++v) {
+    const smvs_fusion_view& fv = views[v];
+    if (!fv.depth) continue;
+    if (fv.width < 1 || fv.height < 1) return Fail(SMVS_EINVAL, "fusion: image %d has no size", v);
+    if (opt->with_normal && !fv.normal) return Fail(SMVS_EINVAL, "fusion: image %d has no normal map", v);
+    total += (uint64_t)fv.width * (uint64_t)fv.height;
+  }
+  if (total >= (1ull << 31)) return Fail(SMVS_EINVAL, "fusion: 2^31 pixels or more");
+  smvs_fusion* f = new (std::nothrow) smvs_fusion();
+  if (!f) return Fail(SMVS_ENOMEM, "fusion: out of host memory");
+  f->opt = *opt;
+  f->num_views = num_views;
+  f->views.assign(views, views + num_views);
+  f->ov_off.assign(overlap_offsets, overlap_offsets + num_views + 1);
+  f->ov_img.assign(overlap_images ? overlap_images : overlap_offsets,
+                   (overlap_images ? overlap_images : overlap_offsets) + overlap_offsets[num_views]);
+  f->used.assign(num_views, 0);
+  f->fused.assign(num_views, 0);
+  f->total = std::max<uint64_t>(total, 1);
+  f->device = opt->gpu_index;
+  if (t_cap_closure > 0) f->cap_closure = std::min(t_cap_closure, kCap);
+  if (t_cap_replay > 0) f->cap_replay = std::min(t_cap_replay, kCap);
+  if (t_cap_stack > 0) f->cap_stack = std::min(t_cap_stack, kStackSh);
+  auto fail = [&](int st) {
+    FreeAll(f);
+    delete f;
+    return st;
+  };
+  if (cudaSetDevice(f->device) != cudaSuccess) return fail(Fail(SMVS_ECUDA, "fusion: cannot use GPU %d", f->device));
+  if (stream) {
+    f->stream = (cudaStream_t)stream;
+  } else {
+    if (cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(Fail(SMVS_ECUDA, "fusion: cannot create a stream"));
+    f->own_stream = true;
+  }
+  f->pool = smvs_internal_device_pool(f->device);
+  if (!f->pool) return fail(Fail(SMVS_ECUDA, "fusion: no device memory pool"));
+  // Constants (StereoFusion's constructor, fusion.cc:648-663).
+  FConsts& c = f->consts;
+  c.max_sq_reproj = (float)(opt->max_reproj_error * opt->max_reproj_error);
+  c.min_cos = (float)std::cos(opt->max_normal_error * 0.0174532925199432954743716805978692718781530857086181640625);
+  float thr = (float)opt->max_depth_error;
+  if ((double)thr > opt->max_depth_error) thr = std::nextafter(thr, -INFINITY);
+  c.derr_thr = thr;
+  c.max_depth_error = opt->max_depth_error;
+  c.with_normal = opt->with_normal ? 1 : 0;
+  c.min_pix = opt->min_num_pixels;
+  c.max_pix = opt->max_num_pixels;
+  c.max_depth = opt->max_traversal_depth;
+  c.min_vis = opt->min_num_visible_images;
+  // Image table.
+  f->h_views.resize(num_views);
+  uint64_t base = 0;
+  for (int v = 0; v < num_views; ++v) {
+    FView& hv = f->h_views[v];
+    memset(&hv, 0, sizeof(hv));
+    ComposeP(views[v].K, views[v].R, views[v].T, hv.P);
+    ComposeInvP(hv.P, hv.iP);
+    hv.W = views[v].width;
+    hv.H = views[v].height;
+    hv.base = (uint32_t)base;
+    hv.ov_begin = overlap_offsets[v];
+    hv.ov_end = overlap_offsets[v + 1];
+    f->used[v] = views[v].depth != nullptr;
+    if (f->used[v]) base += (uint64_t)hv.W * (uint64_t)hv.H;
+    else hv.W = hv.H = 0;
+  }
+  int st;
+  const size_t T = (size_t)f->total;
+  const size_t nov = std::max<size_t>((size_t)overlap_offsets[num_views], 1);
+  if ((st = Alloc(f, &f->d_views, (size_t)num_views)) || (st = Alloc(f, &f->d_ov, nov)) ||
+      (st = Alloc(f, &f->d_trav, (size_t)num_views)) || (st = Alloc(f, &f->d_D, T)) || (st = Alloc(f, &f->d_X, T)) ||
+      (st = Alloc(f, &f->d_Y, T)) || (st = Alloc(f, &f->d_Z, T)) || (st = Alloc(f, &f->d_G, T)) ||
+      (st = Alloc(f, &f->d_rgb, 3 * T)) || (st = Alloc(f, &f->d_mask, T)) || (st = Alloc(f, &f->d_claim_cnt, T)) ||
+      (st = Alloc(f, &f->d_claim_off, T + 1)) || (st = Alloc(f, &f->d_vis_pool, T)) ||
+      (st = Alloc(f, &f->d_out_pts, T / 2 + 1)) || (st = Alloc(f, &f->d_out_visoff, T / 2 + 2)) ||
+      (st = Alloc(f, &f->d_out_vis, T)) || (st = Alloc(f, &f->d_shear, 1)) || (st = Alloc(f, &f->d_ticket, 1)) ||
+      (st = Alloc(f, &f->d_n_over, 1)) || (st = Alloc(f, &f->d_stats, 3)) || (st = Alloc(f, &f->d_used, 1)) ||
+      (st = Alloc(f, &f->d_vis_cursor, 1)) || (st = Alloc(f, &f->d_totals, 2)))
+    return fail(st);
+  if (opt->with_normal &&
+      ((st = Alloc(f, &f->d_NX, T)) || (st = Alloc(f, &f->d_NY, T)) || (st = Alloc(f, &f->d_NZ, T))))
+    return fail(st);
+  // Record pool: 64 words per pixel of the largest image to start with; grows on demand.
+  uint64_t max_px = 1;
+  for (int v = 0; v < num_views; ++v)
+    if (f->used[v]) max_px = std::max<uint64_t>(max_px, (uint64_t)views[v].width * views[v].height);
+  f->pool_words = (size_t)std::min<uint64_t>(max_px * 64ull, 0xfffffff0ull);
+  if ((st = Alloc(f, &f->d_pool, f->pool_words))) return fail(st);
+  auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
+    return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, f->stream);
+  };
+  std::vector<uint8_t> trav(f->used.begin(), f->used.end());
+  if (up(f->d_views, f->h_views.data(), sizeof(FView) * num_views) != cudaSuccess ||
+      (overlap_offsets[num_views] > 0 &&
+       up(f->d_ov, overlap_images, sizeof(int32_t) * overlap_offsets[num_views]) != cudaSuccess) ||
+      up(f->d_trav, trav.data(), (size_t)num_views) != cudaSuccess ||
+      cudaMemsetAsync(f->d_mask, 0, T, f->stream) != cudaSuccess ||
+      cudaMemsetAsync(f->d_claim_cnt, 0, T * 4, f->stream) != cudaSuccess ||
+      cudaMemsetAsync(f->d_rgb, 0, 3 * T, f->stream) != cudaSuccess ||
+      cudaMemsetAsync(f->d_totals, 0, 2 * sizeof(unsigned long long), f->stream) != cudaSuccess ||
+      cudaMemsetAsync(f->d_out_visoff, 0, sizeof(uint64_t), f->stream) != cudaSuccess ||
+      cudaMemsetAsync(f->d_stats, 0, 3 * sizeof(uint32_t), f->stream) != cudaSuccess)
+    return fail(Fail(SMVS_ECUDA, "fusion: upload failed"));
+  // Maps and point maps.
+  const cudaMemcpyKind kind = memory == SMVS_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  for (int v = 0; v < num_views; ++v) {
+    if (!f->used[v]) continue;
+    const FView& hv = f->h_views[v];
+    const size_t plane = (size_t)hv.W * hv.H;
+    if (cudaMemcpyAsync(f->d_D + hv.base, views[v].depth, plane * 4, kind, f->stream) != cudaSuccess)
+      return fail(Fail(SMVS_ECUDA, "fusion: depth map copy failed"));
+    if (views[v].color &&
+        cudaMemcpyAsync(f->d_rgb + 3ull * hv.base, views[v].color, plane * 3, kind, f->stream) != cudaSuccess)
+      return fail(Fail(SMVS_ECUDA, "fusion: color copy failed"));
+    float* d_normal = nullptr;
+    if (opt->with_normal) {
+      if (memory == SMVS_MEM_HOST) {
+        if ((st = Alloc(f, &d_normal, 3 * plane))) return fail(st);
+        if (cudaMemcpyAsync(d_normal, views[v].normal, plane * 12, kind, f->stream) != cudaSuccess)
+          return fail(Fail(SMVS_ECUDA, "fusion: normal map copy failed"));
+      } else {
+        d_normal = const_cast<float*>(views[v].normal);
+      }
+    }
+    const float* R = views[v].R;
+    PointMapKernel<<<Blocks(plane, 256), 256, 0, f->stream>>>(
+        hv, R[0], R[1], R[2], R[3], R[4], R[5], R[6], R[7], R[8], d_normal, c.with_normal,
+        views[v].color != nullptr, f->d_D, f->d_X, f->d_Y, f->d_Z, f->d_NX, f->d_NY, f->d_NZ, f->d_G, f->d_rgb);
+    ++f->launches;
+    if (memory == SMVS_MEM_HOST) Free(f, d_normal);
+    if (cudaGetLastError() != cudaSuccess) return fail(Fail(SMVS_ECUDA, "fusion: point map launch failed"));
+  }
+  // The caller's maps are not referenced after this point.
+  if (cudaStreamSynchronize(f->stream) != cudaSuccess) return fail(Fail(SMVS_ECUDA, "fusion: upload failed"));
+  // Replay grid: every block resident.
+  int per_sm = 0, sms = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ReplayKernel, 32 * kReplayWarps, 0) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f->device) != cudaSuccess || per_sm < 1)
+    return fail(Fail(SMVS_ECUDA, "fusion: cannot size the replay grid"));
+  f->replay_blocks = per_sm * sms;
+  *out = f;
+  return SMVS_OK;
+}
+
+int smvs_fusion_run(smvs_fusion* f) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (f->ran) return Fail(SMVS_ESTATE, "fusion: run may be called once");
+  if (cudaSetDevice(f->device) != cudaSuccess) return Fail(SMVS_ECUDA, "fusion: cannot use GPU %d", f->device);
+  f->ran = true;
+  int start = 0;
+  for (int i = 0; i < f->num_views; ++i)
+    if (!f->views[i].is_rig) {
+      start = i;
+      break;
+    }
+  for (int image = start; image >= 0; image = FindNextImage(f, image)) {
+    if (!f->used[image]) continue;
+    int st = FuseImage(f, image);
+    if (st) return st;
+    f->fused[image] = 255;
+    f->order.push_back(image);
+  }
+  int st = CheckStatus(f);
+  if (st) return st;
+  unsigned long long totals[2];
+  FU_CUDA(cudaMemcpyAsync(totals, f->d_totals, sizeof(totals), cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  f->num_points = totals[0];
+  f->num_vis = totals[1];
+  Harvest(f);
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_sizes(smvs_fusion* f, size_t* num_points, size_t* num_visibility) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (!f->ran) return Fail(SMVS_ESTATE, "fusion: run first");
+  if (num_points) *num_points = (size_t)f->num_points;
+  if (num_visibility) *num_visibility = (size_t)f->num_vis;
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_points(smvs_fusion* f, smvs_fused_point* points, uint64_t* vis_offsets, uint32_t* vis_images) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (!f->ran) return Fail(SMVS_ESTATE, "fusion: run first");
+  if (points && f->num_points)
+    FU_CUDA(cudaMemcpyAsync(points, f->d_out_pts, f->num_points * sizeof(smvs_fused_point), cudaMemcpyDefault,
+                            f->stream));
+  if (vis_offsets)
+    FU_CUDA(cudaMemcpyAsync(vis_offsets, f->d_out_visoff, (f->num_points + 1) * sizeof(uint64_t), cudaMemcpyDefault,
+                            f->stream));
+  if (vis_images && f->num_vis)
+    FU_CUDA(cudaMemcpyAsync(vis_images, f->d_out_vis, f->num_vis * sizeof(uint32_t), cudaMemcpyDefault, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_device_points(smvs_fusion* f, const smvs_fused_point** points, const uint64_t** vis_offsets,
+                                  const uint32_t** vis_images) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (!f->ran) return Fail(SMVS_ESTATE, "fusion: run first");
+  if (points) *points = f->d_out_pts;
+  if (vis_offsets) *vis_offsets = f->d_out_visoff;
+  if (vis_images) *vis_images = f->d_out_vis;
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_image_order(smvs_fusion* f, int* order, int* count) {
+  if (!f || !count) return Fail(SMVS_EINVAL, "null argument");
+  *count = (int)f->order.size();
+  if (order && !f->order.empty()) memcpy(order, f->order.data(), f->order.size() * sizeof(int));
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_mask(smvs_fusion* f, int view, uint8_t* out) {
+  if (!f || !out) return Fail(SMVS_EINVAL, "null argument");
+  if (view < 0 || view >= f->num_views) return Fail(SMVS_EINVAL, "fusion: image %d out of range", view);
+  const FView& hv = f->h_views[view];
+  const size_t plane = (size_t)f->views[view].width * (size_t)f->views[view].height;
+  if (!f->used[view]) {
+    memset(out, 0, plane);
+    return SMVS_OK;
+  }
+  FU_CUDA(cudaMemcpyAsync(out, f->d_mask + hv.base, plane, cudaMemcpyDefault, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  return SMVS_OK;
+}
+
+int smvs_fusion_set_profiling(smvs_fusion* f, int enable) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  f->profiling = enable != 0;
+  return SMVS_OK;
+}
+
+int smvs_fusion_get_profile(smvs_fusion* f, int kind, int* count, double* total_ms) {
+  if (!f || !count || !total_ms || kind < 0 || kind > 3) return Fail(SMVS_EINVAL, "bad profile query");
+  Harvest(f);
+  *count = f->prof_count[kind];
+  *total_ms = f->prof_ms[kind];
+  return SMVS_OK;
+}
+
+int64_t smvs_fusion_launch_count(smvs_fusion* f) { return f ? f->launches : 0; }
+
+int smvs_test_fusion_caps(int closure_cap, int replay_cap, int replay_stack) {
+  if (closure_cap < 0 || replay_cap < 0 || replay_stack < 0 || (replay_stack > 0 && replay_stack < 2))
+    return Fail(SMVS_EINVAL, "fusion caps: bad values");
+  t_cap_closure = closure_cap;
+  t_cap_replay = replay_cap;
+  t_cap_stack = replay_stack;
+  return SMVS_OK;
+}
+
+void smvs_fusion_destroy(smvs_fusion* f) {
+  if (!f) return;
+  cudaSetDevice(f->device);
+  FreeAll(f);
+  delete f;
+}
+
+}  // extern "C"

@@ -131,6 +131,15 @@ def _is_cuda_tensor(x) -> bool:
     return hasattr(x, "is_cuda") and bool(getattr(x, "is_cuda"))
 
 
+def _sync_producers(keep, stream) -> None:
+    """The library reads device inputs on its own stream: when no stream is
+    given, wait for the torch stream that produced them (and for any
+    contiguous() copy made here) before handing their addresses over."""
+    if stream is None and any(_is_cuda_tensor(o) for o in keep if o is not None):
+        import torch
+        torch.cuda.current_stream().synchronize()
+
+
 def _addr(x):
     """(pointer, keep-alive object, is_device) of an array-like."""
     if x is None:
@@ -212,6 +221,7 @@ class PatchMatchACMMCuda:
         self.problem = problem
         lib = N.lib()
         prob, keep = _problem_struct(problem)
+        _sync_producers(keep, stream)
         handle = C.c_void_p()
         stream_ptr = C.c_void_p(int(stream)) if stream is not None else None
         N.check(lib.smvs_create(C.byref(options.to_c()), C.byref(prob), stream_ptr, C.byref(handle)))

@@ -506,3 +506,30 @@ def ring_scene(seed: int = 0, num_cameras: int = 24, scale: float = 0.125, radiu
     depths = np.concatenate([v.depth_gt[v.depth_gt > 0] for v in views])
     return Scene(views, refs[0], jobs[0][1], float(depths.min()) * 0.9, float(depths.max()) * 1.1,
                  name=f"ring(seed={seed},{num_cameras} cameras,scale={scale})", meta={"jobs": jobs}), jobs
+
+
+def fusion_inputs(scene: Scene, seed: int = 0, rel_noise: float = 0.002, outlier_frac: float = 0.03,
+                  hole_frac: float = 0.02, normal_noise_deg: float = 3.0, rig_every: int = 0):
+    """(images, overlapping_images) for StereoFusion: every view's noisy depth
+    and normal maps (``noisy_maps``), an RGB bitmap made from the grey image
+    (red = grey, green and blue shifted so the channels differ), and as the
+    overlapping list of each view every other view, nearest camera centre
+    first. With rig_every > 0 every rig_every-th view is flagged as a rig image."""
+    from .fusion import FusionImage
+    maps = noisy_maps(scene, seed=seed, rel_noise=rel_noise, outlier_frac=outlier_frac, hole_frac=hole_frac,
+                      normal_noise_deg=normal_noise_deg)
+    images = []
+    centres = []
+    for k, (v, (d, n)) in enumerate(zip(scene.views, maps)):
+        g = np.clip(np.rint(v.image), 0, 255).astype(np.int32)
+        rgb = np.stack([g, (g * 3 + 17) % 256, 255 - g], -1).astype(np.uint8)
+        images.append(FusionImage(K=v.K, R=v.R, T=v.T, depth=d, normal=n, color=rgb,
+                                  is_rig=bool(rig_every and k % rig_every == 0)))
+        centres.append(-np.asarray(v.R, np.float64).T @ np.asarray(v.T, np.float64))
+    centres = np.array(centres)
+    overlaps = []
+    for k in range(len(images)):
+        dist = np.linalg.norm(centres - centres[k], axis=1)
+        order = [int(i) for i in np.argsort(dist, kind="stable") if i != k]
+        overlaps.append(order)
+    return images, overlaps
