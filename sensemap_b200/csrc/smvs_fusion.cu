@@ -48,18 +48,22 @@ constexpr int kBlank = 3;              // blank_size (fusion.cc:1757, :1831)
 constexpr int kCap = 256;              // record capacity of the closure pass (pixels)
 constexpr int kBigCap = 65535;         // record capacity of the overflow pass (u16 indices)
 constexpr int kBigBatch = 256;         // overflow seeds per launch
-// Scratch bytes of one overflow thread: gid (u32) | derr (f32) | vid (u16),
-// rounded to 16 so every thread's arrays stay aligned.
-constexpr size_t kBigStride = ((size_t)kBigCap * 10u + 15u) & ~(size_t)15u;
+// Scratch bytes of one overflow thread: gid (u32) | derr (f32) | vid (u16) |
+// hash slots (u16, from the next 16-byte boundary) | eoff (u32); a multiple of
+// 16 so every thread's arrays stay aligned.
+constexpr size_t kBigSlotsOff = ((size_t)kBigCap * 10u + 15u) & ~(size_t)15u;
+constexpr size_t kBigEoffOff = kBigSlotsOff + 2u * 2u * 65536u;  // eoff (u32, kBigCap + 1)
+constexpr size_t kBigStride = (kBigEoffOff + 4u * ((size_t)kBigCap + 1u) + 15u) & ~(size_t)15u;
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr uint32_t kOver = 0xfffffffeu;
-constexpr int kReplayWarps = 8;        // warps per replay block
+constexpr int kReplayWarps = 4;        // warps per replay block
+constexpr int kEdgeSh = 1024;          // push-list entries of a record staged in shared memory
 constexpr int kStackSh = 512;          // replay stack entries kept in shared memory per warp
 constexpr int kScanItems = 4096;       // items per scan block (256 threads x 16)
 constexpr unsigned long long kWaitLimitNs = 20ull * 1000 * 1000 * 1000;  // bounded waits: 20 s
 
 // Status bits written by the kernels.
-constexpr uint32_t kStTimeout = 1u, kStPool = 2u, kStBad = 4u;
+constexpr uint32_t kStTimeout = 1u, kStPool = 2u, kStBad = 4u, kStBig = 8u;
 
 int Fail(int code, const char* fmt, ...) {
   char buf[512];
@@ -208,11 +212,63 @@ __global__ void PointMapKernel(FView v, float R0, float R1, float R2, float R3, 
 }
 
 // ---- closure ---------------------------------------------------------------
+// Membership of a closure under construction: open addressing over the pixel
+// index, slots hold node index + 1 (0 = empty).
+struct NodeSet {
+  uint16_t* slot;
+  uint32_t mask;  // table size - 1 (a power of two, at least twice the capacity)
+  __device__ __forceinline__ uint32_t Home(uint32_t g) const { return (g * 0x9E3779B1u) >> 7 & mask; }
+  __device__ __forceinline__ void Clear() const {
+    for (uint32_t i = 0; i <= mask; ++i) slot[i] = 0;
+  }
+  __device__ __forceinline__ int Find(const uint32_t* gid, uint32_t g) const {
+    for (uint32_t h = Home(g);; h = (h + 1) & mask) {
+      const uint32_t e = slot[h];
+      if (e == 0) return -1;
+      if (gid[e - 1] == g) return (int)e - 1;
+    }
+  }
+  __device__ __forceinline__ void Insert(uint32_t g, int idx) const {
+    uint32_t h = Home(g);
+    while (slot[h] != 0) h = (h + 1) & mask;
+    slot[h] = (uint16_t)(idx + 1);
+  }
+};
+
+// The seed point's projection into image u (column, row, depth), computed once
+// per image: a small direct-mapped cache keyed by the image index.
+struct SeedProj {
+  int u[16];
+  float col[16], row[16], z[16];
+  __device__ __forceinline__ void Clear() {
+    for (int i = 0; i < 16; ++i) u[i] = -1;
+  }
+  __device__ __forceinline__ void Get(const FView& fu, int ui, float sx, float sy, float sz, float* pc, float* pr,
+                                      float* pz) {
+    const int h = ui & 15;
+    if (u[h] != ui) {
+      const float p0 = Dot4p(fu.P, sx, sy, sz, 1.0f), p1 = Dot4p(fu.P + 4, sx, sy, sz, 1.0f),
+                  p2 = Dot4p(fu.P + 8, sx, sy, sz, 1.0f);
+      u[h] = ui;
+      col[h] = __fdiv_rn(p0, p2);
+      row[h] = __fdiv_rn(p1, p2);
+      z[h] = p2;
+    }
+    *pc = col[h];
+    *pr = row[h];
+    *pz = z[h];
+  }
+};
+
 // The pixels the seed's traversal can accept (see the file comment) into
-// gid/vid/derr; returns their count, 0 when the seed itself is fused or has no
-// valid depth, -1 when there are more than `cap`.
+// gid/vid/derr, and the push lists between them (eoff/edges, in the reference's
+// push order: overlapping_images_ of the pixel's image, :2073-2092) while they
+// fit `ecap` (*ne > ecap otherwise). Returns the pixel count, 0 when the seed
+// itself is fused or has no valid depth, -1 when there are more than `cap`.
 __device__ __forceinline__ int BuildClosure(const FMaps& m, const FConsts& c, uint32_t sg, int sv, uint32_t* gid,
-                                            uint16_t* vid, float* derr, int cap) {
+                                            uint16_t* vid, float* derr, const NodeSet& set, int cap,
+                                            uint32_t* eoff, uint16_t* edges, uint32_t ecap, uint32_t* ne) {
+  *ne = 0;
   if (m.mask[sg]) return 0;
   if (!ValidDepth(m.D[sg])) return 0;
   const float sx = m.X[sg], sy = m.Y[sg], sz = m.Z[sg];
@@ -222,11 +278,17 @@ __device__ __forceinline__ int BuildClosure(const FMaps& m, const FConsts& c, ui
     s1 = m.NY[sg];
     s2 = m.NZ[sg];
   }
+  SeedProj proj;
+  proj.Clear();
+  set.Clear();
   gid[0] = sg;
   vid[0] = (uint16_t)sv;
   derr[0] = 0.0f;
+  set.Insert(sg, 0);
   int cnt = 1;
+  uint32_t e = 0;
   for (int i = 0; i < cnt; ++i) {
+    eoff[i] = e;
     const uint32_t g = gid[i];
     const FView& fv = m.views[vid[i]];
     const float x = m.X[g], y = m.Y[g], z = m.Z[g];
@@ -238,42 +300,48 @@ __device__ __forceinline__ int BuildClosure(const FMaps& m, const FConsts& c, ui
       if (!ProjectPixel(fu, x, y, z, &row, &col)) continue;
       const uint32_t q = fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col;
       if (m.mask[q]) continue;
-      bool seen = false;
-      for (int j = 0; j < cnt; ++j)
-        if (gid[j] == q) {
-          seen = true;
-          break;
-        }
-      if (seen) continue;
-      const float dq = m.D[q];
-      if (!ValidDepth(dq)) continue;
-      // Reprojection and depth error of the seed point in image u (:1893-1912).
-      const float p0 = Dot4p(fu.P, sx, sy, sz, 1.0f), p1 = Dot4p(fu.P + 4, sx, sy, sz, 1.0f),
-                  p2 = Dot4p(fu.P + 8, sx, sy, sz, 1.0f);
-      const float cdiff = __fsub_rn(__fdiv_rn(p0, p2), (float)col);
-      const float rdiff = __fsub_rn(__fdiv_rn(p1, p2), (float)row);
-      const float sq = __fadd_rn(__fmul_rn(cdiff, cdiff), __fmul_rn(rdiff, rdiff));
-      if (sq > c.max_sq_reproj) continue;
-      const float de = __fdiv_rn(fabsf(__fsub_rn(p2, dq)), dq);
-      if (de > c.derr_thr) continue;
-      if (c.with_normal && Dot3(s0, s1, s2, m.NX[q], m.NY[q], m.NZ[q]) < c.min_cos) continue;  // :1944-1948
-      if (cnt == cap) return -1;
-      gid[cnt] = q;
-      vid[cnt] = (uint16_t)u;
-      derr[cnt] = de;
-      ++cnt;
+      int j = set.Find(gid, q);
+      if (j < 0) {
+        const float dq = m.D[q];
+        if (!ValidDepth(dq)) continue;
+        // Reprojection and depth error of the seed point in image u (:1893-1912).
+        float pc, pr, pz;
+        proj.Get(fu, u, sx, sy, sz, &pc, &pr, &pz);
+        const float cdiff = __fsub_rn(pc, (float)col), rdiff = __fsub_rn(pr, (float)row);
+        const float sq = __fadd_rn(__fmul_rn(cdiff, cdiff), __fmul_rn(rdiff, rdiff));
+        if (sq > c.max_sq_reproj) continue;
+        const float de = __fdiv_rn(fabsf(__fsub_rn(pz, dq)), dq);
+        if (de > c.derr_thr) continue;
+        if (c.with_normal && Dot3(s0, s1, s2, m.NX[q], m.NY[q], m.NZ[q]) < c.min_cos) continue;  // :1944-1948
+        if (cnt == cap) return -1;
+        j = cnt;
+        gid[cnt] = q;
+        vid[cnt] = (uint16_t)u;
+        derr[cnt] = de;
+        set.Insert(q, cnt);
+        ++cnt;
+      }
+      if (e < ecap) edges[e] = (uint16_t)j;
+      ++e;
     }
   }
+  eoff[cnt] = e;
+  *ne = e;
   return cnt;
 }
 
-// Writes the record of a closure; false when the pool is full.
+// Writes the record of a closure; false when the pool is full. The push lists
+// are copied from BuildClosure's, or computed again when they did not fit.
 __device__ bool WriteRecord(const FMaps& m, const FRecs& r, uint32_t seed, const uint32_t* gid, const uint16_t* vid,
-                            const float* derr, int cnt) {
-  uint32_t ebound = 0;
-  for (int i = 0; i < cnt; ++i) {
-    const FView& fv = m.views[vid[i]];
-    ebound += (uint32_t)(fv.ov_end - fv.ov_begin);
+                            const float* derr, const NodeSet& set, int cnt, const uint32_t* leoff,
+                            const uint16_t* ledges, uint32_t lne, bool have_edges) {
+  uint32_t ebound = lne;
+  if (!have_edges) {
+    ebound = 0;
+    for (int i = 0; i < cnt; ++i) {
+      const FView& fv = m.views[vid[i]];
+      ebound += (uint32_t)(fv.ov_end - fv.ov_begin);
+    }
   }
   const uint32_t words = RecWords((uint32_t)cnt, ebound);
   const unsigned long long off = atomicAdd(r.used, (unsigned long long)words);
@@ -295,33 +363,34 @@ __device__ bool WriteRecord(const FMaps& m, const FRecs& r, uint32_t seed, const
     rp[i] = -1;
     rv[i] = vid[i];
   }
-  // Push lists between record pixels, in the reference's push order
-  // (overlapping_images_ of the pixel's image, :2073-2092).
   uint32_t e = 0;
-  for (int i = 0; i < cnt; ++i) {
-    eoff[i] = e;
-    const uint32_t g = gid[i];
-    const FView& fv = m.views[vid[i]];
-    const float x = m.X[g], y = m.Y[g], z = m.Z[g];
-    for (int k = fv.ov_begin; k < fv.ov_end; ++k) {
-      const int u = m.ov[k];
-      if (!m.trav[u]) continue;
-      const FView& fu = m.views[u];
-      int row, col;
-      if (!ProjectPixel(fu, x, y, z, &row, &col)) continue;
-      const uint32_t q = fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col;
-      for (int j = 0; j < cnt; ++j)
-        if (gid[j] == q) {
-          if (e < ebound) edges[e] = (uint16_t)j;
-          ++e;
-          break;
-        }
+  if (have_edges) {
+    for (int i = 0; i <= cnt; ++i) eoff[i] = leoff[i];
+    for (uint32_t q = 0; q < lne; ++q) edges[q] = ledges[q];
+    e = lne;
+  } else {
+    for (int i = 0; i < cnt; ++i) {
+      eoff[i] = e;
+      const uint32_t g = gid[i];
+      const FView& fv = m.views[vid[i]];
+      const float x = m.X[g], y = m.Y[g], z = m.Z[g];
+      for (int k = fv.ov_begin; k < fv.ov_end; ++k) {
+        const int u = m.ov[k];
+        if (!m.trav[u]) continue;
+        const FView& fu = m.views[u];
+        int row, col;
+        if (!ProjectPixel(fu, x, y, z, &row, &col)) continue;
+        const int j = set.Find(gid, fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col);
+        if (j < 0) continue;
+        if (e < ebound) edges[e] = (uint16_t)j;
+        ++e;
+      }
     }
+    eoff[cnt] = e;
+    if (e > ebound) atomicOr(&r.stats[2], kStBad);
   }
-  eoff[cnt] = e;
   rec[0] = (uint32_t)cnt;
   rec[1] = e;
-  if (e > ebound) atomicOr(&r.stats[2], kStBad);
   r.rec_off[seed] = (uint32_t)off;
   atomicMax(&r.stats[0], (uint32_t)cnt);
   atomicMax(&r.stats[1], e);
@@ -335,13 +404,23 @@ __device__ __forceinline__ uint32_t SeedPixel(const FMaps& m, const FImage& im, 
   return fv.base + row * (uint32_t)fv.W + col;
 }
 
+constexpr int kSetSlots = 2 * kCap;          // hash slots of the closure pass
+constexpr int kBigSetSlots = 2 * 65536;      // hash slots of the overflow pass
+constexpr int kEdgeLocal = 2048;             // push-list entries kept by the closure pass
+
 __global__ void __launch_bounds__(128) ClosureKernel(FMaps m, FConsts c, FImage im, FRecs r) {
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= im.nseeds) return;
   uint32_t gid[kCap];
   uint16_t vid[kCap];
   float derr[kCap];
-  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, im.cap);
+  uint16_t slots[kSetSlots];
+  uint32_t eoff[kCap + 1];
+  uint16_t edges[kEdgeLocal];
+  const NodeSet set{slots, (uint32_t)kSetSlots - 1u};
+  uint32_t ne = 0;
+  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, set, im.cap, eoff, edges,
+                               kEdgeLocal, &ne);
   if (cnt == 0) {
     r.rec_off[s] = kEmpty;
     return;
@@ -352,10 +431,10 @@ __global__ void __launch_bounds__(128) ClosureKernel(FMaps m, FConsts c, FImage 
     r.over_list[k] = s;
     return;
   }
-  WriteRecord(m, r, s, gid, vid, derr, cnt);
+  WriteRecord(m, r, s, gid, vid, derr, set, cnt, eoff, edges, ne, ne <= (uint32_t)kEdgeLocal);
 }
 
-// Seeds over kCap, with their scratch in global memory.
+// Seeds over the closure pass's capacity, with their scratch in global memory.
 __global__ void __launch_bounds__(64) ClosureBigKernel(FMaps m, FConsts c, FImage im, FRecs r, uint32_t first,
                                                        uint32_t count, uint8_t* scratch) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -365,13 +444,18 @@ __global__ void __launch_bounds__(64) ClosureBigKernel(FMaps m, FConsts c, FImag
   uint32_t* gid = reinterpret_cast<uint32_t*>(base);
   float* derr = reinterpret_cast<float*>(base + (size_t)kBigCap * 4u);
   uint16_t* vid = reinterpret_cast<uint16_t*>(base + (size_t)kBigCap * 8u);
-  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, kBigCap);
+  uint16_t* slots = reinterpret_cast<uint16_t*>(base + kBigSlotsOff);
+  uint32_t* eoff = reinterpret_cast<uint32_t*>(base + kBigEoffOff);
+  const NodeSet set{slots, (uint32_t)kBigSetSlots - 1u};
+  uint32_t ne = 0;
+  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, set, kBigCap, eoff, nullptr, 0,
+                               &ne);
   if (cnt <= 0) {  // cannot be empty here; over kBigCap is reported
-    if (cnt < 0) atomicOr(&r.stats[2], kStBad);
+    if (cnt < 0) atomicOr(&r.stats[2], kStBig);
     r.rec_off[s] = kEmpty;
     return;
   }
-  WriteRecord(m, r, s, gid, vid, derr, cnt);
+  WriteRecord(m, r, s, gid, vid, derr, set, cnt, eoff, nullptr, 0, false);
 }
 
 // ---- claims and predecessors ------------------------------------------------
@@ -422,21 +506,6 @@ __global__ void ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt, c
   }
 }
 
-__global__ void ClaimSortKernel(const uint32_t* claim_off, uint32_t total, uint32_t* claim_list) {
-  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
-    const uint32_t a = claim_off[g], b = claim_off[g + 1];
-    for (uint32_t i = a + 1; i < b; ++i) {
-      const uint32_t x = claim_list[i];
-      uint32_t j = i;
-      while (j > a && claim_list[j - 1] > x) {
-        claim_list[j] = claim_list[j - 1];
-        --j;
-      }
-      claim_list[j] = x;
-    }
-  }
-}
-
 // Predecessor of each (seed, pixel) and the shear K of the ticket order:
 // key(p) < key(s) for every predecessor p of s needs K (i_s - i_p) > j_p - j_s.
 __global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* claim_off, const uint32_t* claim_list,
@@ -450,23 +519,15 @@ __global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* cla
   int need = 1;
   for (uint32_t k = 0; k < v.cnt; ++k) {
     const uint32_t g = v.gid[k];
-    uint32_t lo = claim_off[g], hi = claim_off[g + 1];
-    const uint32_t a = lo;
-    while (lo < hi) {  // first entry >= s
-      const uint32_t mid = (lo + hi) >> 1;
-      if (claim_list[mid] < s) lo = mid + 1; else hi = mid;
+    // The latest earlier claimant of this pixel (the list is in no order).
+    int32_t best = -1;
+    for (uint32_t q = claim_off[g], end = claim_off[g + 1]; q < end; ++q) {
+      const uint32_t cl = claim_list[q];
+      if (cl < s && (int32_t)cl > best) best = (int32_t)cl;
     }
-    if (lo >= claim_off[g + 1] || claim_list[lo] != s) {
-      atomicOr(&r.stats[2], kStBad);
-      v.pred[k] = -1;
-      continue;
-    }
-    if (lo == a) {
-      v.pred[k] = -1;
-      continue;
-    }
-    const uint32_t p = claim_list[lo - 1];
-    v.pred[k] = (int32_t)p;
+    v.pred[k] = best;
+    if (best < 0) continue;
+    const uint32_t p = (uint32_t)best;
     const int ip = (int)(p / (uint32_t)Cs), jp = (int)(p - (uint32_t)ip * (uint32_t)Cs);
     if (ip < is) {
       const int num = jp - js, den = is - ip;
@@ -522,8 +583,11 @@ struct FReplay {
 
 struct WarpShared {
   uint32_t stack[kStackSh];
+  uint32_t gid[kCap];        // the record, staged before the wait
+  uint32_t eoff[kCap + 1];
   float vals[kCap];
   uint32_t ids[kCap];
+  uint16_t edges[kEdgeSh];
   uint16_t acc[kCap];
   uint8_t flags[kCap];
   float med[2];
@@ -579,18 +643,28 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     if (off >= kOver) continue;  // no record: nothing to fuse, nobody waits for it
     const RecView v = OpenRecord(r.pool, off);
     const int cnt = (int)v.cnt;
-    // Storage: shared memory, or this warp's scratch for large records.
+    // Storage: shared memory (the record is staged there), or this warp's
+    // scratch for large records (read in place).
     uint8_t* flags;
     uint16_t* acc;
     uint32_t* stack;
     float* vals;
     uint32_t* ids;
-    if (cnt <= rp.shared_cnt && v.ne + 1 <= (uint32_t)rp.shared_stack) {
+    const uint32_t* rgid = v.gid;
+    const uint32_t* reoff = v.eoff;
+    const uint16_t* redges = v.edges;
+    if (cnt <= rp.shared_cnt && v.ne + 1 <= (uint32_t)rp.shared_stack && v.ne <= (uint32_t)kEdgeSh) {
       flags = sh.flags;
       acc = sh.acc;
       stack = sh.stack;
       vals = sh.vals;
       ids = sh.ids;
+      for (int k = lane; k < cnt; k += 32) sh.gid[k] = v.gid[k];
+      for (int k = lane; k <= cnt; k += 32) sh.eoff[k] = v.eoff[k];
+      for (uint32_t k = lane; k < v.ne; k += 32) sh.edges[k] = v.edges[k];
+      rgid = sh.gid;
+      reoff = sh.eoff;
+      redges = sh.edges;
     } else {
       if ((uint32_t)cnt > rp.scratch_cnt || v.ne + 1 > rp.scratch_stack || !rp.scratch) {
         if (lane == 0) {
@@ -606,24 +680,28 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
       acc = reinterpret_cast<uint16_t*>(base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 8u);
       flags = base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 10u;
     }
-    // Wait for the predecessors (every earlier seed that may touch these pixels).
+    // Wait for the predecessors (every earlier seed that may touch these
+    // pixels): spin, then back off, bounded in time.
     for (int k = lane; k < cnt; k += 32) {
       const int32_t p = v.pred[k];
       if (p < 0) continue;
-      const unsigned long long t0 = GlobalTimer();
-      unsigned ns = 32;
-      while (LoadAcquire(&rp.done[p]) == 0u) {
+      unsigned long long t0 = 0;
+      unsigned ns = 0;
+      for (uint32_t it = 0; LoadAcquire(&rp.done[p]) == 0u; ++it) {
+        if (it < 4096) continue;
+        if (ns == 0) t0 = GlobalTimer();
+        ns = ns < 256 ? ns + 32 : 256;
         __nanosleep(ns);
-        ns = ns < 256 ? ns * 2 : 256;
         if (GlobalTimer() - t0 > kWaitLimitNs) {
           atomicOr(&r.stats[2], kStTimeout);
           break;
         }
       }
     }
+    // The acquires above order the predecessors' mask writes before these
+    // reads for the whole warp (the barrier orders the lanes).
     __syncwarp();
-    __threadfence();
-    for (int k = lane; k < cnt; k += 32) flags[k] = *(volatile const uint8_t*)(m.mask + v.gid[k]);
+    for (int k = lane; k < cnt; k += 32) flags[k] = *(volatile const uint8_t*)(m.mask + rgid[k]);
     __syncwarp();
     // The reference's traversal (:1836-2094) on the record: LIFO stack of
     // (pixel, traversal depth); a pushed pixel that is already fused would be
@@ -640,8 +718,8 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
         if (nacc >= c.max_pix) break;
         if ((int)d + 1 >= c.max_depth) continue;
         const uint32_t nd = d + 1 < 0xffffu ? d + 1 : 0xffffu;
-        for (uint32_t q = v.eoff[k]; q < v.eoff[k + 1]; ++q) {
-          const uint32_t j = v.edges[q];
+        for (uint32_t q = reoff[k], qe = reoff[k + 1]; q < qe; ++q) {
+          const uint32_t j = redges[q];
           if (!flags[j]) stack[top++] = j | (nd << 16);
         }
       }
@@ -649,8 +727,9 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     }
     __syncwarp();
     const int n = sh.nacc;
-    for (int i = lane; i < n; i += 32) *(volatile uint8_t*)(m.mask + v.gid[acc[i]]) = 1;
-    __threadfence();
+    for (int i = lane; i < n; i += 32) *(volatile uint8_t*)(m.mask + rgid[acc[i]]) = 1;
+    // Release the successors: the barrier orders every lane's mask writes
+    // before lane 0's release store.
     __syncwarp();
     if (lane == 0) StoreRelease(&rp.done[s], 1u);
     // The fused point (:2098-2180).
@@ -678,7 +757,7 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     const float* maps[3] = {m.X, m.Y, m.Z};
     float xyz[3];
     for (int a = 0; a < 3; ++a) {
-      for (int i = lane; i < n; i += 32) vals[i] = maps[a][v.gid[acc[i]]];
+      for (int i = lane; i < n; i += 32) vals[i] = maps[a][rgid[acc[i]]];
       __syncwarp();
       xyz[a] = WarpMedian(vals, n, sh.med, lane);
     }
@@ -690,7 +769,7 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
       const float* nmaps[3] = {m.NX, m.NY, m.NZ};
       float fn[3];
       for (int a = 0; a < 3; ++a) {
-        for (int i = lane; i < n; i += 32) vals[i] = nmaps[a][v.gid[acc[i]]];
+        for (int i = lane; i < n; i += 32) vals[i] = nmaps[a][rgid[acc[i]]];
         __syncwarp();
         fn[a] = WarpMedian(vals, n, sh.med, lane);
       }
@@ -703,7 +782,7 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     }
     uint8_t rgb[3];
     for (int ch = 0; ch < 3; ++ch) {
-      for (int i = lane; i < n; i += 32) vals[i] = (float)m.rgb[3ull * v.gid[acc[i]] + ch];
+      for (int i = lane; i < n; i += 32) vals[i] = (float)m.rgb[3ull * rgid[acc[i]] + ch];
       __syncwarp();
       float med = roundf(WarpMedian(vals, n, sh.med, lane));
       med = med < 255.0f ? med : 255.0f;  // TruncateCast<float, uint8_t>
@@ -714,7 +793,7 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     pt.g = rgb[1];
     pt.b = rgb[2];
     // Mean gradient in traversal order, then the score (:2157-2166).
-    for (int i = lane; i < n; i += 32) vals[i] = m.G[v.gid[acc[i]]];
+    for (int i = lane; i < n; i += 32) vals[i] = m.G[rgid[acc[i]]];
     __syncwarp();
     float m_conf = 0.0f;
     if (lane == 0) {
@@ -1202,6 +1281,8 @@ int FuseImage(smvs_fusion* f, int image) {
       FU_CUDA(cudaGetLastError());
       if ((st = ReadStats(f, stats, &n_over, &used))) return st;
     }
+    if (stats[2] & kStBig)
+      return Fail(SMVS_EINVAL, "fusion: a seed of image %d reaches more than %d candidate pixels", image, kBigCap);
     if (stats[2] & kStBad) return Fail(SMVS_ECUDA, "fusion: inconsistent cluster record (image %d)", image);
     if (!(stats[2] & kStPool)) break;
     if (attempt >= 8) return Fail(SMVS_ENOMEM, "fusion: record pool cannot grow further");
@@ -1230,13 +1311,11 @@ int FuseImage(smvs_fusion* f, int image) {
     if ((st = Scan(f, f->d_claim_cnt, f->total, f->d_claim_off))) return st;
     ClaimFillKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt,
                                                                  f->d_claim_off, f->d_claim_list);
-    ClaimSortKernel<<<Blocks(f->total, 256), 256, 0, f->stream>>>(f->d_claim_off, (uint32_t)f->total,
-                                                                   f->d_claim_list);
     PredKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, Cs, f->d_claim_off,
                                                            f->d_claim_list, f->d_shear);
     // 3. Ticket order.
     KeyCountKernel<<<Blocks(nkeys, 256), 256, 0, f->stream>>>((uint32_t)nkeys, Rs, Cs, f->d_shear, f->d_keycnt);
-    f->launches += 4;
+    f->launches += 3;
     if ((st = Scan(f, f->d_keycnt, nkeys, f->d_keyoff))) return st;
     SeqKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>((uint32_t)nseeds, Cs, f->d_shear, f->d_keyoff, f->d_seq);
     ++f->launches;

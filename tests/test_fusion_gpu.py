@@ -114,3 +114,13 @@ def test_profile_and_errors(planes):
         assert all(ms >= 0 for _, ms in prof.values())
         with pytest.raises(N.SmvsError):
             f.Run()
+
+
+@pytest.mark.parametrize("depth", [100, 6])
+def test_many_views_large_records(depth):
+    """Eleven mutually overlapping views: records of a hundred pixels and more,
+    where the traversal-depth limit can bind."""
+    hs = syn.heightfield_scene(seed=6, width=320, height=240, focal=240.0, num_src=10, device="cuda")
+    ims, ov = syn.fusion_inputs(hs, seed=7)
+    opts = FusionOptions(max_traversal_depth=depth)
+    _same(_run(opts, ims, ov), O.fusion_run(opts, ims, ov))
