@@ -891,6 +891,9 @@ def run_fusion(args):
 
     f, out = step(dev, True, profile=True)
     prof = f.Profile()
+    chains, shears = f.DependencyChains(with_shear=True)
+    per_image = f.ImageProfile()
+    replay_times = f.ReplayTimes()
     npts = len(out[0])
     f.close()
     peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -941,7 +944,9 @@ def run_fusion(args):
                            "l2": f"inputs larger than L2 ({V} x {args.width}x{args.height} depth, normal and "
                                  f"color maps)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clock_info,
-                "fusion": {"points": npts}}
+                "fusion": {"points": npts, "replay_chain_steps": chains, "ticket_shear": shears, "image_ms": per_image,
+                           "replay_wait_post_us_seeds": replay_times,
+                           "replay_us_per_chain_step": round(1000.0 * prof["replay"][1] / max(sum(chains), 1), 3)}}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -33,6 +33,24 @@ int smvs_test_calibrate(int kind, double seconds, double* rate);
  * shared memory. Results do not change; the paths taken do. */
 int smvs_test_fusion_caps(int closure_cap, int replay_cap, int replay_stack);
 
+/* With profiling on during smvs_fusion_run: per fused image (in fusion order)
+ * the longest chain of seeds that each waited for the previous one (the
+ * number of sequential replay steps the image needed) and, optionally, the
+ * shear K of its ticket order (key = column + K x row of the seed grid). */
+int smvs_test_fusion_chains(smvs_fusion* f, uint32_t* chains, uint32_t* shears, int capacity, int* count);
+
+/* With profiling on: device milliseconds per fused image (in fusion order) and
+ * kernel kind (smvs_fusion_kernel), ms[4 * image + kind]. */
+int smvs_test_fusion_image_ms(smvs_fusion* f, double* ms, int capacity, int* count);
+
+/* With profiling on: per fused image, the mean microseconds a replayed seed
+ * spent waiting for its predecessors and from then until it released its
+ * successors, the number of seeds with a record, their mean record size and
+ * mean reachable set, how many replayed the traversal one pixel at a time, and
+ * the mean microseconds of the three steps after the wait (reading the masks,
+ * finding the fused pixels, marking them and releasing): 9 values per image. */
+int smvs_test_fusion_replay_times(smvs_fusion* f, double* out, int capacity, int* count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -251,6 +251,9 @@ _SIGNATURES = {
                                            C.c_void_p]),
     "smvs_test_calibrate": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_double)]),
     "smvs_test_fusion_caps": (C.c_int, [C.c_int, C.c_int, C.c_int]),
+    "smvs_test_fusion_chains": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "smvs_test_fusion_image_ms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "smvs_test_fusion_replay_times": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
 }
 
 _LIB = None

@@ -56,6 +56,7 @@ constexpr size_t kBigEoffOff = kBigSlotsOff + 2u * 2u * 65536u;  // eoff (u32, k
 constexpr size_t kBigStride = (kBigEoffOff + 4u * ((size_t)kBigCap + 1u) + 15u) & ~(size_t)15u;
 constexpr uint32_t kEmpty = 0xffffffffu;
 constexpr uint32_t kOver = 0xfffffffeu;
+constexpr uint32_t kRetry = 0xfffffffdu;  // the record did not fit the pool; built again after it grows
 constexpr int kReplayWarps = 4;        // warps per replay block
 constexpr int kEdgeSh = 1024;          // push-list entries of a record staged in shared memory
 constexpr int kStackSh = 512;          // replay stack entries kept in shared memory per warp
@@ -130,7 +131,7 @@ struct FRecs {
   uint32_t* pool;
   unsigned long long pool_words;
   unsigned long long* used;   // bump cursor (words)
-  uint32_t* rec_off;          // per seed: word offset, kEmpty or kOver
+  uint32_t* rec_off;          // per seed: word offset, or kEmpty, kOver, kRetry (no record)
   uint32_t* over_list;        // seeds over kCap
   uint32_t* n_over;
   uint32_t* stats;            // [0] max cnt, [1] max nE, [2] status
@@ -347,7 +348,7 @@ __device__ bool WriteRecord(const FMaps& m, const FRecs& r, uint32_t seed, const
   const unsigned long long off = atomicAdd(r.used, (unsigned long long)words);
   if (off + words > r.pool_words || off + words > 0xfffffff0ull) {
     atomicOr(&r.stats[2], kStPool);
-    r.rec_off[seed] = kEmpty;
+    r.rec_off[seed] = kRetry;
     return false;
   }
   uint32_t* rec = r.pool + off;
@@ -408,30 +409,223 @@ constexpr int kSetSlots = 2 * kCap;          // hash slots of the closure pass
 constexpr int kBigSetSlots = 2 * 65536;      // hash slots of the overflow pass
 constexpr int kEdgeLocal = 2048;             // push-list entries kept by the closure pass
 
-__global__ void __launch_bounds__(128) ClosureKernel(FMaps m, FConsts c, FImage im, FRecs r) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= im.nseeds) return;
+// One warp per seed. The closure under construction lives in shared memory:
+// a hash set of its pixels (key = pixel index, value = node index), the
+// nodes (pixel, image, depth error, point) and their push lists.
+constexpr int kClosureWarps = 4;  // warps (seeds in flight) per closure block
+constexpr uint32_t kNoKey = 0xffffffffu;
+struct ClosureShared;
+
+struct ClosureShared {
+  uint32_t keys[kSetSlots];
   uint32_t gid[kCap];
-  uint16_t vid[kCap];
   float derr[kCap];
-  uint16_t slots[kSetSlots];
   uint32_t eoff[kCap + 1];
-  uint16_t edges[kEdgeLocal];
-  const NodeSet set{slots, (uint32_t)kSetSlots - 1u};
-  uint32_t ne = 0;
-  const int cnt = BuildClosure(m, c, SeedPixel(m, im, s), im.view, gid, vid, derr, set, im.cap, eoff, edges,
-                               kEdgeLocal, &ne);
-  if (cnt == 0) {
-    r.rec_off[s] = kEmpty;
-    return;
+  uint32_t dpre[kCap + 1];             // push counts of the frontier, prefix-summed
+  uint32_t ecnt[kCap];
+  uint16_t kidx[kSetSlots];
+  uint16_t vid[kCap];
+};
+
+// Exclusive prefix sum over a[lo..hi) into out[lo..hi], out[lo] = base.
+__device__ __forceinline__ void WarpPrefix(const uint32_t* a, uint32_t* out, int lo, int hi, uint32_t base,
+                                           int lane) {
+  uint32_t carry = base;
+  for (int i0 = lo; i0 < hi; i0 += 32) {
+    const int i = i0 + lane;
+    const uint32_t x = i < hi ? a[i] : 0u;
+    uint32_t incl = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (i < hi) out[i] = carry + incl - x;
+    carry += __shfl_sync(0xffffffffu, incl, 31);
   }
-  if (cnt < 0) {
-    r.rec_off[s] = kOver;
-    const uint32_t k = atomicAdd(r.n_over, 1u);
-    r.over_list[k] = s;
-    return;
+  if (lane == 0) out[hi] = carry;
+  __syncwarp();
+}
+
+constexpr size_t kClosureSmem = sizeof(ClosureShared) * kClosureWarps;
+
+// `stage`: kEdgeLocal push-list entries per warp of the grid (global memory;
+// a few MB for the whole grid, so they stay in L2).
+__global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FConsts c, FImage im, FRecs r,
+                                                                    int only_retry, uint16_t* stage) {
+  extern __shared__ __align__(16) unsigned char closure_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  ClosureShared& sh = reinterpret_cast<ClosureShared*>(closure_smem)[w];
+  uint16_t* const edges = stage + ((size_t)blockIdx.x * kClosureWarps + w) * kEdgeLocal;
+  const unsigned lt = (1u << lane) - 1u;
+  for (uint32_t s = blockIdx.x * kClosureWarps + w; s < im.nseeds; s += gridDim.x * kClosureWarps) {
+    if (only_retry && r.rec_off[s] != kRetry) continue;
+    const uint32_t sg = SeedPixel(m, im, s);
+    if (m.mask[sg] || !ValidDepth(m.D[sg])) {
+      if (lane == 0) r.rec_off[s] = kEmpty;
+      continue;
+    }
+    const float sx = m.X[sg], sy = m.Y[sg], sz = m.Z[sg];
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    if (c.with_normal) {
+      s0 = m.NX[sg];
+      s1 = m.NY[sg];
+      s2 = m.NZ[sg];
+    }
+    for (int h = lane; h < kSetSlots; h += 32) sh.keys[h] = kNoKey;
+    __syncwarp();
+    if (lane == 0) {
+      const uint32_t h = ((sg * 0x9E3779B1u) >> 7) & (uint32_t)(kSetSlots - 1);
+      sh.keys[h] = sg;
+      sh.kidx[h] = 0;
+      sh.gid[0] = sg;
+      sh.vid[0] = (uint16_t)im.view;
+      sh.derr[0] = 0.0f;
+      sh.eoff[0] = 0;
+    }
+    __syncwarp();
+    int cnt = 1, head = 0;
+    uint32_t ecur = 0;
+    bool over = false;
+    // Breadth-first waves: every (frontier pixel, overlapping image) pair is
+    // one lane's candidate; pairs run in pixel-major, image order, so the push
+    // lists come out in the reference's order.
+    while (head < cnt && !over) {
+      const int tail = cnt;
+      for (int i = head + lane; i < tail; i += 32) {
+        const FView& fv = m.views[sh.vid[i]];
+        sh.ecnt[i] = (uint32_t)(fv.ov_end - fv.ov_begin);
+      }
+      __syncwarp();
+      WarpPrefix(sh.ecnt, sh.dpre, head, tail, 0u, lane);
+      for (int i = head + lane; i < tail; i += 32) sh.ecnt[i] = 0;
+      __syncwarp();
+      const uint32_t P = sh.dpre[tail];
+      for (uint32_t p0 = 0; p0 < P && !over; p0 += 32) {
+        const uint32_t p = p0 + lane;
+        // 0 none, 1 found/duplicate (read kidx[h] later), 2 owner of a new node
+        int kind = 0, i = 0, u = 0;
+        uint32_t h = 0, q = 0;
+        float de = 0.f;
+        if (p < P) {
+          int lo = head, hi = tail - 1;  // the frontier pixel whose pushes hold p
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (sh.dpre[mid] <= p) lo = mid; else hi = mid - 1;
+          }
+          i = lo;
+          const FView& fv = m.views[sh.vid[i]];
+          u = m.ov[fv.ov_begin + (int)(p - sh.dpre[i])];
+          int row, col;
+          const uint32_t gi = sh.gid[i];
+          if (m.trav[u] && ProjectPixel(m.views[u], m.X[gi], m.Y[gi], m.Z[gi], &row, &col)) {
+            const FView& fu = m.views[u];
+            q = fu.base + (uint32_t)row * (uint32_t)fu.W + (uint32_t)col;
+            if (!m.mask[q]) {
+              h = ((q * 0x9E3779B1u) >> 7) & (uint32_t)(kSetSlots - 1);
+              const volatile uint32_t* vkeys = sh.keys;  // other lanes insert concurrently
+              uint32_t key;
+              while ((key = vkeys[h]) != kNoKey && key != q) h = (h + 1) & (uint32_t)(kSetSlots - 1);
+              if (key == q) {
+                kind = 1;
+              } else {
+                const float dq = m.D[q];
+                bool ok = ValidDepth(dq);
+                if (ok) {
+                  const float p0 = Dot4p(fu.P, sx, sy, sz, 1.0f), p1 = Dot4p(fu.P + 4, sx, sy, sz, 1.0f),
+                              p2 = Dot4p(fu.P + 8, sx, sy, sz, 1.0f);
+                  const float cdiff = __fsub_rn(__fdiv_rn(p0, p2), (float)col);
+                  const float rdiff = __fsub_rn(__fdiv_rn(p1, p2), (float)row);
+                  const float sq = __fadd_rn(__fmul_rn(cdiff, cdiff), __fmul_rn(rdiff, rdiff));
+                  de = __fdiv_rn(fabsf(__fsub_rn(p2, dq)), dq);
+                  ok = !(sq > c.max_sq_reproj) && !(de > c.derr_thr);
+                  if (ok && c.with_normal) ok = !(Dot3(s0, s1, s2, m.NX[q], m.NY[q], m.NZ[q]) < c.min_cos);
+                }
+                if (ok) {  // claim a slot; a lane of this round may hold the same pixel
+                  for (;;) {
+                    const uint32_t old = atomicCAS(&sh.keys[h], kNoKey, q);
+                    if (old == kNoKey) { kind = 2; break; }
+                    if (old == q) { kind = 1; break; }
+                    h = (h + 1) & (uint32_t)(kSetSlots - 1);
+                  }
+                }
+              }
+            }
+          }
+        }
+        __syncwarp();
+        const unsigned own = __ballot_sync(0xffffffffu, kind == 2);
+        int j = -1;
+        if (kind == 2) {
+          j = cnt + __popc(own & lt);
+          if (j < im.cap) {
+            sh.kidx[h] = (uint16_t)j;
+            sh.gid[j] = q;
+            sh.vid[j] = (uint16_t)u;
+            sh.derr[j] = de;
+          }
+        }
+        cnt += __popc(own);
+        if (cnt > im.cap) over = true;
+        __syncwarp();
+        if (kind == 1) j = sh.kidx[h];
+        const unsigned val = __ballot_sync(0xffffffffu, j >= 0);
+        const uint32_t at = ecur + (uint32_t)__popc(val & lt);
+        if (j >= 0 && !over) {
+          if (at < (uint32_t)kEdgeLocal) edges[at] = (uint16_t)j;
+          atomicAdd(&sh.ecnt[i], 1u);
+        }
+        ecur += (uint32_t)__popc(val);
+        if (ecur > (uint32_t)kEdgeLocal) over = true;
+        __syncwarp();
+      }
+      if (!over) WarpPrefix(sh.ecnt, sh.eoff, head, tail, sh.eoff[head], lane);
+      head = tail;
+    }
+    if (over) {
+      if (lane == 0) {
+        r.rec_off[s] = kOver;
+        const uint32_t k = atomicAdd(r.n_over, 1u);
+        r.over_list[k] = s;
+      }
+      continue;
+    }
+    // The record, written by the warp.
+    const uint32_t ne = ecur;
+    const uint32_t words = RecWords((uint32_t)cnt, ne);
+    unsigned long long off = 0;
+    if (lane == 0) off = atomicAdd(r.used, (unsigned long long)words);
+    off = __shfl_sync(0xffffffffu, off, 0);
+    if (off + words > r.pool_words || off + words > 0xfffffff0ull) {
+      if (lane == 0) {
+        atomicOr(&r.stats[2], kStPool);
+        r.rec_off[s] = kRetry;
+      }
+      continue;
+    }
+    uint32_t* rec = r.pool + off;
+    uint32_t* rg = rec + 2;
+    float* rd = reinterpret_cast<float*>(rg + cnt);
+    int32_t* rpd = reinterpret_cast<int32_t*>(rd + cnt);
+    uint32_t* reo = reinterpret_cast<uint32_t*>(rpd + cnt);
+    uint16_t* rv = reinterpret_cast<uint16_t*>(reo + cnt + 1);
+    uint16_t* redg = rv + 2 * ((cnt + 1) / 2);
+    for (int k = lane; k < cnt; k += 32) {
+      rg[k] = sh.gid[k];
+      rd[k] = sh.derr[k];
+      rpd[k] = -1;
+      rv[k] = sh.vid[k];
+    }
+    for (int k = lane; k <= cnt; k += 32) reo[k] = sh.eoff[k];
+    for (uint32_t k = lane; k < ne; k += 32) redg[k] = edges[k];
+    if (lane == 0) {
+      rec[0] = (uint32_t)cnt;
+      rec[1] = ne;
+      r.rec_off[s] = (uint32_t)off;
+      atomicMax(&r.stats[0], (uint32_t)cnt);
+      atomicMax(&r.stats[1], ne);
+    }
+    __syncwarp();
   }
-  WriteRecord(m, r, s, gid, vid, derr, set, cnt, eoff, edges, ne, ne <= (uint32_t)kEdgeLocal);
 }
 
 // Seeds over the closure pass's capacity, with their scratch in global memory.
@@ -487,7 +681,7 @@ __global__ void ClaimCountKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt) 
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
-  if (off >= kOver) return;
+  if (off >= kRetry) return;
   const RecView v = OpenRecord(r.pool, off);
   for (uint32_t k = 0; k < v.cnt; ++k) atomicAdd(&claim_cnt[v.gid[k]], 1u);
 }
@@ -497,7 +691,7 @@ __global__ void ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt, c
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
-  if (off >= kOver) return;
+  if (off >= kRetry) return;
   const RecView v = OpenRecord(r.pool, off);
   for (uint32_t k = 0; k < v.cnt; ++k) {
     const uint32_t g = v.gid[k];
@@ -513,10 +707,14 @@ __global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* cla
   const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
-  if (off >= kOver) return;
+  if (off >= kRetry) return;
   RecView v = OpenRecord(r.pool, off);
   const int is = (int)(s / (uint32_t)Cs), js = (int)(s - (uint32_t)is * (uint32_t)Cs);
   int need = 1;
+  // The record's predecessors, each once, at the front of pred[] (the replay
+  // only waits for them); the first 32 distinct ones are recognised.
+  int32_t seen[32];
+  uint32_t nu = 0, nseen = 0;
   for (uint32_t k = 0; k < v.cnt; ++k) {
     const uint32_t g = v.gid[k];
     // The latest earlier claimant of this pixel (the list is in no order).
@@ -525,8 +723,16 @@ __global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* cla
       const uint32_t cl = claim_list[q];
       if (cl < s && (int32_t)cl > best) best = (int32_t)cl;
     }
-    v.pred[k] = best;
     if (best < 0) continue;
+    bool dup = false;
+    for (uint32_t t = 0; t < nseen; ++t)
+      if (seen[t] == best) {
+        dup = true;
+        break;
+      }
+    if (dup) continue;
+    if (nseen < 32) seen[nseen++] = best;
+    v.pred[nu++] = best;  // nu <= k: entries not yet visited are never read
     const uint32_t p = (uint32_t)best;
     const int ip = (int)(p / (uint32_t)Cs), jp = (int)(p - (uint32_t)ip * (uint32_t)Cs);
     if (ip < is) {
@@ -535,6 +741,7 @@ __global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* cla
       need = max(need, fl + 1);
     }
   }
+  for (uint32_t k = nu; k < v.cnt; ++k) v.pred[k] = -1;
   if (need > 1) atomicMax(shear, min(need, Cs));
 }
 
@@ -579,6 +786,9 @@ struct FReplay {
   uint32_t scratch_stack;     // stack capacity of a scratch region
   int shared_cnt;             // records up to this many pixels ...
   int shared_stack;           // ... and stack entries replay in shared memory
+  uint32_t* level;            // with profiling: dependency depth of each seed (else null)
+  uint32_t* chain;            // with profiling: the image's longest dependency chain
+  unsigned long long* times;  // with profiling: summed ns [waiting, after the wait until release], seeds
 };
 
 struct WarpShared {
@@ -628,6 +838,63 @@ __device__ float WarpMedian(const float* vals, int n, float* med, int lane) {
   return r;
 }
 
+// Waits until *flag is set: a short spin, then a growing back-off (fewer loads
+// for L2 to serve while most warps wait), bounded in time (status bit on
+// timeout).
+__device__ __forceinline__ void WaitDone(const uint32_t* flag, uint32_t* stats) {
+  unsigned long long t0 = 0;
+  unsigned ns = 0;
+  for (uint32_t it = 0; LoadAcquire(flag) == 0u; ++it) {
+    if (it < 64) continue;
+    if (ns == 0) t0 = GlobalTimer();
+    ns = ns < 1024 ? ns + 64 : 1024;
+    __nanosleep(ns);
+    if (GlobalTimer() - t0 > kWaitLimitNs) {
+      atomicOr(&stats[2], kStTimeout);
+      return;
+    }
+  }
+}
+
+// The reference's traversal (:1836-2094) on a record, by one lane: LIFO stack
+// of (pixel, traversal depth). flags: nonzero = already fused; accepted pixels
+// are flagged and listed in acc in the order the reference fuses them. A
+// pushed pixel that is already fused would be skipped when popped, so it is
+// not pushed. Returns the number accepted.
+__device__ int SeqTraversal(uint8_t* __restrict__ flags, uint32_t* __restrict__ stack, uint16_t* __restrict__ acc,
+                            const uint32_t* __restrict__ reoff, const uint16_t* __restrict__ redges, int max_pix,
+                            int max_depth) {
+  int nacc = 0, top = 0;
+  if (!flags[0]) stack[top++] = 0u;
+  while (top > 0) {
+    const uint32_t e = stack[--top];
+    const uint32_t k = e & 0xffffu, d = e >> 16;
+    if (flags[k]) continue;
+    flags[k] = 1;
+    acc[nacc++] = (uint16_t)k;
+    if (nacc >= max_pix) break;
+    if ((int)d + 1 >= max_depth) continue;
+    const uint32_t nd = (d + 1 < 0xffffu ? d + 1 : 0xffffu) << 16;
+    uint32_t q = reoff[k];
+    const uint32_t qe = reoff[k + 1];
+    // Four pushes at a time: the loads of a batch overlap (pushes only write
+    // the stack, so the flags they read do not change within the batch).
+    for (; q + 4 <= qe; q += 4) {
+      const uint32_t j0 = redges[q], j1 = redges[q + 1], j2 = redges[q + 2], j3 = redges[q + 3];
+      const uint8_t f0 = flags[j0], f1 = flags[j1], f2 = flags[j2], f3 = flags[j3];
+      if (!f0) stack[top++] = j0 | nd;
+      if (!f1) stack[top++] = j1 | nd;
+      if (!f2) stack[top++] = j2 | nd;
+      if (!f3) stack[top++] = j3 | nd;
+    }
+    for (; q < qe; ++q) {
+      const uint32_t j = redges[q];
+      if (!flags[j]) stack[top++] = j | nd;
+    }
+  }
+  return nacc;
+}
+
 __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FConsts c, FRecs r, FReplay rp) {
   __shared__ WarpShared shm[kReplayWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -640,98 +907,175 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     if (t >= rp.nseeds) break;
     const uint32_t s = rp.seq[t];
     const uint32_t off = r.rec_off[s];
-    if (off >= kOver) continue;  // no record: nothing to fuse, nobody waits for it
+    if (off >= kRetry) continue;  // no record: nothing to fuse, nobody waits for it
     const RecView v = OpenRecord(r.pool, off);
     const int cnt = (int)v.cnt;
-    // Storage: shared memory (the record is staged there), or this warp's
-    // scratch for large records (read in place).
-    uint8_t* flags;
-    uint16_t* acc;
-    uint32_t* stack;
+    // Storage: the per-pixel arrays in shared memory when the record has at
+    // most shared_cnt pixels, the stack when it fits shared_stack entries, and
+    // the record itself staged there when it fits; anything larger lives in
+    // this warp's global scratch (or is read from the record in place).
+    const bool node_sh = cnt <= rp.shared_cnt;
+    const bool stack_sh = v.ne + 1 <= (uint32_t)rp.shared_stack;
+    if ((!node_sh && (uint32_t)cnt > rp.scratch_cnt) || (!stack_sh && v.ne + 1 > rp.scratch_stack) ||
+        ((!node_sh || !stack_sh) && !rp.scratch)) {
+      if (lane == 0) {
+        atomicOr(&r.stats[2], kStBad);
+        StoreRelease(&rp.done[s], 1u);
+      }
+      continue;
+    }
+    uint8_t* base = rp.scratch ? rp.scratch + gw * ScratchPer(rp.scratch_cnt, rp.scratch_stack) : nullptr;
+    uint32_t* stack = stack_sh ? sh.stack : reinterpret_cast<uint32_t*>(base);
     float* vals;
     uint32_t* ids;
-    const uint32_t* rgid = v.gid;
-    const uint32_t* reoff = v.eoff;
-    const uint16_t* redges = v.edges;
-    if (cnt <= rp.shared_cnt && v.ne + 1 <= (uint32_t)rp.shared_stack && v.ne <= (uint32_t)kEdgeSh) {
-      flags = sh.flags;
-      acc = sh.acc;
-      stack = sh.stack;
+    uint16_t* acc;
+    uint8_t* flags;
+    if (node_sh) {
       vals = sh.vals;
       ids = sh.ids;
-      for (int k = lane; k < cnt; k += 32) sh.gid[k] = v.gid[k];
-      for (int k = lane; k <= cnt; k += 32) sh.eoff[k] = v.eoff[k];
-      for (uint32_t k = lane; k < v.ne; k += 32) sh.edges[k] = v.edges[k];
-      rgid = sh.gid;
-      reoff = sh.eoff;
-      redges = sh.edges;
+      acc = sh.acc;
+      flags = sh.flags;
     } else {
-      if ((uint32_t)cnt > rp.scratch_cnt || v.ne + 1 > rp.scratch_stack || !rp.scratch) {
-        if (lane == 0) {
-          atomicOr(&r.stats[2], kStBad);
-          StoreRelease(&rp.done[s], 1u);
-        }
-        continue;
-      }
-      uint8_t* base = rp.scratch + gw * ScratchPer(rp.scratch_cnt, rp.scratch_stack);
-      stack = reinterpret_cast<uint32_t*>(base);
       vals = reinterpret_cast<float*>(base + (size_t)rp.scratch_stack * 4u);
       ids = reinterpret_cast<uint32_t*>(base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 4u);
       acc = reinterpret_cast<uint16_t*>(base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 8u);
       flags = base + (size_t)rp.scratch_stack * 4u + (size_t)rp.scratch_cnt * 10u;
     }
+    const uint32_t* rgid = v.gid;
+    const uint32_t* reoff = v.eoff;
+    const uint16_t* redges = v.edges;
+    if (node_sh) {
+      for (int k = lane; k < cnt; k += 32) sh.gid[k] = v.gid[k];
+      for (int k = lane; k <= cnt; k += 32) sh.eoff[k] = v.eoff[k];
+      rgid = sh.gid;
+      reoff = sh.eoff;
+      if (v.ne <= (uint32_t)kEdgeSh) {
+        for (uint32_t k = lane; k < v.ne; k += 32) sh.edges[k] = v.edges[k];
+        redges = sh.edges;
+      }
+    }
+    unsigned long long tw0 = 0;
+    if (rp.times) tw0 = GlobalTimer();
     // Wait for the predecessors (every earlier seed that may touch these
-    // pixels): spin, then back off, bounded in time.
-    for (int k = lane; k < cnt; k += 32) {
-      const int32_t p = v.pred[k];
-      if (p < 0) continue;
-      unsigned long long t0 = 0;
-      unsigned ns = 0;
-      for (uint32_t it = 0; LoadAcquire(&rp.done[p]) == 0u; ++it) {
-        if (it < 4096) continue;
-        if (ns == 0) t0 = GlobalTimer();
-        ns = ns < 256 ? ns + 32 : 256;
-        __nanosleep(ns);
-        if (GlobalTimer() - t0 > kWaitLimitNs) {
-          atomicOr(&r.stats[2], kStTimeout);
-          break;
-        }
+    // pixels; the distinct ones come first in pred[]). Lane 0 waits for the
+    // latest of them, usually the last to finish; then every lane checks its
+    // own entries.
+    {
+      int32_t latest = -1;
+      for (int k = lane; k < cnt; k += 32) {
+        const int32_t p = v.pred[k];
+        if (p < 0) break;
+        latest = max(latest, p);
+      }
+      for (int o = 16; o > 0; o >>= 1) latest = max(latest, __shfl_xor_sync(0xffffffffu, latest, o));
+      if (lane == 0 && latest >= 0) WaitDone(rp.done + latest, r.stats);
+      __syncwarp();
+      for (int k = lane; k < cnt; k += 32) {
+        const int32_t p = v.pred[k];
+        if (p < 0) break;
+        WaitDone(rp.done + p, r.stats);
       }
     }
     // The acquires above order the predecessors' mask writes before these
     // reads for the whole warp (the barrier orders the lanes).
     __syncwarp();
-    for (int k = lane; k < cnt; k += 32) flags[k] = *(volatile const uint8_t*)(m.mask + rgid[k]);
-    __syncwarp();
-    // The reference's traversal (:1836-2094) on the record: LIFO stack of
-    // (pixel, traversal depth); a pushed pixel that is already fused would be
-    // skipped when popped, so it is not pushed.
-    if (lane == 0) {
-      int nacc = 0, top = 0;
-      if (!flags[0]) stack[top++] = 0u;
-      while (top > 0) {
-        const uint32_t e = stack[--top];
-        const uint32_t k = e & 0xffffu, d = e >> 16;
-        if (flags[k]) continue;
-        flags[k] = 1;
-        acc[nacc++] = (uint16_t)k;
-        if (nacc >= c.max_pix) break;
-        if ((int)d + 1 >= c.max_depth) continue;
-        const uint32_t nd = d + 1 < 0xffffu ? d + 1 : 0xffffu;
-        for (uint32_t q = reoff[k], qe = reoff[k + 1]; q < qe; ++q) {
-          const uint32_t j = redges[q];
-          if (!flags[j]) stack[top++] = j | (nd << 16);
-        }
+    unsigned long long tw1 = 0;
+    if (rp.times) tw1 = GlobalTimer();
+    // Masks are read from L2 (ld.global.cg): other SMs wrote them; a batch of
+    // loads is in flight at once.
+    {
+      int k = lane;
+      for (; k + 96 < cnt; k += 128) {
+        const uint8_t a0 = __ldcg(m.mask + rgid[k]), a1 = __ldcg(m.mask + rgid[k + 32]),
+                      a2 = __ldcg(m.mask + rgid[k + 64]), a3 = __ldcg(m.mask + rgid[k + 96]);
+        flags[k] = a0;
+        flags[k + 32] = a1;
+        flags[k + 64] = a2;
+        flags[k + 96] = a3;
       }
-      sh.nacc = nacc;
+      for (; k < cnt; k += 32) flags[k] = __ldcg(m.mask + rgid[k]);
+    }
+    if (rp.level) {  // profiling: the longest chain of waits ending at this seed
+      uint32_t lv = 0;
+      for (int k = lane; k < cnt; k += 32) {
+        const int32_t p = v.pred[k];
+        if (p < 0) break;
+        lv = max(lv, *(volatile const uint32_t*)(rp.level + p));
+      }
+      for (int o = 16; o > 0; o >>= 1) lv = max(lv, __shfl_xor_sync(0xffffffffu, lv, o));
+      if (lane == 0) {
+        rp.level[s] = lv + 1;
+        atomicMax(rp.chain, lv + 1);
+      }
+    }
+    __syncwarp();
+    unsigned long long tw_m = 0;
+    if (rp.times) tw_m = GlobalTimer();
+    // Which record pixels the traversal fuses. Without a binding limit it fuses
+    // exactly the pixels reachable from the seed through pixels not fused yet:
+    // the warp finds them in parallel (state 0 free, 1 fused before, 2 reached,
+    // 3 expanded). The limits cannot bind when at most min(max_num_pixels,
+    // max_traversal_depth) pixels are reachable (a pixel's traversal depth is
+    // below the number fused); otherwise lane 0 replays the traversal itself.
+    bool in_order = false;
+    {
+      volatile uint8_t* vf = flags;
+      if (lane == 0 && vf[0] == 0) vf[0] = 2;
+      __syncwarp();
+      for (;;) {
+        bool any = false;
+        for (int k = lane; k < cnt; k += 32) {
+          if (vf[k] != 2) continue;
+          vf[k] = 3;
+          any = true;
+          for (uint32_t q = reoff[k], qe = reoff[k + 1]; q < qe; ++q) {
+            const uint32_t j = redges[q];
+            if (vf[j] == 0) vf[j] = 2;
+          }
+        }
+        __syncwarp();
+        if (!__any_sync(0xffffffffu, any)) break;
+      }
+      int reach = 0;
+      for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int k = k0 + lane;
+        const bool a = k < cnt && vf[k] == 3;
+        const unsigned bal = __ballot_sync(0xffffffffu, a);
+        if (a) acc[reach + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)k;
+        reach += __popc(bal);
+      }
+      if (rp.times && lane == 0) {
+        atomicAdd(rp.times + 3, (unsigned long long)cnt);
+        atomicAdd(rp.times + 4, (unsigned long long)reach);
+        if (reach > c.max_pix || reach > c.max_depth) atomicAdd(rp.times + 5, 1ull);
+      }
+      if (reach > c.max_pix || reach > c.max_depth) {
+        for (int k = lane; k < cnt; k += 32) vf[k] = vf[k] == 1 ? 1 : 0;
+        __syncwarp();
+        if (lane == 0) reach = SeqTraversal(flags, stack, acc, reoff, redges, c.max_pix, c.max_depth);
+        reach = __shfl_sync(0xffffffffu, reach, 0);
+        in_order = true;
+      }
+      if (lane == 0) sh.nacc = reach;
     }
     __syncwarp();
     const int n = sh.nacc;
+    unsigned long long tw_b = 0;
+    if (rp.times) tw_b = GlobalTimer();
     for (int i = lane; i < n; i += 32) *(volatile uint8_t*)(m.mask + rgid[acc[i]]) = 1;
     // Release the successors: the barrier orders every lane's mask writes
     // before lane 0's release store.
     __syncwarp();
     if (lane == 0) StoreRelease(&rp.done[s], 1u);
+    if (rp.times && lane == 0) {
+      const unsigned long long tw2 = GlobalTimer();
+      atomicAdd(rp.times, tw1 - tw0);
+      atomicAdd(rp.times + 1, tw2 - tw1);
+      atomicAdd(rp.times + 2, 1ull);
+      atomicAdd(rp.times + 6, tw_m - tw1);
+      atomicAdd(rp.times + 7, tw_b - tw_m);
+      atomicAdd(rp.times + 8, tw2 - tw_b);
+    }
     // The fused point (:2098-2180).
     if (n < c.min_pix) continue;
     // Images of the cluster, ascending.
@@ -792,16 +1136,26 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     pt.r = rgb[0];
     pt.g = rgb[1];
     pt.b = rgb[2];
-    // Mean gradient in traversal order, then the score (:2157-2166).
-    for (int i = lane; i < n; i += 32) vals[i] = m.G[rgid[acc[i]]];
-    __syncwarp();
-    float m_conf = 0.0f;
-    if (lane == 0) {
-      for (int i = 0; i < n; ++i) m_conf = __fadd_rn(m_conf, vals[i]);
-      m_conf = __fdiv_rn(m_conf, (float)n);
+    // Mean gradient in traversal order, then the score (:2157-2166). The mean
+    // only counts below three images; it needs the pixels in the order the
+    // reference fused them, which the parallel search does not give.
+    float m_conf = 1.0f;
+    if (nvis < 3) {
+      if (!in_order) {
+        for (int k = lane; k < cnt; k += 32) flags[k] = flags[k] == 1 ? 1 : 0;
+        __syncwarp();
+        if (lane == 0) SeqTraversal(flags, stack, acc, reoff, redges, c.max_pix, c.max_depth);
+        __syncwarp();
+      }
+      for (int i = lane; i < n; i += 32) vals[i] = m.G[rgid[acc[i]]];
+      __syncwarp();
+      if (lane == 0) {
+        m_conf = 0.0f;
+        for (int i = 0; i < n; ++i) m_conf = __fadd_rn(m_conf, vals[i]);
+        m_conf = __fdiv_rn(m_conf, (float)n);
+      }
+      m_conf = __shfl_sync(0xffffffffu, m_conf, 0);
     }
-    m_conf = __shfl_sync(0xffffffffu, m_conf, 0);
-    if (nvis >= 3) m_conf = 1.0f;
     m_conf = __fsub_rn(1.0f, m_conf);
     __syncwarp();
     for (int i = lane + 1; i < n; i += 32) vals[i - 1] = v.derr[acc[i]];
@@ -1004,11 +1358,18 @@ struct smvs_fusion {
   uint64_t num_points = 0, num_vis = 0;
   bool ran = false;
   int replay_blocks = 0;
+  int closure_blocks = 0;
+  uint16_t* d_stage = nullptr;  // the closure warps' push-list staging
   int cap_closure = kCap, cap_replay = kCap, cap_stack = kStackSh;
+  uint32_t* d_level = nullptr;  // profiling: per-seed dependency depth, per-image longest chain
+  uint32_t* d_chain = nullptr;
+  unsigned long long* d_times = nullptr;  // profiling: per image [wait ns, post-wait ns, seeds]
+  size_t level_cap = 0;
   int64_t launches = 0;
   std::vector<int> h_rows;
   bool profiling = false;
-  struct Timed { int kind; cudaEvent_t a, b; };
+  struct Timed { int kind, image; cudaEvent_t a, b; };
+  std::vector<double> prof_image_ms;  // 4 per image in fusion order
   std::vector<Timed> timed;
   int prof_count[4] = {0, 0, 0, 0};
   double prof_ms[4] = {0, 0, 0, 0};
@@ -1028,7 +1389,7 @@ struct ProfScope {
   ~ProfScope() {
     if (!a) return;
     cudaEventRecord(b, f->stream);
-    f->timed.push_back({kind, a, b});
+    f->timed.push_back({kind, (int)f->order.size(), a, b});
   }
 };
 
@@ -1038,6 +1399,8 @@ void Harvest(smvs_fusion* f) {
     if (cudaEventSynchronize(t.b) == cudaSuccess && cudaEventElapsedTime(&ms, t.a, t.b) == cudaSuccess) {
       f->prof_count[t.kind] += 1;
       f->prof_ms[t.kind] += ms;
+      if ((size_t)(4 * t.image + 4) > f->prof_image_ms.size()) f->prof_image_ms.resize(4 * t.image + 4, 0.0);
+      f->prof_image_ms[4 * t.image + t.kind] += ms;
     }
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
@@ -1078,6 +1441,7 @@ void FreeAll(smvs_fusion* f) {
     Free(f, f->d_shear); Free(f, f->d_ticket); Free(f, f->d_n_over); Free(f, f->d_stats);
     Free(f, f->d_used); Free(f, f->d_vis_cursor); Free(f, f->d_totals);
     Free(f, f->d_out_pts); Free(f, f->d_out_visoff); Free(f, f->d_out_vis);
+    Free(f, f->d_level); Free(f, f->d_chain); Free(f, f->d_stage); Free(f, f->d_times);
   }
   if (f->stream) cudaStreamSynchronize(f->stream);
   if (f->own_stream && f->stream) cudaStreamDestroy(f->stream);
@@ -1258,20 +1622,22 @@ int FuseImage(smvs_fusion* f, int image) {
   // 1. Closure records (the pool grows until every record fits).
   uint32_t stats[3] = {0, 0, 0}, n_over = 0;
   unsigned long long used = 0;
-  for (int attempt = 0;; ++attempt) {
-    ImageStartKernel<<<1, 1, 0, f->stream>>>(f->d_shear, f->d_ticket, f->d_used, f->d_vis_cursor, f->d_n_over,
-                                             f->d_stats);
+  ImageStartKernel<<<1, 1, 0, f->stream>>>(f->d_shear, f->d_ticket, f->d_used, f->d_vis_cursor, f->d_n_over,
+                                           f->d_stats);
+  ++f->launches;
+  {
+    ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
+    ClosureKernel<<<f->closure_blocks, 32 * kClosureWarps, kClosureSmem, f->stream>>>(m, f->consts, im, Recs(f),
+                                                                                         0, f->d_stage);
     ++f->launches;
-    {
-      ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
-      ClosureKernel<<<Blocks(nseeds, 128), 128, 0, f->stream>>>(m, f->consts, im, Recs(f));
-      ++f->launches;
-    }
-    FU_CUDA(cudaGetLastError());
+  }
+  FU_CUDA(cudaGetLastError());
+  uint32_t big_done = 0;
+  for (int attempt = 0;; ++attempt) {
     if ((st = ReadStats(f, stats, &n_over, &used))) return st;
-    if (!(stats[2] & kStPool) && n_over > 0) {
+    if (n_over > big_done) {  // seeds over the closure pass's capacity
       if (!f->d_big_scratch && (st = Alloc(f, &f->d_big_scratch, (size_t)kBigBatch * kBigStride))) return st;
-      for (uint32_t first = 0; first < n_over; first += kBigBatch) {
+      for (uint32_t first = big_done; first < n_over; first += kBigBatch) {
         const uint32_t count = std::min<uint32_t>(kBigBatch, n_over - first);
         ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
         ClosureBigKernel<<<Blocks(count, 64), 64, 0, f->stream>>>(m, f->consts, im, Recs(f), first, count,
@@ -1279,6 +1645,7 @@ int FuseImage(smvs_fusion* f, int image) {
         ++f->launches;
       }
       FU_CUDA(cudaGetLastError());
+      big_done = n_over;
       if ((st = ReadStats(f, stats, &n_over, &used))) return st;
     }
     if (stats[2] & kStBig)
@@ -1286,15 +1653,28 @@ int FuseImage(smvs_fusion* f, int image) {
     if (stats[2] & kStBad) return Fail(SMVS_ECUDA, "fusion: inconsistent cluster record (image %d)", image);
     if (!(stats[2] & kStPool)) break;
     if (attempt >= 8) return Fail(SMVS_ENOMEM, "fusion: record pool cannot grow further");
-    // Grow the pool to what this image asked for, plus a margin.
+    // Grow the pool to what this image asked for, plus a margin, keeping the
+    // records that fit; only the seeds whose records did not fit run again.
+    const size_t old_words = f->pool_words;
     const size_t want = (size_t)std::min<unsigned long long>(used + used / 4 + (1ull << 20), 0xfffffff0ull);
-    if (want <= f->pool_words) return Fail(SMVS_ENOMEM, "fusion: record pool limit (16 GB) reached");
+    if (want <= old_words) return Fail(SMVS_ENOMEM, "fusion: record pool limit (16 GB) reached");
+    uint32_t* grown = nullptr;
+    if ((st = Alloc(f, &grown, want))) return st;
+    FU_CUDA(cudaMemcpyAsync(grown, f->d_pool, old_words * sizeof(uint32_t), cudaMemcpyDeviceToDevice, f->stream));
     Free(f, f->d_pool);
+    f->d_pool = grown;
     f->pool_words = want;
-    if ((st = Alloc(f, &f->d_pool, f->pool_words))) return st;
-    const uint32_t zero = 0;
-    FU_CUDA(cudaMemcpyAsync(f->d_stats + 2, &zero, sizeof(zero), cudaMemcpyHostToDevice, f->stream));
-    FU_CUDA(cudaStreamSynchronize(f->stream));
+    const unsigned long long resume = old_words;
+    const uint32_t status = stats[2] & ~kStPool;
+    FU_CUDA(cudaMemcpyAsync(f->d_used, &resume, sizeof(resume), cudaMemcpyHostToDevice, f->stream));
+    FU_CUDA(cudaMemcpyAsync(f->d_stats + 2, &status, sizeof(status), cudaMemcpyHostToDevice, f->stream));
+    {
+      ProfScope ps(f, SMVS_FUSION_KERNEL_CLOSURE);
+      ClosureKernel<<<f->closure_blocks, 32 * kClosureWarps, kClosureSmem, f->stream>>>(m, f->consts, im,
+                                                                                           Recs(f), 1, f->d_stage);
+      ++f->launches;
+    }
+    FU_CUDA(cudaGetLastError());
   }
   const uint32_t max_cnt = stats[0], max_ne = stats[1];
   // 2. Claims and predecessors.
@@ -1354,6 +1734,26 @@ int FuseImage(smvs_fusion* f, int image) {
     rp.scratch_stack = f->d_replay_scratch ? f->replay_scratch_stack : 0;
     rp.shared_cnt = f->cap_replay;
     rp.shared_stack = f->cap_stack;
+    rp.level = nullptr;
+    rp.chain = nullptr;
+    rp.times = nullptr;
+    if (f->profiling) {
+      if (nseeds > f->level_cap) {
+        Free(f, f->d_level);
+        f->level_cap = nseeds;
+        if ((st = Alloc(f, &f->d_level, nseeds))) { f->level_cap = 0; return st; }
+      }
+      if (!f->d_chain && (st = Alloc(f, &f->d_chain, 2 * (size_t)f->num_views))) return st;
+      const int k = (int)f->order.size();
+      FU_CUDA(cudaMemsetAsync(f->d_chain + k, 0, sizeof(uint32_t), f->stream));
+      FU_CUDA(cudaMemcpyAsync(f->d_chain + f->num_views + k, f->d_shear, sizeof(uint32_t),
+                              cudaMemcpyDeviceToDevice, f->stream));
+      rp.level = f->d_level;
+      rp.chain = f->d_chain + k;
+      if (!f->d_times && (st = Alloc(f, &f->d_times, 9 * (size_t)f->num_views))) return st;
+      FU_CUDA(cudaMemsetAsync(f->d_times + 9 * k, 0, 9 * sizeof(unsigned long long), f->stream));
+      rp.times = f->d_times + 9 * k;
+    }
     ProfScope ps(f, SMVS_FUSION_KERNEL_REPLAY);
     ReplayKernel<<<f->replay_blocks, 32 * kReplayWarps, 0, f->stream>>>(m, f->consts, Recs(f), rp);
     ++f->launches;
@@ -1517,7 +1917,21 @@ int smvs_fusion_create(const smvs_fusion_options* opt, const smvs_fusion_view* v
   uint64_t max_px = 1;
   for (int v = 0; v < num_views; ++v)
     if (f->used[v]) max_px = std::max<uint64_t>(max_px, (uint64_t)views[v].width * views[v].height);
-  f->pool_words = (size_t)std::min<uint64_t>(max_px * 64ull, 0xfffffff0ull);
+  // A seed's record holds at most the pixels within the reprojection radius of
+  // its point in the image and in each overlapping image (about 16 each for
+  // the default 2 pixels), each with one push per overlapping image. Start the
+  // pool at that bound for the largest image (within a quarter of the free
+  // device memory); it grows if an image needs more.
+  int max_deg = 0;
+  for (int v = 0; v < num_views; ++v) max_deg = std::max(max_deg, overlap_offsets[v + 1] - overlap_offsets[v]);
+  const double radius = std::max(opt->max_reproj_error, 0.5);
+  const uint64_t disk = (uint64_t)std::ceil((2.0 * radius + 1.0) * (2.0 * radius + 1.0));
+  const uint32_t cnt_est = (uint32_t)std::min<uint64_t>(kCap, disk * (uint64_t)(1 + max_deg));
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = 0;
+  uint64_t est = max_px * (uint64_t)RecWords(cnt_est, cnt_est * (uint32_t)max_deg);
+  est = std::min<uint64_t>(est, std::max<uint64_t>(free_b / 16, max_px * 64ull));
+  f->pool_words = (size_t)std::min<uint64_t>(std::max<uint64_t>(est, max_px * 64ull), 0xfffffff0ull);
   if ((st = Alloc(f, &f->d_pool, f->pool_words))) return fail(st);
   auto up = [&](void* dst, const void* src, size_t bytes) -> cudaError_t {
     return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, f->stream);
@@ -1571,6 +1985,14 @@ int smvs_fusion_create(const smvs_fusion_options* opt, const smvs_fusion_view* v
       cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, f->device) != cudaSuccess || per_sm < 1)
     return fail(Fail(SMVS_ECUDA, "fusion: cannot size the replay grid"));
   f->replay_blocks = per_sm * sms;
+  if (cudaFuncSetAttribute(ClosureKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kClosureSmem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ClosureKernel, 32 * kClosureWarps, kClosureSmem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return fail(Fail(SMVS_ECUDA, "fusion: cannot size the closure grid"));
+  f->closure_blocks = per_sm * sms;
+  if ((st = Alloc(f, &f->d_stage, (size_t)f->closure_blocks * kClosureWarps * kEdgeLocal))) return fail(st);
   *out = f;
   return SMVS_OK;
 }
@@ -1673,6 +2095,58 @@ int smvs_fusion_get_profile(smvs_fusion* f, int kind, int* count, double* total_
 }
 
 int64_t smvs_fusion_launch_count(smvs_fusion* f) { return f ? f->launches : 0; }
+
+int smvs_test_fusion_chains(smvs_fusion* f, uint32_t* chains, uint32_t* shears, int capacity, int* count) {
+  if (!f || !count || capacity < 0 || (capacity > 0 && !chains)) return Fail(SMVS_EINVAL, "null argument");
+  if (!f->ran || !f->d_chain) return Fail(SMVS_ESTATE, "fusion chains: run with profiling first");
+  const int n = std::min<int>((int)f->order.size(), capacity);
+  *count = (int)f->order.size();
+  if (n > 0) {
+    FU_CUDA(cudaMemcpyAsync(chains, f->d_chain, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost, f->stream));
+    if (shears)
+      FU_CUDA(cudaMemcpyAsync(shears, f->d_chain + f->num_views, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                              f->stream));
+    FU_CUDA(cudaStreamSynchronize(f->stream));
+  }
+  return SMVS_OK;
+}
+
+int smvs_test_fusion_image_ms(smvs_fusion* f, double* ms, int capacity, int* count) {
+  if (!f || !count || capacity < 0 || (capacity > 0 && !ms)) return Fail(SMVS_EINVAL, "null argument");
+  Harvest(f);
+  const int n = (int)(f->prof_image_ms.size() / 4);
+  *count = n;
+  for (int i = 0; i < std::min(n, capacity) * 4; ++i) ms[i] = f->prof_image_ms[i];
+  return SMVS_OK;
+}
+
+int smvs_test_fusion_replay_times(smvs_fusion* f, double* out, int capacity, int* count) {
+  if (!f || !count || capacity < 0 || (capacity > 0 && !out)) return Fail(SMVS_EINVAL, "null argument");
+  if (!f->ran || !f->d_times) return Fail(SMVS_ESTATE, "fusion replay times: run with profiling first");
+  const int n = (int)f->order.size();
+  *count = n;
+  std::vector<unsigned long long> t(9 * (size_t)n);
+  if (n > 0) {
+    FU_CUDA(cudaMemcpyAsync(t.data(), f->d_times, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                            f->stream));
+    FU_CUDA(cudaStreamSynchronize(f->stream));
+  }
+  for (int i = 0; i < std::min(n, capacity); ++i) {
+    const unsigned long long* ti = t.data() + 9 * i;
+    const double seeds = (double)std::max<unsigned long long>(ti[2], 1);
+    double* o = out + 9 * i;
+    o[0] = (double)ti[0] / seeds / 1000.0;
+    o[1] = (double)ti[1] / seeds / 1000.0;
+    o[2] = (double)ti[2];
+    o[3] = (double)ti[3] / seeds;
+    o[4] = (double)ti[4] / seeds;
+    o[5] = (double)ti[5];
+    o[6] = (double)ti[6] / seeds / 1000.0;
+    o[7] = (double)ti[7] / seeds / 1000.0;
+    o[8] = (double)ti[8] / seeds / 1000.0;
+  }
+  return SMVS_OK;
+}
 
 int smvs_test_fusion_caps(int closure_cap, int replay_cap, int replay_stack) {
   if (closure_cap < 0 || replay_cap < 0 || replay_stack < 0 || (replay_stack > 0 && replay_stack < 2))

@@ -182,6 +182,40 @@ class StereoFusion:
             out[name] = (cnt.value, ms.value)
         return out
 
+    def DependencyChains(self, with_shear: bool = False):
+        """Per fused image, the longest chain of seeds that waited on one another
+        (recorded when profiling was on during Run); with_shear also returns the
+        shear K of each image's ticket order."""
+        buf = np.zeros(max(len(self._shape), 1), dtype=np.uint32)
+        shr = np.zeros_like(buf)
+        cnt = C.c_int()
+        N.check(N.lib().smvs_test_fusion_chains(self._handle(), buf.ctypes.data, shr.ctypes.data, len(buf),
+                                                C.byref(cnt)))
+        n = min(cnt.value, len(buf))
+        chains = [int(x) for x in buf[:n]]
+        return (chains, [int(x) for x in shr[:n]]) if with_shear else chains
+
+    def ImageProfile(self) -> list:
+        """With profiling: per fused image, {kernel kind: device ms}."""
+        buf = np.zeros(4 * max(len(self._shape), 1), dtype=np.float64)
+        cnt = C.c_int()
+        N.check(N.lib().smvs_test_fusion_image_ms(self._handle(), buf.ctypes.data, len(buf) // 4, C.byref(cnt)))
+        n = min(cnt.value, len(buf) // 4)
+        return [{name: round(float(buf[4 * i + k]), 3) for k, name in enumerate(N.FUSION_KERNEL_NAMES)}
+                for i in range(n)]
+
+    def ReplayTimes(self) -> list:
+        """With profiling: per fused image (mean us waiting, mean us from the end
+        of the wait to the release, seeds with a record, mean record size, mean
+        reachable set, seeds replayed one pixel at a time, mean us reading masks,
+        finding the fused pixels, marking and releasing)."""
+        buf = np.zeros(9 * max(len(self._shape), 1), dtype=np.float64)
+        cnt = C.c_int()
+        N.check(N.lib().smvs_test_fusion_replay_times(self._handle(), buf.ctypes.data, len(buf) // 9,
+                                                      C.byref(cnt)))
+        n = min(cnt.value, len(buf) // 9)
+        return [tuple(round(float(x), 3) for x in buf[9 * i:9 * i + 9]) for i in range(n)]
+
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_fusion_launch_count(self._handle()))
 

@@ -112,8 +112,17 @@ def test_profile_and_errors(planes):
         prof = f.Profile()
         assert prof["closure"][0] >= 5 and prof["replay"][0] == 5
         assert all(ms >= 0 for _, ms in prof.values())
+        chains = f.DependencyChains()
+        assert len(chains) == 5 and all(c >= 1 for c in chains)
+        pts = f.GetFusedPoints().copy()
+    # Profiling adds the chain bookkeeping to the replay; results do not change.
+    assert np.array_equal(pts.view(np.uint8), O.fusion_run(FusionOptions(), ims, ov)["points"].view(np.uint8))
+    with StereoFusion(FusionOptions(), ims, ov) as f:
+        f.Run()
         with pytest.raises(N.SmvsError):
-            f.Run()
+            f.Run()  # Run may be called once
+        with pytest.raises(N.SmvsError):
+            f.DependencyChains()  # recorded only with profiling
 
 
 @pytest.mark.parametrize("depth", [100, 6])
