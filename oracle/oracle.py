@@ -62,6 +62,9 @@ def lib():
         h.orc_fusion_run.restype = C.c_void_p
         h.orc_fusion_run.argtypes = [C.POINTER(N.smvs_fusion_options), C.POINTER(N.smvs_fusion_view), C.c_int,
                                      C.c_void_p, C.c_void_p, C.c_int]
+        h.orc_fusion_run_threads.restype = C.c_void_p
+        h.orc_fusion_run_threads.argtypes = [C.POINTER(N.smvs_fusion_options), C.POINTER(N.smvs_fusion_view), C.c_int,
+                                             C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         h.orc_fusion_sizes.restype = C.c_int
         h.orc_fusion_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t), C.POINTER(C.c_int)]
         h.orc_fusion_copy.restype = C.c_int
@@ -309,17 +312,19 @@ def init_from_dense_points(width, height, K, R, T, xyz, normals, level=2):
     return d, n, (r[0], r[1])
 
 
-def fusion_run(options, images, overlapping_images, max_images: int = 0, masks: bool = True) -> dict:
+def fusion_run(options, images, overlapping_images, max_images: int = 0, masks: bool = True,
+               threads: int = 1) -> dict:
     """StereoFusion's image loop on the CPU (smvs_oracle_fusion.c) with the
     arguments of sensemap_b200.fusion.StereoFusion: points (structured array),
     visibility CSR (vis_offsets, vis_images), the image order and each image's
-    fused-pixel mask."""
+    fused-pixel mask. threads > 1 runs the reference's concurrent row slices
+    (for timing only: the result then depends on the timing)."""
     from sensemap_b200.fusion import fusion_structs
     views, off, flat, memory, keep = fusion_structs(images, overlapping_images)
     if memory != N.MEM_HOST:
         raise ValueError("the oracle reads host arrays")
-    h = lib().orc_fusion_run(C.byref(options.to_c()), views, len(images), off.ctypes.data, flat.ctypes.data,
-                             int(max_images))
+    h = lib().orc_fusion_run_threads(C.byref(options.to_c()), views, len(images), off.ctypes.data,
+                                     flat.ctypes.data, int(max_images), int(threads))
     if not h:
         raise ValueError("orc_fusion_run rejected its arguments")
     try:

@@ -99,6 +99,11 @@ int orc_init_from_dense_points(const smvs_view* view, const float* xyz, const fl
  * that many images. Returns a result handle, NULL on bad arguments or no memory. */
 void* orc_fusion_run(const smvs_fusion_options* opt, const smvs_fusion_view* views, int num_views,
                      const int32_t* overlap_offsets, const int32_t* overlap_images, int max_images);
+/* The same with the reference's concurrent row slices on `threads` threads
+ * (threads > 1): a timing baseline whose results depend on the timing. */
+void* orc_fusion_run_threads(const smvs_fusion_options* opt, const smvs_fusion_view* views, int num_views,
+                             const int32_t* overlap_offsets, const int32_t* overlap_images, int max_images,
+                             int threads);
 int orc_fusion_sizes(void* h, size_t* num_points, size_t* num_vis, int* order_count);
 int orc_fusion_copy(void* h, smvs_fused_point* points, uint64_t* vis_offsets, uint32_t* vis_images, int* order);
 int orc_fusion_mask(void* h, int view, int width, int height, uint8_t* out);

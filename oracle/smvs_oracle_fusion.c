@@ -35,6 +35,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <omp.h>
+
 #include "smvs_oracle.h"
 
 #define BLANK 3 /* blank_size, fusion.cc:1757 and :1831 */
@@ -232,7 +234,7 @@ static int fuse(fuse_ctx* c, int image, int row0, int col0) {
     const fview* v = &c->fv[e.view];
     const size_t pix = (size_t)e.row * v->W + e.col;
     uint8_t* mask = c->masks[e.view];
-    if (mask[pix]) continue;
+    if (__atomic_load_n(&mask[pix], __ATOMIC_RELAXED)) continue;
     const float depth = c->views[e.view].depth[pix];
     if (!(depth > 0.0f) || !isfinite(depth)) continue;
     float depth_error = 0.0f;
@@ -276,7 +278,7 @@ static int fuse(fuse_ctx* c, int image, int row0, int col0) {
         grad = sqrtf(gx * gx + gy * gy);
       }
     }
-    mask[pix] = 1;
+    __atomic_store_n(&mask[pix], (uint8_t)1, __ATOMIC_RELAXED);
     if (cluster_reserve(cl, n + 1)) return -1;
     cl->x[n] = xyz[0];
     cl->y[n] = xyz[1];
@@ -358,11 +360,24 @@ static int fuse(fuse_ctx* c, int image, int row0, int col0) {
   score = (1.0f < mixed) ? 1.0f : mixed;
   if (!isfinite(score)) return 0;
   p.score = score;
-  return emit_point(c, &p, cl->vis, nvis);
+  int rc;
+#pragma omp critical(orc_fusion_emit)
+  rc = emit_point(c, &p, cl->vis, nvis);
+  return rc;
 }
 
 void* orc_fusion_run(const smvs_fusion_options* opt, const smvs_fusion_view* views, int nv, const int32_t* ov_off,
                      const int32_t* ov_img, int max_images) {
+  return orc_fusion_run_threads(opt, views, nv, ov_off, ov_img, max_images, 1);
+}
+
+/* threads > 1: the reference's concurrent FuseImage (:1201-1205): `threads`
+ * row slices of each image run at once on that many OpenMP threads, sharing
+ * the pixel masks without order (relaxed atomics where the reference races)
+ * and appending points under a lock. Results then depend on the timing, as
+ * the reference's do: this form is a timing baseline, not a checker. */
+void* orc_fusion_run_threads(const smvs_fusion_options* opt, const smvs_fusion_view* views, int nv,
+                             const int32_t* ov_off, const int32_t* ov_img, int max_images, int threads) {
   if (!opt || !views || nv < 1 || !ov_off || (ov_off[nv] > 0 && !ov_img) || opt->min_num_pixels < 2 ||
       opt->max_num_pixels < opt->min_num_pixels || opt->max_traversal_depth < 1 || opt->step_size < 1 ||
       opt->num_slices < 1 || opt->min_num_visible_images < 0)
@@ -421,16 +436,40 @@ void* orc_fusion_run(const smvs_fusion_options* opt, const smvs_fusion_view* vie
     for (int image = start; ok && image >= 0; image = find_next_image(image, nv, ov_off, ov_img, used, fused, views)) {
       if (!used[image]) continue;
       if (max_images > 0 && o->order_count >= max_images) break;
-      const int W = views[image].width, H = views[image].height, T = opt->num_slices;
+      const int W = views[image].width, H = views[image].height;
+      const int T = threads > 1 ? threads : opt->num_slices;
       const int hs = (H + T - 1) / T;
-      for (int t = 0; ok && t < T; ++t) { /* FuseImage (:1730-1792), slice t */
-        const int limit = hs * (t + 1) < H ? hs * (t + 1) : H;
-        const int row_end = limit < H - BLANK ? limit : H - BLANK;
-        for (int row = hs * t > BLANK ? hs * t : BLANK; ok && row < row_end; row += opt->step_size)
-          for (int col = BLANK; ok && col < W - BLANK; col += opt->step_size) {
-            if (o->masks[image][(size_t)row * W + col]) continue;
-            ok = fuse(&c, image, row, col) == 0;
+      if (threads <= 1) {
+        for (int t = 0; ok && t < T; ++t) { /* FuseImage (:1730-1792), slice t */
+          const int limit = hs * (t + 1) < H ? hs * (t + 1) : H;
+          const int row_end = limit < H - BLANK ? limit : H - BLANK;
+          for (int row = hs * t > BLANK ? hs * t : BLANK; ok && row < row_end; row += opt->step_size)
+            for (int col = BLANK; ok && col < W - BLANK; col += opt->step_size) {
+              if (o->masks[image][(size_t)row * W + col]) continue;
+              ok = fuse(&c, image, row, col) == 0;
+            }
+        }
+      } else {
+        int failed = 0;
+#pragma omp parallel num_threads(T)
+        {
+          fuse_ctx lc = c;
+          lc.stack = NULL;
+          lc.stack_cap = 0;
+          memset(&lc.cl, 0, sizeof(lc.cl));
+          for (int t = omp_get_thread_num(); t < T; t += omp_get_num_threads()) {
+            const int limit = hs * (t + 1) < H ? hs * (t + 1) : H;
+            const int row_end = limit < H - BLANK ? limit : H - BLANK;
+            for (int row = hs * t > BLANK ? hs * t : BLANK; row < row_end; row += opt->step_size)
+              for (int col = BLANK; col < W - BLANK; col += opt->step_size) {
+                if (__atomic_load_n(&o->masks[image][(size_t)row * W + col], __ATOMIC_RELAXED)) continue;
+                if (fuse(&lc, image, row, col)) __atomic_store_n(&failed, 1, __ATOMIC_RELAXED);
+              }
           }
+          cluster_free(&lc.cl);
+          free(lc.stack);
+        }
+        ok = !failed;
       }
       fused[image] = 255;
       o->order[o->order_count++] = image;

@@ -143,3 +143,16 @@ def test_oracle_on_a_larger_scene():
     assert np.all(np.abs(np.sqrt(P["nx"] ** 2 + P["ny"] ** 2 + P["nz"] ** 2) - 1) < 1e-5)
     assert np.all((P["score"] >= 0) & (P["score"] <= 1))
     assert sum(int(m.sum()) for m in r["masks"]) >= 5 * len(P)
+
+
+def test_oracle_concurrent_slices_timing_mode():
+    """The timing baseline with the reference's concurrent row slices: its
+    result depends on the timing, but it fuses the same scene into a similar
+    cloud."""
+    scene = syn.planes_scene(seed=3, width=320, height=240, focal=256.0, num_src=4)
+    ims, ov = syn.fusion_inputs(scene, seed=1)
+    one = O.fusion_run(FusionOptions(), ims, ov, masks=False)
+    many = O.fusion_run(FusionOptions(), ims, ov, masks=False, threads=4)
+    assert abs(len(many["points"]) - len(one["points"])) < 0.1 * len(one["points"])
+    nvis = np.diff(many["vis_offsets"].astype(np.int64))
+    assert nvis.min() >= 3 and many["order"] == one["order"]
