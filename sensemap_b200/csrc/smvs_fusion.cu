@@ -677,23 +677,28 @@ __device__ __forceinline__ RecView OpenRecord(uint32_t* pool, uint32_t off) {
   return v;
 }
 
-__global__ void ClaimCountKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+// One warp per seed in the claim and predecessor kernels: lanes take the
+// record's pixels, so the record is read coalesced and the atomics of a seed
+// are in flight together.
+__global__ void __launch_bounds__(256) ClaimCountKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt) {
+  const uint32_t s = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const uint32_t lane = threadIdx.x & 31;
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
   if (off >= kRetry) return;
   const RecView v = OpenRecord(r.pool, off);
-  for (uint32_t k = 0; k < v.cnt; ++k) atomicAdd(&claim_cnt[v.gid[k]], 1u);
+  for (uint32_t k = lane; k < v.cnt; k += 32) atomicAdd(&claim_cnt[v.gid[k]], 1u);
 }
 
-__global__ void ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt, const uint32_t* claim_off,
-                                uint32_t* claim_list) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt,
+                                                       const uint32_t* claim_off, uint32_t* claim_list) {
+  const uint32_t s = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const uint32_t lane = threadIdx.x & 31;
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
   if (off >= kRetry) return;
   const RecView v = OpenRecord(r.pool, off);
-  for (uint32_t k = 0; k < v.cnt; ++k) {
+  for (uint32_t k = lane; k < v.cnt; k += 32) {
     const uint32_t g = v.gid[k];
     const uint32_t slot = atomicSub(&claim_cnt[g], 1u) - 1u;  // leaves claim_cnt at zero
     claim_list[claim_off[g] + slot] = s;
@@ -702,47 +707,61 @@ __global__ void ClaimFillKernel(FRecs r, uint32_t nseeds, uint32_t* claim_cnt, c
 
 // Predecessor of each (seed, pixel) and the shear K of the ticket order:
 // key(p) < key(s) for every predecessor p of s needs K (i_s - i_p) > j_p - j_s.
-__global__ void PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* claim_off, const uint32_t* claim_list,
-                           int* shear) {
-  const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+// The record's predecessors are written once each at the front of pred[] (the
+// replay only waits for them), the rest -1; the first 64 distinct ones are
+// recognised as repeats, any beyond that may repeat.
+constexpr int kPredSeen = 64;
+
+__global__ void __launch_bounds__(256) PredKernel(FRecs r, uint32_t nseeds, int Cs, const uint32_t* claim_off,
+                                                  const uint32_t* claim_list, int* shear) {
+  __shared__ int32_t seen_all[8][kPredSeen];
+  const uint32_t s = (uint32_t)(((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+  const uint32_t lane = threadIdx.x & 31;
+  int32_t* seen = seen_all[threadIdx.x >> 5];
   if (s >= nseeds) return;
   const uint32_t off = r.rec_off[s];
   if (off >= kRetry) return;
   RecView v = OpenRecord(r.pool, off);
   const int is = (int)(s / (uint32_t)Cs), js = (int)(s - (uint32_t)is * (uint32_t)Cs);
+  const unsigned lt = (1u << lane) - 1u;
   int need = 1;
-  // The record's predecessors, each once, at the front of pred[] (the replay
-  // only waits for them); the first 32 distinct ones are recognised.
-  int32_t seen[32];
-  uint32_t nu = 0, nseen = 0;
-  for (uint32_t k = 0; k < v.cnt; ++k) {
-    const uint32_t g = v.gid[k];
-    // The latest earlier claimant of this pixel (the list is in no order).
+  uint32_t nu = 0;
+  for (uint32_t k0 = 0; k0 < v.cnt; k0 += 32) {
+    const uint32_t k = k0 + lane;
     int32_t best = -1;
-    for (uint32_t q = claim_off[g], end = claim_off[g + 1]; q < end; ++q) {
-      const uint32_t cl = claim_list[q];
-      if (cl < s && (int32_t)cl > best) best = (int32_t)cl;
-    }
-    if (best < 0) continue;
-    bool dup = false;
-    for (uint32_t t = 0; t < nseen; ++t)
-      if (seen[t] == best) {
-        dup = true;
-        break;
+    if (k < v.cnt) {
+      // The latest earlier claimant of this pixel (the list is in no order).
+      const uint32_t g = v.gid[k];
+      for (uint32_t q = claim_off[g], end = claim_off[g + 1]; q < end; ++q) {
+        const uint32_t cl = claim_list[q];
+        if (cl < s && (int32_t)cl > best) best = (int32_t)cl;
       }
-    if (dup) continue;
-    if (nseen < 32) seen[nseen++] = best;
-    v.pred[nu++] = best;  // nu <= k: entries not yet visited are never read
-    const uint32_t p = (uint32_t)best;
-    const int ip = (int)(p / (uint32_t)Cs), jp = (int)(p - (uint32_t)ip * (uint32_t)Cs);
-    if (ip < is) {
-      const int num = jp - js, den = is - ip;
-      const int fl = num >= 0 ? num / den : -((-num + den - 1) / den);
-      need = max(need, fl + 1);
     }
+    bool fresh = best >= 0;
+    const uint32_t known = nu < (uint32_t)kPredSeen ? nu : (uint32_t)kPredSeen;
+    for (uint32_t t = 0; fresh && t < known; ++t)
+      if (seen[t] == best) fresh = false;
+    const unsigned same = __match_any_sync(0xffffffffu, best);
+    fresh = fresh && (same & lt) == 0;  // the first lane holding this value
+    const unsigned nw = __ballot_sync(0xffffffffu, fresh);
+    if (fresh) {
+      const uint32_t pos = nu + (uint32_t)__popc(nw & lt);
+      v.pred[pos] = best;  // pos <= k: this kernel reads no pred[] entry
+      if (pos < (uint32_t)kPredSeen) seen[pos] = best;
+      const uint32_t p = (uint32_t)best;
+      const int ip = (int)(p / (uint32_t)Cs), jp = (int)(p - (uint32_t)ip * (uint32_t)Cs);
+      if (ip < is) {
+        const int num = jp - js, den = is - ip;
+        const int fl = num >= 0 ? num / den : -((-num + den - 1) / den);
+        need = max(need, fl + 1);
+      }
+    }
+    nu += (uint32_t)__popc(nw);
+    __syncwarp();
   }
-  for (uint32_t k = nu; k < v.cnt; ++k) v.pred[k] = -1;
-  if (need > 1) atomicMax(shear, min(need, Cs));
+  for (uint32_t k = nu + lane; k < v.cnt; k += 32) v.pred[k] = -1;
+  for (int o = 16; o > 0; o >>= 1) need = max(need, __shfl_xor_sync(0xffffffffu, need, o));
+  if (lane == 0 && need > 1) atomicMax(shear, min(need, Cs));
 }
 
 // ---- ticket order ------------------------------------------------------------
@@ -1686,12 +1705,12 @@ int FuseImage(smvs_fusion* f, int image) {
       f->claim_list_cap = (size_t)claims + 1024;
       if ((st = Alloc(f, &f->d_claim_list, f->claim_list_cap))) { f->claim_list_cap = 0; return st; }
     }
-    ClaimCountKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt);
+    ClaimCountKernel<<<Blocks(32 * nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt);
     ++f->launches;
     if ((st = Scan(f, f->d_claim_cnt, f->total, f->d_claim_off))) return st;
-    ClaimFillKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt,
+    ClaimFillKernel<<<Blocks(32 * nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, f->d_claim_cnt,
                                                                  f->d_claim_off, f->d_claim_list);
-    PredKernel<<<Blocks(nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, Cs, f->d_claim_off,
+    PredKernel<<<Blocks(32 * nseeds, 256), 256, 0, f->stream>>>(Recs(f), (uint32_t)nseeds, Cs, f->d_claim_off,
                                                            f->d_claim_list, f->d_shear);
     // 3. Ticket order.
     KeyCountKernel<<<Blocks(nkeys, 256), 256, 0, f->stream>>>((uint32_t)nkeys, Rs, Cs, f->d_shear, f->d_keycnt);
