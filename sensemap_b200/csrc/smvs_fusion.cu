@@ -864,9 +864,9 @@ __device__ __forceinline__ void WaitDone(const uint32_t* flag, uint32_t* stats) 
   unsigned long long t0 = 0;
   unsigned ns = 0;
   for (uint32_t it = 0; LoadAcquire(flag) == 0u; ++it) {
-    if (it < 64) continue;
+    if (it < 1024) continue;
     if (ns == 0) t0 = GlobalTimer();
-    ns = ns < 1024 ? ns + 64 : 1024;
+    ns = ns < 256 ? ns + 32 : 256;
     __nanosleep(ns);
     if (GlobalTimer() - t0 > kWaitLimitNs) {
       atomicOr(&stats[2], kStTimeout);
