@@ -819,6 +819,8 @@ struct WarpShared {
   uint16_t edges[kEdgeSh];
   uint16_t acc[kCap];
   uint8_t flags[kCap];
+  uint32_t bits[kCap / 32];  // reachability search: pixels fused before or reached
+  int qtail;
   float med[2];
   int nacc;
 };
@@ -1037,7 +1039,57 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     // max_traversal_depth) pixels are reachable (a pixel's traversal depth is
     // below the number fused); otherwise lane 0 replays the traversal itself.
     bool in_order = false;
-    {
+    if (node_sh) {
+      // Breadth-first search with the record's pixels as bits (fused before,
+      // or reached) and the reached pixels queued in acc: each wave expands
+      // only the frontier.
+      for (int k0 = 0; k0 < cnt; k0 += 32) {
+        const int k = k0 + lane;
+        const unsigned bal = __ballot_sync(0xffffffffu, k < cnt && flags[k] != 0);
+        if (lane == 0) sh.bits[k0 >> 5] = bal;
+      }
+      __syncwarp();
+      if (lane == 0) {
+        int t = 0;
+        if (!(sh.bits[0] & 1u)) {
+          sh.bits[0] |= 1u;
+          acc[0] = 0;
+          t = 1;
+        }
+        sh.qtail = t;
+      }
+      __syncwarp();
+      volatile int* vq = &sh.qtail;
+      volatile uint32_t* vb = sh.bits;
+      int qhead = 0, qt = *vq;
+      __syncwarp();
+      while (qhead < qt) {
+        for (int i = qhead + lane; i < qt; i += 32) {
+          const uint32_t k = acc[i];
+          for (uint32_t q = reoff[k], qe = reoff[k + 1]; q < qe; ++q) {
+            const uint32_t j = redges[q], bit = 1u << (j & 31u);
+            if (vb[j >> 5] & bit) continue;
+            if (!(atomicOr(&sh.bits[j >> 5], bit) & bit)) acc[atomicAdd(&sh.qtail, 1)] = (uint16_t)j;
+          }
+        }
+        __syncwarp();
+        qhead = qt;
+        qt = *vq;
+        __syncwarp();
+      }
+      int reach = qt;
+      if (rp.times && lane == 0) {
+        atomicAdd(rp.times + 3, (unsigned long long)cnt);
+        atomicAdd(rp.times + 4, (unsigned long long)reach);
+        if (reach > c.max_pix || reach > c.max_depth) atomicAdd(rp.times + 5, 1ull);
+      }
+      if (reach > c.max_pix || reach > c.max_depth) {  // flags still hold 1 = fused before
+        if (lane == 0) reach = SeqTraversal(flags, stack, acc, reoff, redges, c.max_pix, c.max_depth);
+        reach = __shfl_sync(0xffffffffu, reach, 0);
+        in_order = true;
+      }
+      if (lane == 0) sh.nacc = reach;
+    } else {
       volatile uint8_t* vf = flags;
       if (lane == 0 && vf[0] == 0) vf[0] = 2;
       __syncwarp();
