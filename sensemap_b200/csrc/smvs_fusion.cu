@@ -419,13 +419,18 @@ struct ClosureShared;
 struct ClosureShared {
   uint32_t keys[kSetSlots];
   uint32_t gid[kCap];
-  float derr[kCap];
-  uint32_t eoff[kCap + 1];
   uint32_t dpre[kCap + 1];             // push counts of the frontier, prefix-summed
   uint32_t ecnt[kCap];
   uint16_t kidx[kSetSlots];
   uint16_t vid[kCap];
 };
+
+// A closure warp's global staging (L2-resident for the whole grid): the push
+// lists, their offsets and the depth errors, each written once and read when
+// the record is written.
+constexpr size_t kStageEoff = 2u * (size_t)kEdgeLocal;                  // u32[kCap + 1]
+constexpr size_t kStageDerr = kStageEoff + 4u * ((size_t)kCap + 1u);   // f32[kCap]
+constexpr size_t kStageBytes = (kStageDerr + 4u * (size_t)kCap + 15u) & ~(size_t)15u;
 
 // Exclusive prefix sum over a[lo..hi) into out[lo..hi], out[lo] = base.
 __device__ __forceinline__ void WarpPrefix(const uint32_t* a, uint32_t* out, int lo, int hi, uint32_t base,
@@ -448,14 +453,17 @@ __device__ __forceinline__ void WarpPrefix(const uint32_t* a, uint32_t* out, int
 
 constexpr size_t kClosureSmem = sizeof(ClosureShared) * kClosureWarps;
 
-// `stage`: kEdgeLocal push-list entries per warp of the grid (global memory;
-// a few MB for the whole grid, so they stay in L2).
+// `stage`: kStageBytes per warp of the grid (global memory; tens of MB for the
+// whole grid, so they stay in L2).
 __global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FConsts c, FImage im, FRecs r,
-                                                                    int only_retry, uint16_t* stage) {
+                                                                    int only_retry, uint8_t* stage) {
   extern __shared__ __align__(16) unsigned char closure_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   ClosureShared& sh = reinterpret_cast<ClosureShared*>(closure_smem)[w];
-  uint16_t* const edges = stage + ((size_t)blockIdx.x * kClosureWarps + w) * kEdgeLocal;
+  uint8_t* const wstage = stage + ((size_t)blockIdx.x * kClosureWarps + w) * kStageBytes;
+  uint16_t* const edges = reinterpret_cast<uint16_t*>(wstage);
+  uint32_t* const eoff = reinterpret_cast<uint32_t*>(wstage + kStageEoff);
+  float* const derr = reinterpret_cast<float*>(wstage + kStageDerr);
   const unsigned lt = (1u << lane) - 1u;
   for (uint32_t s = blockIdx.x * kClosureWarps + w; s < im.nseeds; s += gridDim.x * kClosureWarps) {
     if (only_retry && r.rec_off[s] != kRetry) continue;
@@ -479,8 +487,8 @@ __global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FCo
       sh.kidx[h] = 0;
       sh.gid[0] = sg;
       sh.vid[0] = (uint16_t)im.view;
-      sh.derr[0] = 0.0f;
-      sh.eoff[0] = 0;
+      derr[0] = 0.0f;
+      eoff[0] = 0;
     }
     __syncwarp();
     int cnt = 1, head = 0;
@@ -561,7 +569,7 @@ __global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FCo
             sh.kidx[h] = (uint16_t)j;
             sh.gid[j] = q;
             sh.vid[j] = (uint16_t)u;
-            sh.derr[j] = de;
+            derr[j] = de;
           }
         }
         cnt += __popc(own);
@@ -578,7 +586,7 @@ __global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FCo
         if (ecur > (uint32_t)kEdgeLocal) over = true;
         __syncwarp();
       }
-      if (!over) WarpPrefix(sh.ecnt, sh.eoff, head, tail, sh.eoff[head], lane);
+      if (!over) WarpPrefix(sh.ecnt, eoff, head, tail, eoff[head], lane);
       head = tail;
     }
     if (over) {
@@ -611,11 +619,11 @@ __global__ void __launch_bounds__(32 * kClosureWarps) ClosureKernel(FMaps m, FCo
     uint16_t* redg = rv + 2 * ((cnt + 1) / 2);
     for (int k = lane; k < cnt; k += 32) {
       rg[k] = sh.gid[k];
-      rd[k] = sh.derr[k];
+      rd[k] = derr[k];
       rpd[k] = -1;
       rv[k] = sh.vid[k];
     }
-    for (int k = lane; k <= cnt; k += 32) reo[k] = sh.eoff[k];
+    for (int k = lane; k <= cnt; k += 32) reo[k] = eoff[k];
     for (uint32_t k = lane; k < ne; k += 32) redg[k] = edges[k];
     if (lane == 0) {
       rec[0] = (uint32_t)cnt;
@@ -1430,7 +1438,7 @@ struct smvs_fusion {
   bool ran = false;
   int replay_blocks = 0;
   int closure_blocks = 0;
-  uint16_t* d_stage = nullptr;  // the closure warps' push-list staging
+  uint8_t* d_stage = nullptr;  // the closure warps' global staging
   int cap_closure = kCap, cap_replay = kCap, cap_stack = kStackSh;
   uint32_t* d_level = nullptr;  // profiling: per-seed dependency depth, per-image longest chain
   uint32_t* d_chain = nullptr;
@@ -2063,7 +2071,7 @@ int smvs_fusion_create(const smvs_fusion_options* opt, const smvs_fusion_view* v
       per_sm < 1)
     return fail(Fail(SMVS_ECUDA, "fusion: cannot size the closure grid"));
   f->closure_blocks = per_sm * sms;
-  if ((st = Alloc(f, &f->d_stage, (size_t)f->closure_blocks * kClosureWarps * kEdgeLocal))) return fail(st);
+  if ((st = Alloc(f, &f->d_stage, (size_t)f->closure_blocks * kClosureWarps * kStageBytes))) return fail(st);
   *out = f;
   return SMVS_OK;
 }
