@@ -1,7 +1,7 @@
 """Parity of the CUDA engine (through the C ABI) with the CPU oracle on seeded
 inputs. Tolerances: per-view NCC costs within 2e-3 (median) for the same
-hypothesis; depth within 1 % and normals within 10 degrees (the north-star
-tolerance) on the stated fraction of pixels for iterated runs."""
+hypothesis; depth within 1 % and normals within 10 degrees (the accuracy the
+depth-map stage is held to) on the stated fraction of pixels for iterated runs."""
 import numpy as np
 import pytest
 
