@@ -1678,7 +1678,10 @@ int FuseImage(smvs_fusion* f, int image) {
   }
   const int Rs = (int)f->h_rows.size();
   const int Cs = W - 2 * kBlank > 0 ? (W - 2 * kBlank + step - 1) / step : 0;
-  if (Rs == 0 || Cs == 0) return SMVS_OK;
+  if (Rs == 0 || Cs == 0) {  // no seed pixel: the image is fused all the same
+    FU_CUDA(cudaMemsetAsync(f->d_trav + image, 0, 1, f->stream));
+    return SMVS_OK;
+  }
   const uint64_t nseeds = (uint64_t)Rs * (uint64_t)Cs;
   const uint64_t nkeys = (uint64_t)Cs * (uint64_t)Rs + (uint64_t)Cs;
   int st = EnsureSeeds(f, nseeds, nkeys);

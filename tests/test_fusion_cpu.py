@@ -156,3 +156,17 @@ def test_oracle_concurrent_slices_timing_mode():
     assert abs(len(many["points"]) - len(one["points"])) < 0.1 * len(one["points"])
     nvis = np.diff(many["vis_offsets"].astype(np.int64))
     assert nvis.min() >= 3 and many["order"] == one["order"]
+
+
+def test_oracle_image_without_seed_pixels(tiny):
+    """An image too narrow for a seed (6 pixels: all inside the blank border)
+    is fused without points and never entered by a traversal."""
+    ims, ov = tiny
+    ims = list(ims)
+    im = ims[1]
+    ims[1] = FusionImage(K=im.K, R=im.R, T=im.T, depth=np.ascontiguousarray(im.depth[:, :6]),
+                         normal=np.ascontiguousarray(im.normal[:, :, :6]),
+                         color=np.ascontiguousarray(im.color[:, :6]))
+    r = O.fusion_run(FusionOptions(), ims, ov)
+    _same(r, FP.fuse(FusionOptions(), ims, ov))
+    assert 1 in r["order"] and not r["masks"][1].any()
