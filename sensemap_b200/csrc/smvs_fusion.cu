@@ -8,19 +8,24 @@
 // the reference's Eigen expressions (see the float helpers below).
 //
 // Each image is fused in five steps, all in stream order:
-//   1. closure: every seed pixel (one thread each) collects the pixels its
-//      traversal could ever accept — those that pass its reprojection, depth
-//      and normal tests, are not fused yet and are reachable from it through
-//      such pixels — with the push lists between them (the seed's record);
-//   2. claims: for every pixel the seeds whose records hold it, sorted; each
-//      seed's predecessor on each of its pixels is the previous claimant;
+//   1. closure: every seed pixel (one warp each, its state in shared memory)
+//      collects the pixels its traversal could ever accept — those that pass
+//      its reprojection, depth and normal tests, are not fused yet and are
+//      reachable from it through such pixels — with the push lists between
+//      them in the reference's push order (the seed's record); records over
+//      the shared capacity take a thread-per-seed overflow pass;
+//   2. claims: for every pixel the seeds whose records hold it; each seed's
+//      predecessor on each of its pixels is the latest earlier claimant, and
+//      a record keeps its distinct predecessors;
 //   3. order: a ticket order in which every predecessor comes first (the seed
 //      grid sheared so that key = column + K x row grows along every
 //      predecessor pair);
 //   4. replay: warps take tickets, wait for their predecessors, read the masks
-//      of their record's pixels, replay the reference's depth-first traversal
-//      (explicit stack, limits) on the record, mark the accepted pixels, and
-//      release their successors; then they compute the fused point (medians);
+//      of their record's pixels and find the pixels the reference's traversal
+//      fuses — in parallel (a frontier search) where no limit can bind, else
+//      by replaying its depth-first traversal (explicit stack, limits) — mark
+//      them and release their successors; then they compute the fused point
+//      (medians);
 //   5. compaction of the points in seed order.
 // A traversal only reads or writes the masks of pixels that pass its tests
 // (a pixel that fails them is skipped whether or not it is fused), so two
