@@ -40,7 +40,11 @@ W, H, NSRC, ITERS, RADIUS, STEP = 1600, 1200, 10, 6, 5, 1
 HYP_PER_PIXEL = 14          # 10 propagated + 4 refinement hypotheses per pixel per iteration
 FLOP_PER_TAP = 25           # incremental warp, 1/z, bilinear, 4 moment updates
 METRIC = "depth maps/s (1.6MP,10 src)"
-SWEEP_LAUNCH_DRAM_BYTES = 0.5595e9 + 0.5900e9  # ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch
+CPU_BAND_ROWS = 16         # rows of the CPU oracle's band sample (both passes)
+# DRAM bytes (read + write) of one sweep launch of the bench workload per source
+# storage, from ncu (dram__bytes_read.sum + dram__bytes_write.sum); None until
+# captured for the current kernels.
+SWEEP_DRAM_BYTES: dict = {}
 
 
 def log(*a):
@@ -62,11 +66,10 @@ def parse():
     ap.add_argument("--height", type=int, default=H)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--mode", default="batched", choices=["batched", "engine"],
                     help="batched: views resident once, all jobs of a pass in one batch (smvs_pool); "
                          "engine: one smvs_create/smvs_run per reference view and pass")
-    ap.add_argument("--serving-seconds", type=float, default=12.0,
+    ap.add_argument("--serving-seconds", type=float, default=10.0,
                     help="length of the Poisson-arrival serving measurement (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=2.0, help="job arrivals per second")
     ap.add_argument("--single", action="store_true",
@@ -162,10 +165,10 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def make_options(scene, storage, geometric):
+def make_options(scene, storage, geometric, step=STEP):
     from sensemap_b200.patch_match import PatchMatchOptions
     o = PatchMatchOptions(depth_min=scene.depth_min, depth_max=scene.depth_max, window_radius=RADIUS,
-                          window_step=STEP, sigma_spatial=RADIUS, num_iterations=ITERS,
+                          window_step=step, sigma_spatial=RADIUS, num_iterations=ITERS,
                           geom_consistency=geometric, init_depth_random=not geometric,
                           geom_consistency_regularizer=0.1,  # config/mvs.yaml value
                           image_storage=storage)
@@ -254,26 +257,31 @@ class PoolWorkload:
     """The same scene step through the batched pool: every view resident once,
     11 photometric jobs in one batch, then 11 geometric jobs in one batch."""
 
-    def __init__(self, wl: Workload, block_x: int = 32, ref_tile_tma: bool = True):
+    def __init__(self, wl: Workload, block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 2,
+                 step: int = STEP):
         self.wl = wl
         self.block_x = block_x
         self.ref_tile_tma = ref_tile_tma
+        self.tpp = threads_per_pixel
+        self.step = step
 
-    def _run(self, pool, images):
+    def _run(self, pool, images, on_photo_done=None):
         from sensemap_b200.patch_match import View
         wl, sc = self.wl, self.wl.scene
         for i, v in enumerate(sc.views):
             pool.add_view(i, View(images[i], v.K, v.R, v.T))
-        opt_p = make_options(sc, wl.storage, False)
+        opt_p = make_options(sc, wl.storage, False, self.step)
         photo = []
         for r in range(wl.V):
             opt_p.random_seed = r
             photo.append(pool.submit(opt_p, r, [i for i in range(wl.V) if i != r]))
         pool.run_until_done(photo)
         for j in photo:
+            if on_photo_done is not None:
+                on_photo_done(j)
             pool.keep_maps(j)
             pool.release(j)
-        opt_g = make_options(sc, wl.storage, True)
+        opt_g = make_options(sc, wl.storage, True, self.step)
         geo = []
         for r in range(wl.V):
             opt_g.random_seed = 1000 + r
@@ -284,7 +292,8 @@ class PoolWorkload:
     def new_pool(self, stream):
         from sensemap_b200.pool import DepthMapPool
         return DepthMapPool(memory_budget_bytes=64 << 30, max_active_jobs=self.wl.V, image_storage=self.wl.storage,
-                            sweep_block_x=self.block_x, stream=stream, ref_tile_tma=self.ref_tile_tma)
+                            sweep_block_x=self.block_x, stream=stream, ref_tile_tma=self.ref_tile_tma,
+                            threads_per_pixel=self.tpp)
 
     def step_device(self, stream):
         pool = self.new_pool(stream)
@@ -292,11 +301,15 @@ class PoolWorkload:
         return pool, geo
 
     def step_host(self, stream):
-        """Host images in, geometric depth maps back to host."""
+        """Host images in; every job's depth, normal and confidence maps back to
+        host, for the photometric and the geometric pass (what ProcessProblem
+        reads back and writes, patch_match_controller.cc:4679-4720)."""
         import sensemap_b200._native as NN
+        kinds = (NN.MAP_DEPTH, NN.MAP_NORMAL, NN.MAP_CONF)
         pool = self.new_pool(stream)
-        geo = self._run(pool, self.wl.host)
-        out = [pool.get_map(j, NN.MAP_DEPTH) for j in geo]
+        out = []
+        geo = self._run(pool, self.wl.host, on_photo_done=lambda j: out.extend(pool.get_map(j, k) for k in kinds))
+        out += [pool.get_map(j, k) for j in geo for k in kinds]
         st = pool.stats()
         pool.close()
         h2d = sum(int(t.numel()) * 4 for t in self.wl.host)
@@ -310,39 +323,54 @@ def storage_code(name):
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(scene, storage, seconds_target: float) -> dict:
-    """The oracle (OpenMP transcription of the reference kernel logic) on a
-    band of rows of one photometric pass of the bench workload, scaled to
-    depth maps/s (photometric + geometric pass of a full view)."""
+def cpu_band(scene, maps, rows: int) -> dict:
+    """The oracle (OpenMP transcription of the reference kernel logic, every
+    host thread) on a band of `rows` rows at the middle of view 0, both passes
+    of a depth map: the photometric pass (random initialisation, 6
+    iterations), then the geometric pass (6 iterations) initialised from the
+    band's photometric maps, with the other views' noisy ground-truth maps as
+    the source depth maps. Each pass scores the initial hypotheses of its band
+    and of the rows its sweeps read, and sweeps the band; the pixels of a
+    colour are spread over the threads. Returns both pass times and the depth
+    maps/s a full view would take at this rate (extrapolated by H / rows)."""
     import oracle.oracle as orc
+    from sensemap_b200 import STORE_U8
     from sensemap_b200.patch_match import Problem, View
     V = len(scene.views)
-    views = [View(v.image, v.K, v.R, v.T) for v in scene.views]
-    prob = Problem(0, list(range(1, V)), views)
+    H = scene.views[0].image.shape[0]
+    r0 = H // 2 - rows // 2
+    srcs = list(range(1, V))
     # The reference samples 8-bit textures (patch_match_cuda.cu:229-278): the CPU
     # transcription runs with that storage whatever the GPU form uses.
-    from sensemap_b200 import STORE_U8
-    opt = make_options(scene, STORE_U8, False)
-    Hh = scene.views[0].image.shape[0]
-    r0 = Hh // 2
+    photo = Problem(0, srcs, [View(v.image, v.K, v.R, v.T) for v in scene.views])
     t = time.perf_counter()
-    orc.run(opt, prob, rows=(r0, r0 + 4))
-    t4 = time.perf_counter() - t
-    rows = int(max(4, min(Hh // 2, 4 * seconds_target / max(t4, 1e-3))))
+    ph = orc.run(make_options(scene, STORE_U8, False), photo, rows=(r0, r0 + rows))
+    tp = time.perf_counter() - t
+    d0, n0 = maps[0][0].copy(), maps[0][1].copy()
+    d0[r0:r0 + rows] = ph["depth"][r0:r0 + rows]
+    n0[:, r0:r0 + rows] = ph["normal"][:, r0:r0 + rows]
+    gviews = [View(v.image, v.K, v.R, v.T, depth=d, normal=n) for v, (d, n) in zip(scene.views, maps)]
+    gviews[0] = View(scene.views[0].image, scene.views[0].K, scene.views[0].R, scene.views[0].T, depth=d0, normal=n0)
     t = time.perf_counter()
-    orc.run(opt, prob, rows=(r0, r0 + rows))
-    dt = time.perf_counter() - t
-    per_pass = dt * Hh / rows
-    value = 1.0 / (2.0 * per_pass)
-    return {"value": value, "unit": "depth maps/s", "cores": orc.num_threads(), "kind": "port",
-            "sample": (f"oracle (OpenMP transcription of the reference kernel logic, 8-bit sources) photometric "
-                       f"pass (6 iterations, N={V - 1}) over rows {r0}..{r0 + rows} of a "
-                       f"{scene.views[0].image.shape[1]}x{Hh} view in {dt:.1f} s; scaled by {Hh}/{rows} rows and x2 "
-                       f"for the geometric pass (extrapolated)")}
+    orc.run(make_options(scene, STORE_U8, True), Problem(0, srcs, gviews), rows=(r0, r0 + rows))
+    tg = time.perf_counter() - t
+    per_map = (tp + tg) * H / rows
+    return {"value": 1.0 / per_map, "unit": "depth maps/s", "cores": orc.num_threads(), "kind": "port",
+            "band_rows": rows, "photometric_band_s": tp, "geometric_band_s": tg,
+            "sample": (f"oracle (OpenMP transcription of the reference kernel logic, 8-bit sources), rows "
+                       f"{r0}..{r0 + rows} of view 0 ({scene.views[0].image.shape[1]}x{H}, N={V - 1}): photometric "
+                       f"pass {tp:.2f} s + geometric pass {tg:.2f} s measured; depth maps/s extrapolated by "
+                       f"{H}/{rows} rows")}
+
+
+def cpu_baseline(scene, maps, rows: int) -> dict:
+    return cpu_band(scene, maps, rows)
 
 
 def run_reference(args):
-    world = int(os.environ.get("WORLD_SIZE", "1"))
+    """The reference arm: the oracle's band of both passes (cpu_band), one band
+    per step, on all host threads. The band is sized from the first warm-up
+    step so that the whole run takes about two minutes."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -352,20 +380,27 @@ def run_reference(args):
     oracle_build.build()
     scene = syn.heightfield_scene(seed=0, width=args.width, height=args.height, num_src=args.views - 1,
                                   device="cuda" if torch.cuda.is_available() else "cpu")
-    storage = storage_code(args.storage)
-    per_step = max(2.0, 60.0 / max(1, args.steps + args.warmup))
-    samples = []
-    for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(scene, storage, per_step / 2)
+    maps = syn.noisy_maps(scene, seed=100)
+    total = args.warmup + args.steps
+    rows = CPU_BAND_ROWS
+    samples, band_ms, cb = [], [], None
+    for i in range(total):
+        cb = cpu_band(scene, maps, rows)
+        if i == 0:  # size the band: ~120 s for the whole run, 4..64 rows
+            per_row = (cb["photometric_band_s"] + cb["geometric_band_s"]) / rows
+            rows = int(min(64, max(4, 120.0 / max(1, total) / max(per_row, 1e-6))))
         if i >= args.warmup:
             samples.append(cb["value"])
+            band_ms.append(1000.0 * (cb["photometric_band_s"] + cb["geometric_band_s"]))
     value = statistics.median(samples)
     line = {"metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1000.0 * (args.views) / value, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": statistics.median(band_ms), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": f"heightfield scene, {args.views} views {args.width}x{args.height}, each view "
-                                   f"photometric + geometric PatchMatch (R={RADIUS}, S={STEP}, {ITERS} iterations)",
+                                   f"photometric + geometric PatchMatch (R={RADIUS}, S={STEP}, {ITERS} iterations); "
+                                   f"each step is a {rows}-row band of view 0 through both passes, value extrapolated "
+                                   f"to full views (ms_per_step is the measured band)",
                        "global_batch": args.views, "parallelism": "cpu-openmp"},
             "cpu_baseline": {**cb, "value": value},
             "e2e": {"value": value, "unit": "depth maps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -373,6 +408,157 @@ def run_reference(args):
 
 
 # ---------------------------------------------------------------------------
+def timed_steps(step_fn, steps, warmup, stream, world, clocks=None):
+    """W untimed steps, then K steps bracketed by barrier + synchronize and CUDA
+    events on the launching stream. step_fn() -> (objects to close, launches,
+    getter of (depth, normal) per view). Returns (max-over-ranks ms, launches,
+    getter of the last step, objects of the last step)."""
+    import torch
+    for _ in range(warmup):
+        objs, _, _ = step_fn()
+        torch.cuda.synchronize()
+        for o in objs:
+            o.close()
+    barrier(world)
+    torch.cuda.synchronize()
+    if clocks is not None:
+        clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    keep, launches, getter = [], 0, None
+    ev0.record(stream)
+    for _ in range(steps):
+        objs, n, getter = step_fn()
+        launches += n
+        keep.append(objs)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clock_info = clocks.stop() if clocks is not None else None
+    ms = max_over_ranks(ev0.elapsed_time(ev1), world)
+    for objs in keep[:-1]:
+        for o in objs:
+            o.close()
+    return ms, launches, getter, keep[-1], clock_info
+
+
+def accuracy_of(getter, scene):
+    """Fraction of ground-truth pixels within 1 % depth and within 10 degrees
+    normal, per view and mean."""
+    from sensemap_b200 import synthetic as syn
+    d_acc, n_acc = [], []
+    for i, v in enumerate(scene.views):
+        d, n = getter(i)
+        d_acc.append(syn.depth_accuracy(d, v.depth_gt))
+        n_acc.append(syn.normal_accuracy(n, v.normal_gt, mask=v.depth_gt > 0))
+    return {"within_1pct_gt": float(np.mean(d_acc)), "within_10deg_normal": float(np.mean(n_acc)),
+            "per_view_1pct": [round(a, 4) for a in d_acc]}
+
+
+def pool_step_fn(pw, stream):
+    import sensemap_b200._native as NN
+
+    def step():
+        pool, geo = pw.step_device(stream)
+        return [pool], pool.stats()["launches"], \
+            (lambda i: (pool.get_map(geo[i], NN.MAP_DEPTH), pool.get_map(geo[i], NN.MAP_NORMAL)))
+    return step
+
+
+def engine_step_fn(wl, stream):
+    def step():
+        keep = []
+        geo = wl.step_device(stream, keep)
+        return keep, sum(pm.LaunchCount() for pm in keep), (lambda i: (geo[i].GetDepthMap(), geo[i].GetNormalMap()))
+    return step
+
+
+def reference_kernels_leg(scene, ours_view0, repeats=2) -> dict:
+    """Baseline leg: the reference's own PatchMatch kernels (compiled from its
+    sources into the checker library) on this GPU for view 0 of the bench scene:
+    their launch order, launch shapes, 8-bit layered source texture and a device
+    sync after every launch. The geometric pass of view 0 uses the reference
+    kernels' own photometric maps of every view. Reports seconds per depth map
+    (photometric + geometric pass of view 0, best of `repeats`), its accuracy
+    against ground truth and the agreement of our map of view 0 with it."""
+    import torch
+    from oracle import oracle as O
+    from oracle import ref_oracle as R
+    from sensemap_b200 import STORE_U8
+    from sensemap_b200 import synthetic as syn
+    from sensemap_b200.patch_match import Problem, View
+    if not R.available():
+        return {"unavailable": "reference kernels not built (oracle/_ref)"}
+    V = len(scene.views)
+    fviews = [O.FilterView(v.K, v.R, v.T, v.depth_gt, v.normal_gt) for v in scene.views]
+    plain = [View(v.image, v.K, v.R, v.T) for v in scene.views]
+    photo_maps, poses_of = [], {}
+    for r in range(V):
+        srcs = [i for i in range(V) if i != r]
+        poses_of[r] = O.cross_filter_poses(fviews, (r, srcs))[2]
+        o = make_options(scene, STORE_U8, False)
+        o.random_seed = r
+        res = R.run(o, Problem(r, srcs, plain), poses_of[r])
+        photo_maps.append((res["depth"], res["normal"]))
+    gviews = [View(v.image, v.K, v.R, v.T, depth=d, normal=n) for v, (d, n) in zip(scene.views, photo_maps)]
+    srcs0 = list(range(1, V))
+    t_photo, t_geo, geo = [], [], None
+    for _ in range(repeats):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        R.run(make_options(scene, STORE_U8, False), Problem(0, srcs0, plain), poses_of[0])
+        torch.cuda.synchronize()
+        t_photo.append(time.perf_counter() - t)
+        t = time.perf_counter()
+        o = make_options(scene, STORE_U8, True)
+        o.random_seed = 1000
+        geo = R.run(o, Problem(0, srcs0, gviews), poses_of[0])
+        torch.cuda.synchronize()
+        t_geo.append(time.perf_counter() - t)
+    v0 = scene.views[0]
+    m = v0.depth_gt > 0
+    d_ours, n_ours = ours_view0
+    agree_d = float(np.mean(np.abs(d_ours[m] - geo["depth"][m]) <= 0.01 * np.abs(geo["depth"][m])))
+    agree_n = syn.normal_accuracy(n_ours, geo["normal"] / np.maximum(
+        np.linalg.norm(geo["normal"], axis=0, keepdims=True), 1e-12), mask=m)
+    per_map = min(t_photo) + min(t_geo)
+    return {"what": "the reference's kernel_functions.cu (built with its own flags, --use_fast_math) on this GPU, "
+                    "PatchMatchACMMCuda::Run's launch order and syncs, 8-bit layered source texture; host wall time "
+                    "of one photometric + one geometric pass of view 0 (best of %d)" % repeats,
+            "seconds_per_depth_map": per_map, "depth_maps_per_s": 1.0 / per_map,
+            "photometric_s": min(t_photo), "geometric_s": min(t_geo),
+            "within_1pct_gt": syn.depth_accuracy(geo["depth"], v0.depth_gt),
+            "within_10deg_normal": syn.normal_accuracy(geo["normal"], v0.normal_gt, mask=m),
+            "ours_vs_reference_view0": {"within_1pct_depth": agree_d, "within_10deg_normal": agree_n}}
+
+
+def ncc_fp64_leg(scene, storage, tune, stream, samples=10000) -> dict:
+    """Per-pixel NCC cost error of the GPU against the oracle's FP64 evaluator:
+    one photometric pass of view 0 in the measured form, then for `samples`
+    seeded pixels the GPU's per-view cost of its final hypothesis against the
+    FP64 evaluation of the same hypothesis (direct homography per tap, exact
+    bilinear weights, exact exp)."""
+    import oracle.oracle as orc
+    from sensemap_b200.patch_match import PatchMatchACMMCuda, Problem, View
+    V = len(scene.views)
+    opt = make_options(scene, storage, False)
+    dev_prob = Problem(0, list(range(1, V)), [View(v.image, v.K, v.R, v.T) for v in scene.views])
+    with PatchMatchACMMCuda(opt, dev_prob, stream=stream) as pm:
+        pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"])
+        pm.Run()
+        depth, normal, cost = pm.GetDepthMap(), pm.GetNormalMap(), pm.GetCostMap()
+    rng = np.random.default_rng(11)
+    Hh, Ww = depth.shape
+    rows = rng.integers(0, Hh, samples)
+    cols = rng.integers(0, Ww, samples)
+    _, c64 = orc.eval_costs(opt, dev_prob, rows, cols, depth[rows, cols], normal[:, rows, cols].T)
+    gpu = cost[:, rows, cols].T.astype(np.float64)
+    err = np.abs(gpu - c64).ravel()
+    return {"samples": int(samples) * (V - 1), "median": float(np.median(err)), "p99": float(np.percentile(err, 99)),
+            "frac_below_1e-2": float(np.mean(err < 1e-2)),
+            "what": "GPU per-view NCC cost of the final hypothesis (photometric pass of view 0, %s storage) vs the "
+                    "FP64 evaluation of the same hypothesis" % {1: "u8", 2: "f16", 3: "f32"}.get(storage, "?")}
+
+
 def main():
     args = parse()
     if args.workload == "cross-filter":
@@ -395,6 +581,7 @@ def main():
     from sensemap_b200 import build as engine_build
     from sensemap_b200 import _native as N
     from sensemap_b200 import synthetic as syn
+    from sensemap_b200 import STORE_F32
     engine_build.build()
     N.lib()
     storage = storage_code(args.storage)
@@ -414,65 +601,34 @@ def main():
 
     # Launch shape from the autotuner (one iteration of view 0's photometric
     # pass per candidate, before the timed region; maps do not depend on it).
-    from sensemap_b200.patch_match import autotune
+    from sensemap_b200.patch_match import PatchMatchACMMCuda, autotune
     tune = autotune(make_options(scene, storage, False), wl.problem(0, wl.views(dev_imgs)), stream=sptr, repeats=2)
-    log(f"autotune: block_x={tune['sweep_block_x']} tma={tune['ref_tile_tma']} "
-        f"({', '.join(f'{c['sweep_block_x']}/{int(c['ref_tile_tma'])}: {c['ms_per_sweep']:.2f} ms' for c in tune['candidates'])})")
-    pw = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"])
-    import sensemap_b200._native as NN
+    log(f"autotune: block_x={tune['sweep_block_x']} tpp={tune['threads_per_pixel']} tma={tune['ref_tile_tma']} "
+        f"({', '.join(f'{c['sweep_block_x']}/{c['threads_per_pixel']}: {c['ms_per_sweep']:.2f} ms' for c in tune['candidates'])})")
+    pw = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"],
+                      threads_per_pixel=tune["threads_per_pixel"])
 
-    def device_step():
-        """One step; returns (objects to close, launches, geometric depth getters)."""
-        if args.mode == "engine":
-            keep = []
-            geo = wl.step_device(sptr, keep)
-            return keep, sum(pm.LaunchCount() for pm in keep), [pm.GetDepthMap for pm in geo]
-        pool, geo = pw.step_device(sptr)
-        return [pool], pool.stats()["launches"], [lambda j=j: pool.get_map(j, NN.MAP_DEPTH) for j in geo]
-
-    # Warm-up.
-    for _ in range(args.warmup):
-        objs, _, _ = device_step()
-        torch.cuda.synchronize()
-        for o in objs:
-            o.close()
-    # Timed region (device-resident inputs).
+    # Timed region: the batched form, device-resident inputs.
     clocks = ClockSampler(local)
-    barrier(world)
-    torch.cuda.synchronize()
-    clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    keep, launches = [], 0
-    ev0.record(stream)
-    getters = None
-    for _ in range(args.steps):
-        objs, n, getters = device_step()
-        launches += n
-        keep.append(objs)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    barrier(world)
-    clock_info = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
-    ms = max_over_ranks(ms, world)
+    ms, launches, getter, last, clock_info = timed_steps(
+        pool_step_fn(pw, sptr) if args.mode == "batched" else engine_step_fn(wl, sptr),
+        args.steps, args.warmup, stream, world, clocks)
     depth_maps = args.steps * wl.V * world
     value = depth_maps / (ms / 1000.0)
-    acc = [syn.depth_accuracy(g(), scene.views[i].depth_gt) for i, g in enumerate(getters)]
-    for objs in keep:
-        for o in objs:
-            o.close()
-    del keep
+    acc = accuracy_of(getter, scene)
+    ours_view0 = getter(0)
+    for o in last:
+        o.close()
+    log(f"value {value:.3f} depth maps/s, accuracy {acc['within_1pct_gt']:.4f}")
 
-    # Per-kernel device time (one profiled photometric + geometric pass of view 0).
-    from sensemap_b200.patch_match import PatchMatchACMMCuda
-    prof_keep = []
+    # Per-kernel device time (one profiled photometric pass of view 0).
     views = wl.views(dev_imgs)
     pm = PatchMatchACMMCuda(make_options(scene, storage, False), wl.problem(0, views), stream=sptr)
-    pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"])
+    pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"])
     pm.SetProfiling(True)
     pm.Run()
     prof = pm.Profile()
-    prof_keep.append(pm)
+    pm.close()
     sweep_n, sweep_ms = prof.get("sweep", (0, 0.0))
     T = (2 * RADIUS // STEP + 1) ** 2
     taps_per_launch = (args.width * args.height / 2) * (args.views - 1) * HYP_PER_PIXEL * T
@@ -481,44 +637,86 @@ def main():
     fp32 = ctypes_rate(N, 0)
     tex = ctypes_rate(N, 1)
     peak_taps = min(fp32 / FLOP_PER_TAP, tex)
+    full = (args.width, args.height, args.views) == (W, H, NSRC + 1)
     roof = {"bound": "texture-sampling", "achieved": achieved_tflops, "peak": peak_taps * FLOP_PER_TAP / 1e12,
             "unit": "TFLOP/s", "frac": (taps_per_launch / sweep_avg_s) / peak_taps,
-            # DRAM bytes (read + write) of one launch of this kernel on this workload
-            # (f16 storage), measured with ncu on B200.
-            "traffic": SWEEP_LAUNCH_DRAM_BYTES if (args.width, args.height, args.views) == (W, H, NSRC + 1) else None,
-            "kernel": "SweepKernel<5,1,16>", "taps_per_launch": taps_per_launch, "flop_per_tap": FLOP_PER_TAP,
-            "avg_launch_ms": sweep_avg_s * 1000.0,
+            "traffic": SWEEP_DRAM_BYTES.get(args.storage) if full else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one sweep launch of this workload"
+                              " (profiles/)",
+            "kernel": f"SweepKernel<{RADIUS},{STEP},{tune['threads_per_pixel']}>",
+            "taps_per_launch": taps_per_launch, "flop_per_tap": FLOP_PER_TAP, "avg_launch_ms": sweep_avg_s * 1000.0,
             "peak_source": (f"measured in this process: FP32 FMA {fp32 / 1e12:.1f} TFLOP/s, bilinear texture "
                             f"{tex / 1e9:.0f} Gsample/s; peak = min(FP32/25, texture) taps/s x 25 flop"),
             "kernel_share": {k: round(v[1] / sum(x[1] for x in prof.values()), 4) for k, v in prof.items()}}
-    for p in prof_keep:
-        p.close()
 
     e2e = None
     if not args.no_e2e:
-        # End to end through host buffers (pinned inputs, host outputs).
+        # End to end through host buffers (pinned inputs; depth, normal and
+        # confidence maps of both passes back to host).
         host_step = wl.step_host if args.mode == "engine" else (lambda: pw.step_host(sptr))
         host_step()
         torch.cuda.synchronize()
         barrier(world)
+        e2e_steps = min(args.steps, 3)
         t = time.perf_counter()
         h2d = d2h = 0
-        for _ in range(args.steps):
+        for _ in range(e2e_steps):
             _, h2d, d2h, _ = host_step()
         torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t, world)
-        e2e = {"value": depth_maps / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h}
+        e2e = {"value": e2e_steps * wl.V * world / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+
+    # The plain path: FP32 storage, one engine per reference view and pass.
+    plain_wl = Workload(scene, STORE_F32, dev_imgs, host_imgs)
+    p_steps = min(args.steps, 2)
+    p_ms, p_launches, p_get, p_last, _ = timed_steps(engine_step_fn(plain_wl, sptr), p_steps, 1, stream, world)
+    plain = {"value": p_steps * wl.V * world / (p_ms / 1000.0), "steps": p_steps, "launches": p_launches,
+             "form": "engine (one smvs_create/smvs_run per reference view and pass), FP32 storage, R=5, S=1, default "
+                     "launch shape", **accuracy_of(p_get, scene)}
+    for o in p_last:
+        o.close()
+    log(f"plain {plain['value']:.3f} depth maps/s, accuracy {plain['within_1pct_gt']:.4f}")
+
+    # The autotuner's window-step candidate: the batched form at S=2, accepted
+    # when its ground-truth accuracy is within 0.5 points of the plain path's.
+    pw2 = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"],
+                       threads_per_pixel=tune["threads_per_pixel"], step=2)
+    s_steps = min(args.steps, 4)
+    s_ms, s_launches, s_get, s_last, _ = timed_steps(pool_step_fn(pw2, sptr), s_steps, 1, stream, world)
+    s_acc = accuracy_of(s_get, scene)
+    for o in s_last:
+        o.close()
+    s_value = s_steps * wl.V * world / (s_ms / 1000.0)
+    gap = 100.0 * (plain["within_1pct_gt"] - s_acc["within_1pct_gt"])
+    autotuned = {"window_step": 2 if gap <= 0.5 else STEP, "candidate": {"window_step": 2, "value": s_value,
+                                                                          "steps": s_steps, **s_acc},
+                 "accuracy_gap_pt_vs_plain": gap, "accepted": gap <= 0.5,
+                 "value": s_value if gap <= 0.5 else value,
+                 "ratio_vs_plain": (s_value if gap <= 0.5 else value) / plain["value"],
+                 "gate": "GT depth accuracy (within 1 %) within 0.5 points of the plain path's on this scene"}
+    log(f"window step 2: {s_value:.3f} depth maps/s, accuracy {s_acc['within_1pct_gt']:.4f} (gap {gap:.2f} pt)")
 
     serving = None
     if args.serving_seconds > 0:
-        serving = run_serving(args, wl, sptr)
+        serving = run_serving(args, wl, sptr, tune)
 
-    cpu = None
+    ref_k = ncc = cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(scene, storage, args.cpu_seconds)
-
+        # Baseline legs (after every timed region): the reference's kernels on
+        # this GPU, the FP64 cost check and the CPU transcription.
+        try:
+            ref_k = reference_kernels_leg(scene, ours_view0)
+        except Exception as exc:  # reported, not fatal
+            ref_k = {"unavailable": f"{type(exc).__name__}: {exc}"}
+        ncc = ncc_fp64_leg(scene, storage, tune, sptr)
+        maps = syn.noisy_maps(scene, seed=100)
+        cpu = cpu_baseline(scene, maps, CPU_BAND_ROWS)
     if rank == 0:
+        accuracy = dict(acc)
+        accuracy["ncc_cost_err_fp64"] = ncc
+        if ref_k and "ours_vs_reference_view0" in ref_k:
+            accuracy["vs_reference_kernels"] = ref_k["ours_vs_reference_view0"]
         line = {"metric": METRIC, "value": value, "unit": "depth maps/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -528,32 +726,39 @@ def main():
                            "global_batch": wl.V * world, "parallelism": f"views sharded, {world} replica(s)",
                            "l2": "inputs larger than L2 (11 x 1600x1200 images + maps per step)"},
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "serving": serving,
-                "clocks": clock_info, "autotune": tune,
-                "accuracy": {"within_1pct_gt_mean": float(np.mean(acc)), "per_view": [round(a, 4) for a in acc]}}
+                "clocks": clock_info, "autotune": tune, "accuracy": accuracy, "plain": plain,
+                "autotuned_window": autotuned, "reference_kernels": ref_k}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
 
 
-def run_serving(args, wl, sptr):
+def run_serving(args, wl, sptr, tune) -> dict:
     """Poisson arrivals of photometric depth-map jobs (random reference view of
-    the scene, the other views as sources) into a continuous-batching pool with
-    every view resident; p50/p99 completion latency and throughput."""
+    the scene, the other views as sources), served (a) by the continuous-
+    batching pool with every view resident and (b) by the plain path, one
+    engine per job in arrival order (FP32 storage, default launch shape).
+    p50/p99 completion latency (completion minus arrival) and throughput of
+    each, on the same arrival times."""
+    import torch
+    from sensemap_b200 import STORE_F32
     from sensemap_b200 import serving as srv
-    from sensemap_b200.patch_match import View
+    from sensemap_b200.patch_match import PatchMatchACMMCuda, Problem, View
     from sensemap_b200.pool import DepthMapPool
     sc = wl.scene
     n_jobs = max(4, int(args.serving_rate * args.serving_seconds))
     arrivals = srv.poisson_arrivals(args.serving_rate, n_jobs, seed=1)
     rng = np.random.default_rng(2)
+    refs = [int(rng.integers(0, wl.V)) for _ in range(n_jobs)]
     specs = []
-    for k in range(n_jobs):
-        r = int(rng.integers(0, wl.V))
+    for k, r in enumerate(refs):
         o = make_options(sc, wl.storage, False)
         o.random_seed = 5000 + k
         specs.append(srv.JobSpec(o, r, [i for i in range(wl.V) if i != r]))
-    pool = DepthMapPool(memory_budget_bytes=32 << 30, max_active_jobs=8, image_storage=wl.storage, stream=sptr)
+    slots = 8
+    pool = DepthMapPool(memory_budget_bytes=32 << 30, max_active_jobs=slots, image_storage=wl.storage, stream=sptr,
+                        sweep_block_x=tune["sweep_block_x"], threads_per_pixel=tune["threads_per_pixel"])
     for i, v in enumerate(sc.views):
         pool.add_view(i, View(wl.dev[i], v.K, v.R, v.T))
     acc = []
@@ -567,10 +772,31 @@ def run_serving(args, wl, sptr):
     st = pool.stats()
     pool.close()
     res.pop("latencies")
-    res.update({"arrival_rate_jobs_s": args.serving_rate, "slots": 8, "job": "photometric pass, 1 ref + 10 src, "
-                f"{wl.scene.views[0].image.shape[1]}x{wl.scene.views[0].image.shape[0]}, {ITERS} iterations",
+    res.update({"arrival_rate_jobs_s": args.serving_rate, "slots": slots,
+                "job": f"photometric pass, 1 ref + {wl.V - 1} src, {sc.views[0].image.shape[1]}x"
+                       f"{sc.views[0].image.shape[0]}, {ITERS} iterations",
                 "within_1pct_gt_first_jobs": float(np.mean(acc)) if acc else None,
                 "graphs_built": st["graphs_built"], "pool_steps": st["steps"]})
+
+    # The plain path under the same arrivals: one job at a time.
+    views = [View(wl.dev[i], v.K, v.R, v.T) for i, v in enumerate(sc.views)]
+    lat = np.zeros(n_jobs)
+    t0 = time.perf_counter()
+    for k, r in enumerate(refs):
+        now = time.perf_counter() - t0
+        if arrivals[k] > now:
+            time.sleep(arrivals[k] - now)
+        o = make_options(sc, STORE_F32, False)
+        o.random_seed = 5000 + k
+        with PatchMatchACMMCuda(o, Problem(r, [i for i in range(wl.V) if i != r], views), stream=sptr) as pm:
+            pm.Run()
+            pm.Synchronize()
+        lat[k] = time.perf_counter() - t0 - arrivals[k]
+    wall = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    res["plain"] = {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                    "mean_s": float(lat.mean()), "throughput_jobs_s": n_jobs / wall,
+                    "form": "one engine per job in arrival order, FP32 storage"}
     return res
 
 

@@ -217,10 +217,14 @@ typedef enum smvs_kernel_kind {
 /* Launch-shape knobs of the checkerboard kernels (results do not depend on
  * them). No counterpart in the reference. */
 typedef struct smvs_tuning {
-  int sweep_block_x; /* threads per block in x: 8, 16, 32 (default) or 64; 256 / x in y */
+  int sweep_block_x; /* pixels per block row: 8, 16, 32 (default) or 64 (each spans two
+                        image columns of the checkerboard); a block is 256 threads */
   int ref_tile_tma;  /* 1 (default): stage the reference tile with a TMA load where the image
                         qualifies (rows a multiple of 16 bytes, image at least one tile);
                         0: plain loads */
+  int threads_per_pixel; /* 1, 2 (default) or 4 threads share one pixel's NCC windows; the
+                            smallest value >= this whose shared memory fits the view count
+                            is used. Maps do not depend on it. */
 } smvs_tuning;
 int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 /* The launch shape in use and whether the last smvs_run staged its reference
@@ -228,8 +232,8 @@ int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 int smvs_get_tuning(const smvs_engine* eng, smvs_tuning* tuning);
 /* Launch-shape autotuner: on a scratch engine for (opt, prob), times one
  * iteration's checkerboard sweep for every launch shape (sweep_block_x 8, 16,
- * 32, 64; reference tiles by TMA where the image qualifies, and by plain
- * loads), best of `repeats` (<= 0: 3), and writes the fastest to `best`. The
+ * 32, 64 x threads_per_pixel 1, 2, 4, reference tiles by TMA where the image
+ * qualifies), best of `repeats` (<= 0: 3), and writes the fastest to `best`. The
  * candidates and their ms per sweep launch go to tried/ms (up to `capacity`),
  * their number to num_tried. Maps do not depend on the choice. */
 int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* stream, int repeats, smvs_tuning* best,
@@ -260,6 +264,7 @@ typedef struct smvs_pool_options {
   int use_graphs;             /* capture each batch's iteration in a CUDA graph */
   int gpu_index;              /* -1 = current device */
   int ref_tile_tma;           /* stage reference tiles with TMA where a view qualifies (smvs_tuning) */
+  int sweep_threads_per_pixel; /* threads per pixel of the checkerboard kernels (smvs_tuning) */
 } smvs_pool_options;
 
 typedef struct smvs_pool_stats {
@@ -307,21 +312,24 @@ void smvs_pool_destroy(smvs_pool* pool);
 /* Largest number of source views smvs_filter_depth_map_noalloc accepts. */
 #define SMVS_NOALLOC_MAX_SRC 32
 /* The geometric-consistency filter of smvs_run_filter, for callers that cannot
- * allocate device memory: processes with a fixed device-memory budget reserved
- * at start-up, code issuing work on a stream that is being captured into a
- * CUDA graph, or hosts whose framework owns every allocation. No counterpart
- * in the reference. It calls no cudaMalloc, cudaFree or other allocating
- * routine: every input and output is a caller-owned device buffer
- * (prob->memory must be SMVS_MEM_DEVICE; prob->ref.depth is the map to filter,
- * each prob->src[i].depth a source view's map, pixels are not read), and the
+ * allocate device memory: a serving process that reserved its whole device
+ * budget at start-up and may not grow it per request, or a host whose
+ * framework owns every device allocation. No counterpart in the reference. It
+ * calls no cudaMalloc, cudaFree or other allocating routine: every input and
+ * output is a caller-owned device buffer (prob->memory must be
+ * SMVS_MEM_DEVICE; prob->ref.depth is the map to filter, each
+ * prob->src[i].depth a source view's map, pixels are not read), and the
  * kernel's scratch — the pose records of at most SMVS_NOALLOC_MAX_SRC source
  * views, 5,504 bytes — lives in a fixed device array that every GPU loading
  * this library holds until the process exits. More source views are rejected
- * with SMVS_EINVAL. The first call on a device looks up that array's address
- * (cudaGetSymbolAddress); make that first call before any stream capture.
- * All calls share the one array and each call overwrites it before its kernel
+ * with SMVS_EINVAL, and the options pass smvs_options_check. The first call on
+ * a device looks up that array's address (cudaGetSymbolAddress); make that
+ * first call before any stream capture. All calls share the one array and each
+ * call overwrites it (with a small kernel on `stream`) before its filter kernel
  * runs, so calls whose work overlaps on the GPU (different streams, or other
- * threads) race; serialise them. Work is enqueued on `stream` (NULL = the
+ * threads) race; serialise them. A CUDA error left pending on the calling
+ * thread by earlier work is returned as SMVS_ECUDA (and thereby cleared)
+ * before anything is enqueued. Work is enqueued on `stream` (NULL = the
  * default stream); `out_depth` is W*H floats. */
 int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs_problem* prob, float* out_depth,
                                   int deduplication, void* stream);

@@ -19,6 +19,11 @@ extern "C" {
  * coordinates xy[2*i], xy[2*i+1]. Host buffers in and out; synchronous. */
 int smvs_test_sample_texture(const float* image, int w, int h, int storage, const float* xy, int n, float* out);
 
+/* Read and clear the CUDA error pending on the calling thread in this
+ * library's runtime (cudaGetLastError); returns its code (0 = none). Lets a
+ * test start from a clean thread state after other tests. */
+int smvs_test_take_cuda_error(void);
+
 /* Throughput calibration on the current device, used as roofline denominators
  * for this path's bounds: kind 0 = FP32 FMA rate (flop/s, FMA = 2 flop),
  * kind 1 = bilinear texture samples/s from an 8-bit texture with warp-coherent

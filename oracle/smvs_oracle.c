@@ -479,12 +479,13 @@ static void init_workspace(ctx_t* c, int random_init, const float* init_depth, c
     }
 }
 
-/* InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior). */
-static void init_conf(ctx_t* c) {
-  const int W = c->W, H = c->H, N = c->N;
-  const size_t WH = (size_t)W * H;
+/* InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior), over rows
+ * [row_begin, row_end). */
+static void init_conf(ctx_t* c, int row_begin, int row_end) {
+  const int W = c->W, N = c->N;
+  const size_t WH = (size_t)W * c->H;
 #pragma omp parallel for schedule(dynamic, 4)
-  for (int row = 0; row < H; ++row) {
+  for (int row = row_begin; row < row_end; ++row) {
     pixref_t pr;
     for (int col = 0; col < W; ++col) {
       const size_t pix = (size_t)row * W + col;
@@ -746,13 +747,18 @@ static void local_opt_pixel(ctx_t* c, int row, int col, uint64_t sk) {
 
 static void half_sweep(ctx_t* c, int colour, int row_begin, int row_end, int local, float th_mc,
                        uint64_t sk) {
-  const int W = c->W;
-#pragma omp parallel for schedule(dynamic, 1)
-  for (int row = row_begin; row < row_end; ++row)
-    for (int col = ((row + colour) & 1); col < W; col += 2) {
-      if (local) local_opt_pixel(c, row, col, sk);
-      else sweep_pixel(c, row, col, th_mc, sk);
-    }
+  /* The pixels of one colour are independent: parallel over pixels (not rows),
+   * so that a band of a few rows still keeps every thread busy. */
+  const int W = c->W, half = (W + 1) / 2;
+  const long n = (long)(row_end - row_begin) * half;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (long i = 0; i < n; ++i) {
+    const int row = row_begin + (int)(i / half);
+    const int col = 2 * (int)(i % half) + ((row + colour) & 1);
+    if (col >= W) continue;
+    if (local) local_opt_pixel(c, row, col, sk);
+    else sweep_pixel(c, row, col, th_mc, sk);
+  }
 }
 
 
@@ -1015,9 +1021,18 @@ int orc_run(const smvs_options* o, const smvs_problem* p, int row_begin, int row
   if (o->has_prior_depth || o->propagate_depth) { ctx_free(&c); return SMVS_EINVAL; }
   if (!o->init_depth_random && (!p->ref.depth || !p->ref.normal)) { ctx_free(&c); return SMVS_EINVAL; }
   init_workspace(&c, o->init_depth_random, p->ref.depth, p->ref.normal, (float)o->depth_min, (float)o->depth_max);
-  init_conf(&c);
   int rb = 0, re = c.H;
   if (row_end > row_begin) { rb = row_begin < 0 ? 0 : row_begin; re = row_end > c.H ? c.H : row_end; }
+  {
+    /* A band run scores the initial hypotheses of the band and of the rows
+     * its sweeps read (neighbour samples reach 21 rows, kernel_functions.cu:
+     * 27-44); other rows keep conf 0 and are never read. */
+    const int margin = 24;
+    const int cb = (rb == 0 && re == c.H) ? 0 : (rb - margin < 0 ? 0 : rb - margin);
+    const int ce = (rb == 0 && re == c.H) ? c.H : (re + margin > c.H ? c.H : re + margin);
+    if (cb > 0 || ce < c.H) memset(c.conf, 0, sizeof(float) * (size_t)c.W * c.H);
+    init_conf(&c, cb, ce);
+  }
   for (int iter = 0; iter < c.num_iter; ++iter) {
     const float th_mc = c.init_mc * expf(-(float)(iter * iter) / c.alpha); /* :778-779 */
     half_sweep(&c, 0, rb, re, 0, th_mc, stage_key(c.seed, stage_sweep(iter, 0)));

@@ -13,7 +13,7 @@
  *     Steele, Lea & Flood, OOPSLA 2014) keyed on (seed, stage, pixel, draw);
  *   - the Marsaglia normal sampler gives up after 32 rejected trials.
  * Parity against the reference's own kernels is checked by running them (built
- * from the reference sources into oracle/_ref by oracle/ref_build.sh) on the
+ * from the reference sources into oracle/_ref by oracle/ref_build.py) on the
  * same inputs: cost-level parity deterministically, full runs statistically.
  */
 #ifndef SMVS_ORACLE_H_

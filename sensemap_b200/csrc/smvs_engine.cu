@@ -159,6 +159,8 @@ struct smvs_engine {
   int* d_status = nullptr;        // bounded waits of the kernels that gave up
   bool use_tma = true;
   bool tma_active = false;        // the last run staged reference tiles with TMA
+  int tpp_used = 0;               // threads per pixel of the last run
+  int tma_polls = 0;              // TMA tile wait bound (0 = default; a test hook shortens it)
   float* d_ggrad = nullptr;     // W*H (median_filter)
   bool has_init = false;
   bool has_src_depth = false;
@@ -255,6 +257,13 @@ int smvs_internal_prepare_job(smvs::JobParams* p, const smvs_options* o) {
     p->th_tab[it] = (float)o->init_ncc_matching_cost * expf(-(float)(it * it) / (float)o->alpha);
   p->blocks_x = (p->W + 2 * p->block_x - 1) / (2 * p->block_x);
   p->conf_blocks_x = (p->W + 31) / 32;
+  // Threads per pixel: the requested value, raised until the block's cost
+  // matrices fit in shared memory (maps do not depend on it).
+  const int tpp = smvs::FitThreadsPerPixel(p->R, smvs::ViewBucket(p->N), p->block_x, p->tpp > 0 ? p->tpp : 2);
+  if (!tpp)
+    return Fail(SMVS_EINVAL, "no launch shape with sweep_block_x=%d fits %d source views in shared memory",
+                p->block_x, p->N);
+  p->tpp = tpp;
   return SMVS_OK;
 }
 
@@ -372,6 +381,10 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
     if (err != cudaSuccess) { delete e; return Fail(SMVS_ECUDA, "cudaSetDevice(%d): %s", opt->gpu_index, cudaGetErrorString(err)); }
   }
   cudaGetDevice(&e->device);
+  {
+    const cudaError_t err = smvs::ConfigureKernels();
+    if (err != cudaSuccess) { delete e; return Fail(SMVS_ECUDA, "kernel set-up: %s", cudaGetErrorString(err)); }
+  }
   if (stream) {
     e->stream = (cudaStream_t)stream;
   } else {
@@ -403,6 +416,7 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   p.geom = opt->geom_consistency;
   p.thk = opt->thk < N ? opt->thk : N;  // patch_match_cuda.cu:949-950
   p.block_x = 32;
+  p.tpp = 2;
   p.geom_reg = (float)opt->geom_consistency_regularizer;
   p.geom_max = (float)opt->geom_consistency_max_cost;
   const float* K = prob->ref.K;
@@ -518,12 +532,12 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
 static int UploadRefMap(smvs_engine* e, smvs::JobParams* p) {
   p->tma_box_w = p->tma_box_h = 0;
   CUtensorMap map;
-  if (!e->use_tma || !smvs::EncodeRefMap(&map, p->ref, p->W, p->H, p->block_x, p->R)) return SMVS_OK;
+  if (!e->use_tma || !smvs::EncodeRefMap(&map, p->ref, p->W, p->H, p->block_x, p->tpp, p->R)) return SMVS_OK;
   // The host descriptor dies at return: copy it before returning.
   SMVS_CUDA(cudaMemcpyAsync(e->d_tmap, &map, sizeof(map), cudaMemcpyHostToDevice, e->stream));
   SMVS_CUDA(cudaStreamSynchronize(e->stream));
   p->tma_box_w = smvs::RefTileW(p->block_x, p->R);
-  p->tma_box_h = smvs::RefTileH(p->block_x, p->R);
+  p->tma_box_h = smvs::RefTileH(p->block_x, p->tpp, p->R);
   return SMVS_OK;
 }
 
@@ -555,12 +569,13 @@ int smvs_run(smvs_engine* e) {
   if ((st = smvs_internal_prepare_job(&p, &o))) return st;
   if ((st = UploadRefMap(e, &p))) return st;
   e->tma_active = p.tma_box_w > 0;
+  e->tpp_used = p.tpp;
   {
     // The checkerboard kernels run as a batch of one job.
     char host[sizeof(smvs::JobParams) + 8 * sizeof(int)];
     int* ints = reinterpret_cast<int*>(host + sizeof(smvs::JobParams));
     memcpy(host, &p, sizeof(p));
-    const int by = 256 / p.block_x;
+    const int by = smvs::SweepRows(p.block_x, p.tpp);
     const int nb = p.blocks_x * ((e->H + by - 1) / by);
     const int ncb = p.conf_blocks_x * ((e->H + 7) / 8);
     ints[0] = 0;             // iteration counter
@@ -577,9 +592,11 @@ int smvs_run(smvs_engine* e) {
     b.total_blocks = nb;
     b.total_conf_blocks = ncb;
     b.block_x = p.block_x;
+    b.tpp = p.tpp;
     b.R = p.R; b.S = p.S; b.NB = smvs::ViewBucket(p.N);
     b.ref_maps = e->d_tmap;
     b.status = e->d_status;
+    b.tma_polls = e->tma_polls;
   }
   if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(b, e->stream); }))) return st;
   int* iters = const_cast<int*>(b.iters);
@@ -694,7 +711,11 @@ int smvs_set_tuning(smvs_engine* e, const smvs_tuning* t) {
   if (!e || !t) return Fail(SMVS_EINVAL, "null argument");
   const int bx = t->sweep_block_x;
   if (bx != 8 && bx != 16 && bx != 32 && bx != 64) return Fail(SMVS_EINVAL, "sweep_block_x must be 8, 16, 32 or 64");
+  const int tpp = t->threads_per_pixel;
+  if (tpp != 1 && tpp != 2 && tpp != 4) return Fail(SMVS_EINVAL, "threads_per_pixel must be 1, 2 or 4");
+  if (!smvs::ValidSweepShape(bx, tpp)) return Fail(SMVS_EINVAL, "sweep_block_x * threads_per_pixel must be <= 256");
   e->jp.block_x = bx;
+  e->jp.tpp = tpp;
   e->use_tma = t->ref_tile_tma != 0;
   return SMVS_OK;
 }
@@ -703,6 +724,7 @@ int smvs_get_tuning(const smvs_engine* e, smvs_tuning* t) {
   if (!e || !t) return Fail(SMVS_EINVAL, "null argument");
   t->sweep_block_x = e->jp.block_x;
   t->ref_tile_tma = e->tma_active ? 1 : 0;
+  t->threads_per_pixel = e->tpp_used > 0 ? e->tpp_used : e->jp.tpp;
   return SMVS_OK;
 }
 
@@ -744,11 +766,14 @@ int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* strea
   int st = smvs_create(&o, prob, stream, &e);
   if (st) return st;
   const int xs[4] = {8, 16, 32, 64};
+  const int ts[3] = {1, 2, 4};
   double best_ms = 0;
   int n = 0;
+  std::vector<smvs_tuning> seen;
   for (int k = 0; k < 4 && st == SMVS_OK; ++k)
-    for (int tma = 1; tma >= 0 && st == SMVS_OK; --tma) {
-      smvs_tuning t{xs[k], tma};
+    for (int j = 0; j < 3 && st == SMVS_OK; ++j) {
+      if (!smvs::ValidSweepShape(xs[k], ts[j])) continue;
+      smvs_tuning t{xs[k], 1, ts[j]};
       if ((st = smvs_set_tuning(e, &t))) break;
       double t_best = 0;
       for (int r = 0; r < (repeats > 0 ? repeats : 3) && st == SMVS_OK; ++r) {
@@ -764,7 +789,11 @@ int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* strea
       if (st) break;
       smvs_tuning used;
       smvs_get_tuning(e, &used);
-      if (tma && !used.ref_tile_tma) continue;  // the image does not qualify: same as the plain candidate
+      bool dup = false;  // threads_per_pixel raised to fit: the same shape as an earlier candidate
+      for (const auto& u : seen)
+        dup = dup || (u.sweep_block_x == used.sweep_block_x && u.threads_per_pixel == used.threads_per_pixel);
+      if (dup) continue;
+      seen.push_back(used);
       if (tried && ms && n < capacity) {
         tried[n] = used;
         ms[n] = t_best;

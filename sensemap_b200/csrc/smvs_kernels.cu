@@ -1,6 +1,8 @@
 // smvs_kernels.cu — per-pixel kernels (image conversion, reference moments,
 // initialisation, mask, geometric-consistency filter) and the dispatch over
 // the window-templated PatchMatch kernels of smvs_sweep.cuh.
+#include <mutex>
+
 #include <cuda_fp16.h>
 
 #include "smvs_device.cuh"
@@ -11,6 +13,8 @@ namespace smvs {
 namespace detail {
 template <int R, int S>
 cudaError_t LaunchWindow(const Batch& b, int op, int colour, cudaStream_t stream);
+template <int R, int S>
+cudaError_t ConfigureWindow();
 }
 
 namespace {
@@ -364,7 +368,35 @@ cudaError_t LaunchAdvance(int* iters, int num_jobs, cudaStream_t stream) {
   return cudaGetLastError();
 }
 
-int ViewBucket(int N) { return N <= 8 ? 8 : (N <= 16 ? 16 : SMVS_MAX_SRC); }
+int ViewBucket(int N) { return (N + 3) & ~3; }
+
+int FitThreadsPerPixel(int R, int nb, int bx, int tpp) {
+  for (int t = tpp; t <= 4; t *= 2)
+    if (ValidSweepShape(bx, t) && SweepKernelSmem(R, nb, bx, t) <= kMaxDynamicSmem &&
+        LocalKernelSmem(R, nb, bx, t) <= kMaxDynamicSmem)
+      return t;
+  return 0;
+}
+
+cudaError_t ConfigureKernels() {
+  static std::mutex mu;
+  static bool done[64] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(mu);
+  if (done[dev]) return cudaSuccess;
+  if (e == cudaSuccess) e = detail::ConfigureWindow<5, 1>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<3, 1>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<7, 1>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<3, 2>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<4, 2>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<5, 2>();
+  if (e == cudaSuccess) e = detail::ConfigureWindow<7, 2>();
+  if (e == cudaSuccess) done[dev] = true;
+  return e;
+}
 
 cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream) {
   dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);

@@ -27,7 +27,8 @@ struct alignas(16) JobParams {
   float refK[4], refiK[4];
   uint64_t stage_key;               // per-launch RNG stage key of the per-pixel kernels
   uint64_t seed;                    // job seed (batched kernels derive stage keys from it)
-  int block_x;                      // checkerboard kernels: threads per block in x (256 / block_x in y)
+  int block_x;                      // checkerboard kernels: pixels per block row (each spans 2 image columns)
+  int tpp;                          // checkerboard kernels: threads per pixel (1, 2 or 4)
   int num_iterations;
   int local_opt;
   int blocks_x;                     // batched launches: this job's checkerboard blocks per row
@@ -61,26 +62,58 @@ struct Batch {
   int num_jobs;
   int total_blocks;             // checkerboard tiling
   int total_conf_blocks;        // full tiling
-  int block_x;                  // shared launch shape of the batch
-  int R, S, NB;                 // shared window and view bucket of the batch
+  int block_x;                  // shared launch shape of the batch: pixels per block row
+  int tpp;                      // and threads per pixel (a block is 256 threads, 256 / tpp pixels)
+  int R, S, NB;                 // shared window; NB = views per pixel in shared memory (>= every job's N)
   const CUtensorMap* ref_maps;  // per job: reference image for TMA tile loads (jobs with tma_box_w > 0)
   int* status;                  // set to 1 when a bounded wait of a kernel gave up
+  int tma_polls;                // mbarrier polls before a TMA tile wait gives up (0 = the default bound)
 };
 
-// Reference tile of the checkerboard kernels (block bx x 256/bx threads, two
-// columns per thread): rows [row0 - R, row0 + by + R), columns starting at
-// col0 - R - RefTileShift(R), so that the first column is a multiple of 4
-// floats (col0 is a multiple of 2 bx >= 16): a TMA box may only start on a
-// 16-byte boundary. The tile's row stride is RefTileW.
+// Checkerboard blocks: 256 threads, tpp threads per pixel, bx pixels per
+// block row (two image columns each) and SweepRows(bx, tpp) pixel rows.
+__host__ __device__ inline int SweepRows(int bx, int tpp) { return 256 / (tpp * bx); }
+// Reference tile of a checkerboard block: rows [row0 - R, row0 + rows + R),
+// columns starting at col0 - R - RefTileShift(R), so that the first column is
+// a multiple of 4 floats (col0 is a multiple of 2 bx >= 16): a TMA box may only
+// start on a 16-byte boundary. The tile's row stride is RefTileW.
 __host__ __device__ inline int RefTileShift(int R) { return (4 - (R & 3)) & 3; }
 __host__ __device__ inline int RefTileW(int bx, int R) { return (2 * bx + 2 * R + RefTileShift(R) + 3) & ~3; }
-__host__ __device__ inline int RefTileH(int bx, int R) { return 256 / bx + 2 * R; }
+__host__ __device__ inline int RefTileH(int bx, int tpp, int R) { return SweepRows(bx, tpp) + 2 * R; }
+// Hypotheses per pixel of the sweep (K_NUM_SAMPS + 3, kernel_functions.h:32).
+constexpr int kSweepHyp = 11;
+// Largest dynamic shared memory a checkerboard block may request (the B200's
+// 227 KB per block minus room for the kernels' static shared memory).
+constexpr size_t kMaxDynamicSmem = 227 * 1024 - 2048;
+// Dynamic shared memory of a sweep block: the reference tile (+128 bytes of
+// alignment slack for the TMA destination), nb pose records, and per pixel the
+// cost matrix, hypotheses, view weights and view probabilities.
+__host__ __device__ inline size_t SweepKernelSmem(int R, int nb, int bx, int tpp) {
+  const size_t P = 256 / tpp;
+  const size_t tile = (size_t)RefTileW(bx, R) * RefTileH(bx, tpp, R);
+  return 128 + sizeof(float) * (tile + (size_t)nb * SMVS_POSE_FLOATS + P * (kSweepHyp * nb + kSweepHyp * 4 + 2 * nb));
+}
+// Same for a local-optimisation block (per pixel: five hypotheses' costs).
+__host__ __device__ inline size_t LocalKernelSmem(int R, int nb, int bx, int tpp) {
+  const size_t P = 256 / tpp;
+  const size_t tile = (size_t)RefTileW(bx, R) * RefTileH(bx, tpp, R);
+  return 128 + sizeof(float) * (tile + (size_t)nb * SMVS_POSE_FLOATS + P * (5 * nb));
+}
+// Same for an InitConf block (32 x 8 pixels, one thread each: the cost vector
+// and its sort order per pixel).
+__host__ __device__ inline size_t InitConfKernelSmem(int R, int nb) {
+  return sizeof(float) * ((size_t)(32 + 2 * R) * (8 + 2 * R) + (size_t)nb * SMVS_POSE_FLOATS + 2 * (size_t)nb * 256);
+}
+// Whether (bx, tpp) is a valid checkerboard launch shape.
+inline bool ValidSweepShape(int bx, int tpp) {
+  return (bx == 8 || bx == 16 || bx == 32 || bx == 64) && (tpp == 1 || tpp == 2 || tpp == 4) && bx * tpp <= 256;
+}
 
 // Encodes the TMA descriptor of a dense W x H FP32 reference image for the
 // checkerboard tile of launch shape bx and window R. Returns false (use plain
 // loads) when the image rows are not a multiple of 16 bytes, the image is
 // smaller than the box, or the driver does not provide the encoder.
-bool EncodeRefMap(CUtensorMap* map, const float* ref, int W, int H, int bx, int R);
+bool EncodeRefMap(CUtensorMap* map, const float* ref, int W, int H, int bx, int tpp, int R);
 
 // All launchers enqueue on `stream` and return the launch status.
 cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, int w, int h, void* out,
@@ -93,8 +126,16 @@ cudaError_t LaunchSweep(const Batch& b, int colour, cudaStream_t stream);
 cudaError_t LaunchLocalOpt(const Batch& b, int colour, cudaStream_t stream);
 // iters[j] += 1 for every job of the batch (after both colours of an iteration).
 cudaError_t LaunchAdvance(int* iters, int num_jobs, cudaStream_t stream);
-// View bucket (max views of the M matrix) for N source views.
+// Views per pixel the checkerboard kernels reserve in shared memory for N
+// source views (N rounded up to a multiple of 4); batches group jobs by it.
 int ViewBucket(int N);
+// The smallest tpp >= `tpp` whose sweep block fits in shared memory for nb
+// views (results do not depend on it); 0 if none does.
+int FitThreadsPerPixel(int R, int nb, int bx, int tpp);
+// Opt every checkerboard kernel into large dynamic shared memory on the
+// current device. Called once per device by the engine and the pool before
+// any launch (and before any stream capture).
+cudaError_t ConfigureKernels();
 cudaError_t LaunchMask(const JobParams& p, const uint8_t* mask, cudaStream_t stream);
 cudaError_t LaunchCurvature(const JobParams& p, uint16_t* curv, cudaStream_t stream);
 cudaError_t LaunchGeomGradient(const JobParams& p, float* ggrad, cudaStream_t stream);

@@ -1,19 +1,21 @@
 // smvs_noalloc.cu — geometric-consistency filter that allocates nothing.
 //
-// For callers that cannot call cudaMalloc: code that runs with a fixed,
-// pre-reserved device-memory budget (a serving process that reserved all of
-// its memory at start-up), code that runs on a stream being captured into a
-// CUDA graph (where allocating would break the capture), or host code called
-// back from a framework that owns all device allocations. The caller passes
-// device buffers for every input and output; the kernel's scratch (the pose
-// records of the source views) lives in a file-scope __device__ array that
-// every GPU loading this library holds until the process exits.
+// For callers that cannot call cudaMalloc: a serving process that reserved its
+// whole device-memory budget at start-up and may not grow it per request, or
+// host code called back from a framework that owns every device allocation
+// and forbids allocating behind its back. The caller passes device buffers for
+// every input and output; the kernel's scratch (the pose records of the source
+// views) lives in a file-scope __device__ array that every GPU loading this
+// library holds until the process exits. The records reach that array through
+// a one-block kernel that takes them as a by-value kernel parameter, so no host
+// buffer has to outlive the call.
 //
 // Same arithmetic as smvs_run_filter (FilterDepthMapsKernel,
 // kernel_functions.cu:3356-3487), except that source depth maps are read from
 // the caller's dense buffers with the bilinear weights the texture unit uses
 // (8-bit positions, integer 1/256 weights with w11 = round(A*B/256)) instead
 // of through texture objects, which this entry point may not create.
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -24,10 +26,22 @@
 
 extern "C" void smvs_internal_set_error(const char* msg);
 
+// Scratch: one 43-float pose record per source view (5,504 bytes). Every call
+// overwrites the records it uses before its filter kernel reads them.
+static __device__ __align__(256) float g_filter_scratch[SMVS_NOALLOC_MAX_SRC * SMVS_POSE_FLOATS];
+
 namespace {
 
-// Scratch: one 43-float pose record per source view (5,504 bytes).
-__device__ __align__(256) float g_filter_scratch[SMVS_NOALLOC_MAX_SRC * SMVS_POSE_FLOATS];
+// The pose records of one call, passed by value to the kernel that stores them
+// in the scratch array (5,504 bytes, within the 32 KB kernel-parameter limit
+// of CUDA 12.1+ on sm_70 and later).
+struct PoseRecords {
+  float v[SMVS_NOALLOC_MAX_SRC * SMVS_POSE_FLOATS];
+};
+
+__global__ void StorePoseRecordsKernel(const PoseRecords rec, int count, float* __restrict__ scratch) {
+  for (int i = threadIdx.x; i < count; i += blockDim.x) scratch[i] = rec.v[i];
+}
 
 struct NoAllocParams {
   int W, H, N;
@@ -121,6 +135,10 @@ void smvs_internal_pose_record(const smvs_view* ref, const smvs_view* src, float
 extern "C" int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs_problem* prob, float* out_depth,
                                              int deduplication, void* stream) {
   if (!opt || !prob || !out_depth) return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: null argument");
+  // The options pass the same check as smvs_create's (which smvs_run_filter
+  // goes through), so both entry points reject the same option sets.
+  const int ost = smvs_options_check(opt);
+  if (ost != SMVS_OK) return ost;
   if (prob->memory != SMVS_MEM_DEVICE)
     return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: depth maps must be device buffers (SMVS_MEM_DEVICE)");
   if (prob->num_src < 1 || prob->num_src > SMVS_NOALLOC_MAX_SRC)
@@ -129,9 +147,13 @@ extern "C" int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs
     return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: the reference view needs width, height and depth");
   if (prob->ref.K[0] == 0.f || prob->ref.K[4] == 0.f)
     return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: zero focal length");
-  for (int i = 0; i < prob->num_src; ++i)
+  if (!prob->src) return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: null source view list");
+  for (int i = 0; i < prob->num_src; ++i) {
     if (!prob->src[i].depth || prob->src[i].width <= 0 || prob->src[i].height <= 0)
       return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: every source view needs width, height and depth");
+    if (prob->src[i].K[0] == 0.f || prob->src[i].K[4] == 0.f)
+      return Fail(SMVS_EINVAL, "smvs_filter_depth_map_noalloc: zero focal length in a source view");
+  }
 
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64)
@@ -165,19 +187,30 @@ extern "C" int smvs_filter_depth_map_noalloc(const smvs_options* opt, const smvs
   p.dedup = deduplication ? 1 : 0;
   p.ref_depth = prob->ref.depth;
   p.out_depth = out_depth;
-  float poses[SMVS_NOALLOC_MAX_SRC * SMVS_POSE_FLOATS];
+  PoseRecords rec;
+  memset(&rec, 0, sizeof(rec));
   for (int i = 0; i < p.N; ++i) {
     p.src_depth[i] = prob->src[i].depth;
     p.src_w[i] = prob->src[i].width;
     p.src_h[i] = prob->src[i].height;
-    smvs_internal_pose_record(&prob->ref, &prob->src[i], poses + i * SMVS_POSE_FLOATS);
+    smvs_internal_pose_record(&prob->ref, &prob->src[i], rec.v + i * SMVS_POSE_FLOATS);
+  }
+  // An error left pending on this thread by earlier CUDA work would otherwise
+  // surface as this call's launch error; report it (this reads and clears it)
+  // and enqueue nothing.
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    char msg[256];
+    snprintf(msg, sizeof(msg),
+             "smvs_filter_depth_map_noalloc: a CUDA error from earlier work was pending on this thread (%s); "
+             "nothing was enqueued",
+             cudaGetErrorName(e));
+    return Fail(SMVS_ECUDA, msg);
   }
   cudaStream_t s = (cudaStream_t)stream;
-  // The records of this call replace the previous call's; pageable source
-  // memory makes the copy complete before this function returns.
-  cudaError_t e = cudaMemcpyAsync(scratch, poses, sizeof(float) * SMVS_POSE_FLOATS * p.N, cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return Fail(SMVS_ECUDA, cudaGetErrorString(e));
-  (void)cudaGetLastError();
+  // The records of this call replace the previous call's (stream-ordered
+  // before the filter kernel that reads them).
+  StorePoseRecordsKernel<<<1, 256, 0, s>>>(rec, p.N * SMVS_POSE_FLOATS, scratch);
   dim3 block(32, 8), grid((p.W + 31) / 32, (p.H + 7) / 8);
   FilterDepthMapsNoAllocKernel<<<grid, block, 0, s>>>(p, scratch);
   e = cudaGetLastError();

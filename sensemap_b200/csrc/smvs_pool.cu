@@ -304,6 +304,7 @@ int smvs_pool_options_default(smvs_pool_options* o) {
   o->use_graphs = 1;
   o->ref_tile_tma = 1;
   o->gpu_index = -1;
+  o->sweep_threads_per_pixel = 2;
   return SMVS_OK;
 }
 
@@ -314,9 +315,16 @@ int smvs_pool_create(const smvs_pool_options* o, void* stream, smvs_pool** out) 
   if (o->image_storage < SMVS_STORE_U8 || o->image_storage > SMVS_STORE_F32) return Fail(SMVS_EINVAL, "bad image_storage");
   const int bx = o->sweep_block_x;
   if (bx != 8 && bx != 16 && bx != 32 && bx != 64) return Fail(SMVS_EINVAL, "sweep_block_x must be 8, 16, 32 or 64");
+  const int tpp = o->sweep_threads_per_pixel;
+  if (tpp != 1 && tpp != 2 && tpp != 4) return Fail(SMVS_EINVAL, "sweep_threads_per_pixel must be 1, 2 or 4");
+  if (!smvs::ValidSweepShape(bx, tpp)) return Fail(SMVS_EINVAL, "sweep_block_x * sweep_threads_per_pixel must be <= 256");
   if (o->gpu_index >= 0) {
     cudaError_t e = cudaSetDevice(o->gpu_index);
     if (e != cudaSuccess) return Fail(SMVS_ECUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  }
+  {
+    const cudaError_t e = smvs::ConfigureKernels();
+    if (e != cudaSuccess) return Fail(SMVS_ECUDA, "kernel set-up: %s", cudaGetErrorString(e));
   }
   auto* P = new smvs_pool();
   P->opt = *o;
@@ -512,13 +520,8 @@ int Admit(smvs_pool* P, PoolJob& J) {
   p.refiK[2] = 1.0f / p.refK[2];
   p.refiK[3] = -p.refK[3] / p.refK[2];
   p.block_x = P->opt.sweep_block_x;
+  p.tpp = P->opt.sweep_threads_per_pixel;
   p.ref = rv.ref;
-  p.tma_box_w = p.tma_box_h = 0;
-  memset(&J.map, 0, sizeof(J.map));
-  if (P->opt.ref_tile_tma && smvs::EncodeRefMap(&J.map, p.ref, W, H, p.block_x, p.R)) {
-    p.tma_box_w = smvs::RefTileW(p.block_x, p.R);
-    p.tma_box_h = smvs::RefTileH(p.block_x, p.R);
-  }
   for (int i = 0; i < N; ++i) {
     PoolView& sv = P->views[J.srcs[i]];
     p.src_tex[i] = sv.tex;
@@ -526,7 +529,16 @@ int Admit(smvs_pool* P, PoolJob& J) {
     sv.last_use = ++P->clock;
   }
   rv.last_use = ++P->clock;
-  smvs_internal_prepare_job(&p, &o);
+  {
+    const int pst = smvs_internal_prepare_job(&p, &o);  // fits threads per pixel to N
+    if (pst) return pst;
+  }
+  p.tma_box_w = p.tma_box_h = 0;
+  memset(&J.map, 0, sizeof(J.map));
+  if (P->opt.ref_tile_tma && smvs::EncodeRefMap(&J.map, p.ref, W, H, p.block_x, p.tpp, p.R)) {
+    p.tma_box_w = smvs::RefTileW(p.block_x, p.R);
+    p.tma_box_h = smvs::RefTileH(p.block_x, p.tpp, p.R);
+  }
   J.block_bytes = JobBytes(W, H, N);
   J.block = P->arena.Reuse(J.block_bytes);  // cached blocks are already counted in bytes_used
   if (!J.block) {
@@ -564,10 +576,10 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
   if (ids.empty()) return SMVS_OK;
   // The staging buffers may still feed the previous upload.
   POOL_CUDA(cudaStreamSynchronize(P->stream));
-  std::map<std::tuple<int, int, int, int>, std::vector<int64_t>> by_key;
+  std::map<std::tuple<int, int, int, int, int>, std::vector<int64_t>> by_key;
   for (int64_t id : ids) {
     const smvs::JobParams& p = P->jobs[id].p;
-    by_key[std::make_tuple(p.R, p.S, smvs::ViewBucket(p.N), p.block_x)].push_back(id);
+    by_key[std::make_tuple(p.R, p.S, smvs::ViewBucket(p.N), p.block_x, p.tpp)].push_back(id);
   }
   int base = 0;
   const int cap = P->capacity;
@@ -585,7 +597,9 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
     b.S = std::get<1>(kv.first);
     b.NB = std::get<2>(kv.first);
     b.block_x = std::get<3>(kv.first);
-    const int by = 256 / b.block_x;
+    b.tpp = std::get<4>(kv.first);
+    b.tma_polls = 0;
+    const int by = smvs::SweepRows(b.block_x, b.tpp);
     int tot = 0, ctot = 0;
     for (int k = 0; k < n; ++k) {
       PoolJob& J = P->jobs[list[k]];

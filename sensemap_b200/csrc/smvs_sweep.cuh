@@ -1,10 +1,19 @@
 // smvs_sweep.cuh — window-templated PatchMatch kernels (internal).
 //
-// Thread-per-pixel checkerboard kernels. Per block: the reference-image tile
-// the window needs and the N pose records are staged in shared memory once;
+// Checkerboard kernels with G threads per pixel (G = 1, 2 or 4, a launch-shape
+// knob). Per block (256 threads, 256 / G pixels): the reference-image tile the
+// window needs and the N pose records are staged in shared memory once;
 // source views are fetched through per-view texture objects over pitched HBM
 // (hardware bilinear, border = 0, the sampling the reference configures at
-// patch_match_cuda.cu:258-278). RNG draws come from a counter-based generator,
+// patch_match_cuda.cu:258-278). A pixel's cost matrix (hypotheses x views),
+// its hypothesis list and its view weights live in shared memory, not in
+// per-thread local memory. The G lanes of a pixel split the window rows of
+// every NCC evaluation and add their partial moments with warp shuffles; all
+// other per-pixel work is done identically by the G lanes (same inputs, same
+// RNG draws), and lane 0 writes shared and global memory. The moments are
+// always summed in one canonical order (rows by index mod 4 into four partial
+// sums, combined as (p0 + p1) + (p2 + p3)), whatever G is, so maps do not
+// depend on the launch shape. RNG draws come from a counter-based generator,
 // so there is no per-pixel state array. Each supported (radius, step) pair is
 // instantiated in its own translation unit (smvs_win_<R>_<S>.cu).
 #pragma once
@@ -16,17 +25,7 @@ namespace smvs {
 namespace detail {
 namespace {  // internal linkage: every window translation unit gets its own copy
 
-constexpr int kThreads = 256;  // threads per block; the block's x/y split is a tuning knob (JobParams)
-// Resident blocks per SM the register allocation of the sweep kernels must
-// allow; 0 leaves the register budget to the compiler.
-#ifndef SMVS_SWEEP_MIN_BLOCKS
-#define SMVS_SWEEP_MIN_BLOCKS 0
-#endif
-#if SMVS_SWEEP_MIN_BLOCKS > 0
-#define SMVS_SWEEP_BOUNDS __launch_bounds__(kThreads, SMVS_SWEEP_MIN_BLOCKS)
-#else
-#define SMVS_SWEEP_BOUNDS __launch_bounds__(kThreads)
-#endif
+constexpr int kThreads = 256;  // threads per checkerboard block
 
 __constant__ float kMWeights[5] = {0.f, 1.f, 2.01f, 3.03f, 4.06f};  // kernel_functions.cu:22
 __constant__ int kNeighborOffs[4][2] = {{0, -1}, {-1, 0}, {0, 1}, {1, 0}};  // :23-25 (first four)
@@ -78,8 +77,8 @@ __device__ __forceinline__ bool MbarPoll(uint32_t bar, uint32_t parity) {
   return done != 0;
 }
 
-__device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity) {
-  for (uint32_t i = 0; i < kTmaWaitPolls; ++i) {
+__device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity, uint32_t polls) {
+  for (uint32_t i = 0; i < polls; ++i) {
     if (MbarPoll(bar, parity)) return true;
     if (i >= 32) __nanosleep(64);
   }
@@ -90,10 +89,10 @@ __device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity) {
 // `map` at column x (a multiple of 4) and row y into `tile` (128-byte aligned
 // shared memory); rows and columns outside the image read as zero (the
 // border of the reference's texture). Every thread waits on the mbarrier with
-// a bounded wait. Returns false after setting *status if the copy did not
-// land; the caller then leaves the block's pixels unchanged.
+// a bounded wait (`polls`). Returns false after setting *status if the copy
+// did not land; the caller then leaves the block's pixels unchanged.
 __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile, int x, int y, uint32_t bytes,
-                                             uint64_t* mbar, int* status) {
+                                             uint64_t* mbar, int* status, uint32_t polls) {
   const uint32_t bar = SmemAddr(mbar);
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
   if (leader) {
@@ -109,10 +108,10 @@ __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile
         ::"r"(SmemAddr(tile)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
         : "memory");
   }
-  const bool landed = MbarWait(bar, 0);
+  const bool landed = MbarWait(bar, 0, polls);
   if (!__syncthreads_or(!landed)) return true;  // block-uniform outcome
   if (leader) atomicExch(status, 1);
-  MbarWait(bar, 0);  // let a late copy land before the block's shared memory is released
+  MbarWait(bar, 0, kTmaWaitPolls);  // let a late copy land before the block's shared memory is released
   return false;
 }
 
@@ -121,9 +120,9 @@ __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile
 // RefTileW floats starting at (row0 - R, col0 - R - RefTileShift(R)).
 template <int R>
 __device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobParams& p, float* tile, int row0,
-                                             int col0, float* poses, uint64_t* mbar) {
-  const int bx = blockDim.x;
-  const int tw = RefTileW(bx, R), th = RefTileH(bx, R);
+                                             int col0, int rows, float* poses, uint64_t* mbar) {
+  const int bx = b.block_x;
+  const int tw = RefTileW(bx, R), th = rows + 2 * R;
   const int x0 = col0 - R - RefTileShift(R), y0 = row0 - R;
   const bool tma = b.ref_maps != nullptr && p.tma_box_w == tw && p.tma_box_h == th;
   if (!tma) {
@@ -132,7 +131,8 @@ __device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobP
   }
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += blockDim.x * blockDim.y) poses[i] = __ldg(p.poses + i);
-  return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, b.status);
+  return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, b.status,
+                      b.tma_polls > 0 ? (uint32_t)b.tma_polls : kTmaWaitPolls);
 }
 
 // Batched launches: find this block's job (binary search over the block
@@ -164,13 +164,42 @@ __device__ __forceinline__ void DecodeBlock(const Batch& b, const int* prefix, J
   __syncthreads();
 }
 
-// ComputeNCCCost<R,S>, kernel_functions.cu:1245-1340. `win` points at the
-// window's top-left in the shared tile (row stride ws).
-template <int R, int S>
+// The lanes of this thread's pixel: G consecutive lanes of the warp.
+template <int G>
+__device__ __forceinline__ unsigned GroupMask() {
+  const unsigned lane = threadIdx.x & 31u;
+  return (G == 1) ? (1u << lane) : (((1u << G) - 1u) << (lane & ~(unsigned)(G - 1)));
+}
+
+// Sum of the four row-class partials a[k] (k = the lane's k-th class) over the
+// pixel's lanes, always as (p0 + p1) + (p2 + p3), where p_c is the sum over the
+// window rows i with i mod 4 == c. Lane l of G owns classes l, l + G, ...
+template <int G>
+__device__ __forceinline__ float CombineClasses(const float* a, unsigned gmask) {
+  if (G == 1) return (a[0] + a[1]) + (a[2] + a[3]);
+  if (G == 2) {
+    const float s01 = a[0] + __shfl_xor_sync(gmask, a[0], 1);
+    const float s23 = a[1] + __shfl_xor_sync(gmask, a[1], 1);
+    return s01 + s23;
+  }
+  const float s = a[0] + __shfl_xor_sync(gmask, a[0], 1);
+  return s + __shfl_xor_sync(gmask, s, 2);
+}
+
+// ComputeNCCCost<R,S>, kernel_functions.cu:1245-1340, with the window rows
+// split over the G lanes of the pixel (lane `lane` takes rows lane, lane + G,
+// ...). `win` points at the window's top-left in the shared tile (row stride
+// ws). The source positions follow the reference's incremental scheme exactly
+// (row starts advanced by one row step at a time, taps by one column step);
+// every lane returns the same value.
+template <int R, int S, int G>
 __device__ __forceinline__ float NccCost(cudaTextureObject_t tex, const float* pose, int row, int col, float depth,
                                          const float n[3], const float iK[4], int W, int H, float center,
-                                         float rsum, float rvar, const float* win, int ws, float sn, float cn) {
+                                         float rsum, float rvar, const float* win, int ws, float sn, float cn,
+                                         int lane, unsigned gmask) {
   constexpr float kMaxCost = 2.0f;
+  constexpr int kRows = 2 * R / S + 1;
+  constexpr int kClasses = 4 / G;  // row classes (mod 4) per lane
   float Hm[9];
   ComposeHomography(pose, row, col, depth, n, iK, Hm);
   const float inv_z0 = 1.0f / (Hm[6] * col + Hm[7] * row + Hm[8]);
@@ -179,44 +208,58 @@ __device__ __forceinline__ float NccCost(cudaTextureObject_t tex, const float* p
   // [quirk] bounds are the reference image's width/height (:1265-1270).
   if (u < 0 || u >= W || v < 0 || v >= H) return kMaxCost;
   const int row_start = row - R, col_start = col - R;
-  float col_src = Hm[0] * col_start + Hm[1] * row_start + Hm[2];
-  float row_src = Hm[3] * col_start + Hm[4] * row_start + Hm[5];
-  float z = Hm[6] * col_start + Hm[7] * row_start + Hm[8];
-  float bcol = col_src, brow = row_src, bz = z;
+  float bcol = Hm[0] * col_start + Hm[1] * row_start + Hm[2];
+  float brow = Hm[3] * col_start + Hm[4] * row_start + Hm[5];
+  float bz = Hm[6] * col_start + Hm[7] * row_start + Hm[8];
   const float h0 = S * Hm[0], h1 = S * Hm[1], h3 = S * Hm[3], h4 = S * Hm[4], h6 = S * Hm[6], h7 = S * Hm[7];
-  float ss = 0.f, sss = 0.f, srs = 0.f, sw = 0.f;
-  // Window rows stay rolled and the taps of a row are unrolled: one copy of
-  // the tap code per call site keeps the kernel inside the instruction cache.
-#pragma unroll 1
-  for (int dr = -R; dr <= R; dr += S) {
-    const float* wrow = win + (dr + R) * ws + R;
-    const float sr = (float)(dr * dr);
+  for (int k = 0; k < lane; ++k) { bcol += h1; brow += h4; bz += h7; }  // this lane's first row
+  float ss[kClasses], sss[kClasses], srs[kClasses], sw[kClasses];
 #pragma unroll
-    for (int dc = -R; dc <= R; dc += S) {
-      const float iz = 1.0f / z;
-      const float fu = iz * col_src + 0.5f;
-      const float fv = iz * row_src + 0.5f;
-      const float rc = wrow[dc];
-      const float sc = tex2D<float>(tex, fu, fv);
-      const float cd = center - rc;
-      const float wgt = __expf(-(sr + (float)(dc * dc)) * sn - cd * cd * cn);
-      const float wsc = wgt * sc;
-      ss += wsc;
-      sss += wsc * sc;
-      srs += wsc * rc;
-      sw += wgt;
-      col_src += h0;
-      row_src += h3;
-      z += h6;
+  for (int k = 0; k < kClasses; ++k) { ss[k] = 0.f; sss[k] = 0.f; srs[k] = 0.f; sw[k] = 0.f; }
+  // Rows in groups of four; within a group this lane takes rows q + lane + k G.
+  // Taps of a row are unrolled; the groups stay rolled (instruction cache).
+#pragma unroll 1
+  for (int q = 0; q < kRows; q += 4) {
+#pragma unroll
+    for (int k = 0; k < kClasses; ++k) {
+      const int i = q + lane + k * G;
+      if (i < kRows) {
+        const int dr = -R + i * S;
+        const float* wrow = win + (dr + R) * ws + R;
+        const float sr = (float)(dr * dr);
+        float col_src = bcol, row_src = brow, z = bz;
+#pragma unroll
+        for (int dc = -R; dc <= R; dc += S) {
+          const float iz = 1.0f / z;
+          const float fu = iz * col_src + 0.5f;
+          const float fv = iz * row_src + 0.5f;
+          const float rc = wrow[dc];
+          const float sc = tex2D<float>(tex, fu, fv);
+          const float cd = center - rc;
+          const float wgt = __expf(-(sr + (float)(dc * dc)) * sn - cd * cd * cn);
+          const float wsc = wgt * sc;
+          ss[k] += wsc;
+          sss[k] += wsc * sc;
+          srs[k] += wsc * rc;
+          sw[k] += wgt;
+          col_src += h0;
+          row_src += h3;
+          z += h6;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < G; ++t) { bcol += h1; brow += h4; bz += h7; }
     }
-    bcol += h1; brow += h4; bz += h7;
-    col_src = bcol; row_src = brow; z = bz;
   }
-  const float isw = 1.0f / sw;
-  ss *= isw; sss *= isw; srs *= isw;
-  const float svar = sss - ss * ss;
+  float tss = CombineClasses<G>(ss, gmask);
+  float tsss = CombineClasses<G>(sss, gmask);
+  float tsrs = CombineClasses<G>(srs, gmask);
+  const float tsw = CombineClasses<G>(sw, gmask);
+  const float isw = 1.0f / tsw;
+  tss *= isw; tsss *= isw; tsrs *= isw;
+  const float svar = tsss - tss * tss;
   if (rvar < 1e-5f || svar < 1e-5f) return kMaxCost;
-  const float cov = srs - rsum * ss;
+  const float cov = tsrs - rsum * tss;
   const float val = 1.0f - cov * rsqrtf(rvar * svar);
   return fmaxf(0.0f, fminf(kMaxCost, val));
 }
@@ -227,19 +270,21 @@ struct PixRef {
   int ws;
 };
 
-template <int R, int S>
+template <int R, int S, int G>
 __device__ __forceinline__ float ViewCost(const JobParams& p, const float* poses, int v, int row, int col,
                                           float depth, const float n[3], const float np[3], const PixRef& pr,
-                                          const float* Kgeom) {
+                                          const float* Kgeom, int lane, unsigned gmask) {
   const float* pose = poses + v * SMVS_POSE_FLOATS;
-  float cost = NccCost<R, S>(p.src_tex[v], pose, row, col, depth, n, p.refiK, p.W, p.H, pr.center, pr.rsum,
-                             pr.rvar, pr.win, pr.ws, p.sn, p.cn);
+  float cost = NccCost<R, S, G>(p.src_tex[v], pose, row, col, depth, n, p.refiK, p.W, p.H, pr.center, pr.rsum,
+                                pr.rvar, pr.win, pr.ws, p.sn, p.cn, lane, gmask);
   if (p.geom)
     cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, Kgeom, p.geom_max);
   return cost;
 }
 
-// InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior).
+// InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior). One thread per
+// pixel; the cost vector and its sort order live in shared memory
+// ([view][pixel], nb views per pixel).
 template <int R, int S>
 __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   extern __shared__ float smem[];
@@ -249,13 +294,17 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   const JobParams& p = sp;
   const int kBX = blockDim.x, kBY = blockDim.y;
   const int tw = kBX + 2 * R, th = kBY + 2 * R;
+  const int nb = b.NB;
   float* tile = smem;
   float* poses = smem + tw * th;
+  float* costs = poses + nb * SMVS_POSE_FLOATS;
+  int* order = reinterpret_cast<int*>(costs + nb * kThreads);
   const int col0 = (blk % p.conf_blocks_x) * kBX, row0 = (blk / p.conf_blocks_x) * kBY;
   StageShared(p, tile, row0 - R, col0 - R, th, tw, poses);
   __syncthreads();
   const int col = col0 + threadIdx.x, row = row0 + threadIdx.y;
   if (col >= p.W || row >= p.H) return;
+  const int t = threadIdx.y * kBX + threadIdx.x;
   const size_t WH = (size_t)p.W * p.H;
   const size_t pix = (size_t)row * p.W + col;
   PixRef pr;
@@ -267,34 +316,54 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   const float np[3] = {p.refiK[0] * col + p.refiK[1], p.refiK[2] * row + p.refiK[3], 1.0f};
   const float n[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
   const float depth = p.depth[pix];
-  float costs[SMVS_MAX_SRC];
-  int order[SMVS_MAX_SRC];
+  const unsigned gmask = GroupMask<1>();
+#define C_(v) costs[(v) * kThreads + t]
+#define O_(v) order[(v) * kThreads + t]
   for (int v = 0; v < p.N; ++v) {
-    costs[v] = ViewCost<R, S>(p, poses, v, row, col, depth, n, np, pr, p.refK);
-    order[v] = v;
-    p.cost[(size_t)v * WH + pix] = costs[v];
+    const float c = ViewCost<R, S, 1>(p, poses, v, row, col, depth, n, np, pr, p.refK, 0, gmask);
+    C_(v) = c;
+    O_(v) = v;
+    p.cost[(size_t)v * WH + pix] = c;
   }
   // Partial bubble sort: only the best thk positions are needed and the
   // reference's full ascending bubble sort (utils.h:212-231) puts the same
   // (stable) values there.
   for (int i = 0; i < p.N - 1; ++i)
     for (int j = 0; j < p.N - 1 - i; ++j)
-      if (costs[j] > costs[j + 1]) {
-        const float t = costs[j]; costs[j] = costs[j + 1]; costs[j + 1] = t;
-        const int o = order[j]; order[j] = order[j + 1]; order[j + 1] = o;
+      if (C_(j) > C_(j + 1)) {
+        const float tc = C_(j); C_(j) = C_(j + 1); C_(j + 1) = tc;
+        const int to = O_(j); O_(j) = O_(j + 1); O_(j + 1) = to;
       }
   float conf = 0.f;
   uint32_t sel = p.view_sel[pix];
-  for (int i = 0; i < p.thk; ++i) { conf += costs[i]; sel |= (1u << order[i]); }
+  for (int i = 0; i < p.thk; ++i) { conf += C_(i); sel |= (1u << O_(i)); }
+#undef C_
+#undef O_
   conf /= kMWeights[p.thk];
   p.conf[pix] = conf;
   p.view_sel[pix] = sel;
 }
 
+// Shared-memory layout of a checkerboard block after the reference tile and
+// the pose records (floats, P pixels, nb views per pixel, pixel index fastest).
+struct SweepSmem {
+  float* M;   // [kMaxHyp][nb][P]  cost of hypothesis h on view v
+  float* HY;  // [kMaxHyp][4][P]   hypotheses (normal xyz, depth)
+  float* VW;  // [nb][P]           view weights
+  float* PR;  // [nb][P]           view probabilities, then their CDF
+};
+
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
-// propagate_depth): one checkerboard colour, one thread per pixel.
-template <int R, int S, int NB>
-__global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
+// propagate_depth): one checkerboard colour, G threads per pixel.
+// Blocks per SM the register allocation must allow: shared memory holds one
+// block per SM at G = 1 (10 views), two at G = 2 and three at G = 4.
+template <int G>
+struct SweepOccupancy {
+  static constexpr int kBlocks = G == 4 ? 3 : 2;
+};
+
+template <int R, int S, int G>
+__global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) SweepKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
@@ -304,16 +373,29 @@ __global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
   if (iter >= p.num_iterations) return;  // finished job of the batch (block-uniform)
   const float th_mc = p.th_tab[iter];
   const uint64_t skey = StageKey(p.seed, StageSweep(iter, colour));
-  const int kBX = blockDim.x, kBY = blockDim.y;
-  const int tw = RefTileW(kBX, R), th = RefTileH(kBX, R);
+  constexpr int P = kThreads / G;
+  const int bx = b.block_x, rows = P / bx, nb = b.NB;
+  const int tw = RefTileW(bx, R), th = rows + 2 * R;
   float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
   float* poses = tile + tw * th;
-  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, poses, &mbar)) return;  // block-uniform
+  SweepSmem sm;
+  sm.M = poses + nb * SMVS_POSE_FLOATS;
+  sm.HY = sm.M + kMaxHyp * nb * P;
+  sm.VW = sm.HY + kMaxHyp * 4 * P;
+  sm.PR = sm.VW + nb * P;
+  const int col0 = (blk % p.blocks_x) * 2 * bx, row0 = (blk / p.blocks_x) * rows;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar)) return;  // block-uniform
   __syncthreads();
-  const int row = row0 + threadIdx.y;
-  const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
-  if (col >= p.W || row >= p.H) return;
+  const int g = threadIdx.x / G, lane = threadIdx.x % G;
+  const int row = row0 + g / bx;
+  const int col = col0 + 2 * (g % bx) + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;  // uniform over the pixel's lanes
+  const unsigned gmask = GroupMask<G>();
+  const bool leader = lane == 0;
+#define M_(h, v) sm.M[((h) * nb + (v)) * P + g]
+#define HY_(h, c) sm.HY[((h) * 4 + (c)) * P + g]
+#define VW_(v) sm.VW[(v) * P + g]
+#define PR_(v) sm.PR[(v) * P + g]
   const int W = p.W, H = p.H, N = p.N;
   const size_t WH = (size_t)W * H;
   const size_t pix = (size_t)row * W + col;
@@ -329,10 +411,9 @@ __global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
   const float vd[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
   const float ivl = rsqrtf(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
 
-  float hyp[kMaxHyp][4];
-  int ns = 0;
-  hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
-  ns = 1;
+  // Hypothesis list (identical in every lane; lane 0 stores it).
+  int ns = 1;
+  if (leader) { HY_(0, 0) = normal[0]; HY_(0, 1) = normal[1]; HY_(0, 2) = normal[2]; HY_(0, 3) = depth; }
   if (grad >= 1.0f) {  // :2237-2276
     float nconf[4], O[4];
     int nvalid = 0;
@@ -359,8 +440,8 @@ __global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
       const size_t q = (size_t)v * W + u;
       float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
       CorrectNormal(nn, vd, ivl);
-      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, v, u, vd);
-      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      const float pd = PropagateDepth(p.depth[q], nn, iK, v, u, vd);
+      if (leader) { HY_(ns, 0) = nn[0]; HY_(ns, 1) = nn[1]; HY_(ns, 2) = nn[2]; HY_(ns, 3) = pd; }
       ns++;
     }
   }
@@ -378,87 +459,104 @@ __global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
       const size_t q = (size_t)br * W + bc;
       float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
       CorrectNormal(nn, vd, ivl);
-      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, br, bc, vd);
-      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      const float pd = PropagateDepth(p.depth[q], nn, iK, br, bc, vd);
+      if (leader) { HY_(ns, 0) = nn[0]; HY_(ns, 1) = nn[1]; HY_(ns, 2) = nn[2]; HY_(ns, 3) = pd; }
       ns++;
     }
   }
+  for (int v = lane; v < N; v += G) M_(0, v) = p.cost[(size_t)v * WH + pix];
+  __syncwarp(gmask);
 
   PixRef pr;
   pr.center = p.ref[pix];
   pr.rsum = p.ref_sum[pix];
   pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
   pr.ws = tw;
-  pr.win = tile + threadIdx.y * tw + (col - col0) + RefTileShift(R);
-  float M[kMaxHyp][NB];
-  for (int v = 0; v < N; ++v) M[0][v] = p.cost[(size_t)v * WH + pix];
-  float vw[NB];
-  float costs[kMaxHyp];
+  pr.win = tile + (g / bx) * tw + (col - col0) + RefTileShift(R);
   // Two evaluation phases share one call site of the cost code: phase 0 scores
   // the propagated hypotheses 1..ns-1, phase 1 the refinement hypotheses 1..4.
   int h_end = ns;
   for (int phase = 0; phase < 2; ++phase) {
-    for (int h = 1; h < h_end; ++h)
-      for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr, p.refK);
+    for (int h = 1; h < h_end; ++h) {
+      const float hn[3] = {HY_(h, 0), HY_(h, 1), HY_(h, 2)};
+      const float hd = HY_(h, 3);
+      for (int v = 0; v < N; ++v) {
+        const float c = ViewCost<R, S, G>(p, poses, v, row, col, hd, hn, vd, pr, p.refK, lane, gmask);
+        if (leader) M_(h, v) = c;
+      }
+    }
+    __syncwarp(gmask);
     if (phase == 1) break;
 
-    // ACMM view selection, :2364-2427.
+    // ACMM view selection, :2364-2427. Per view: its probability (PR), or 0
+    // when the view is not good.
     uint32_t flags = 0;
-    float probs[NB];
     for (int v = 0; v < N; ++v) {
       unsigned n1 = 0, n2 = 0;
       float pv = 0.f;
       for (int h = 0; h < ns; ++h) {
-        const float cst = M[h][v];
+        const float cst = M_(h, v);
         pv += __expf(-cst * cst * p.inv_beta2);
         n1 += (cst < th_mc);
         n2 += (cst > p.max_mc);
       }
-      probs[v] = pv;
       if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
+      else pv = 0.f;
+      if (leader) PR_(v) = pv;
     }
     if (flags == 0) return;
-    for (int v = 0; v < N; ++v)
-      if (!((flags >> v) & 1u)) probs[v] = 0.f;
-    {
+    __syncwarp(gmask);
+    {  // the CDF, into VW
       float sum = 0.f;
-      for (int v = 0; v < N; ++v) sum += probs[v];
+      for (int v = 0; v < N; ++v) sum += PR_(v);
       const float inv = 1.0f / sum;
       float cum = 0.f;
-      for (int v = 0; v < N; ++v) { cum += probs[v] * inv; probs[v] = cum; }
+      for (int v = 0; v < N; ++v) {
+        cum += PR_(v) * inv;
+        if (leader) VW_(v) = cum;
+      }
     }
-    for (int v = 0; v < N; ++v) vw[v] = 0.f;
+    __syncwarp(gmask);
+    // num_samples uniforms draw views: a set of views (random_opt) or a count
+    // per view (in PR, written by lane 0 only).
+    uint32_t drawn = 0;
+    if (leader && !p.random_opt)
+      for (int v = 0; v < N; ++v) PR_(v) = 0.f;
     for (int s = 0; s < p.num_samples; ++s) {
       const float rp = r.Uniform() - FLT_EPSILON;
       for (int v = 0; v < N; ++v)
-        if (probs[v] > rp) {
-          if (p.random_opt) vw[v] = 1.0f; else vw[v] += 1.0f;
+        if (VW_(v) > rp) {
+          drawn |= (1u << v);
+          if (leader && !p.random_opt) PR_(v) += 1.0f;
           break;
         }
     }
+    __syncwarp(gmask);
     float wn = 0.f;
-    for (int v = 0; v < N; ++v) wn += vw[v];
+    for (int v = 0; v < N; ++v) wn += p.random_opt ? (float)((drawn >> v) & 1u) : PR_(v);
     if (wn <= 1e-5f) return;
     const float iwn = 1.0f / wn;
+    if (leader)
+      for (int v = 0; v < N; ++v) VW_(v) = (p.random_opt ? (float)((drawn >> v) & 1u) : PR_(v)) * iwn;
+    __syncwarp(gmask);
     uint32_t sel = 0;
-    for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
-    for (int h = 0; h < ns; ++h) {
-      float cs = 0.f;
-      for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
-      costs[h] = cs;
-    }
-    p.view_sel[pix] = sel;
+    for (int v = 0; v < N; ++v) if (VW_(v) > 0) sel |= (1u << v);
+    if (leader) p.view_sel[pix] = sel;
     int mi = -1;
     {
       float m = FLT_MAX;
-      for (int h = 0; h < ns; ++h)
-        if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
+      for (int h = 0; h < ns; ++h) {
+        float cs = 0.f;
+        for (int v = 0; v < N; ++v) cs += VW_(v) * M_(h, v);
+        if (cs <= m) { m = cs; mi = h; }  // FindMinCost :648-659 ('<=')
+      }
     }
     if (mi < 0) return;
-    depth = hyp[mi][3];
-    normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
+    depth = HY_(mi, 3);
+    normal[0] = HY_(mi, 0); normal[1] = HY_(mi, 1); normal[2] = HY_(mi, 2);
+    __syncwarp(gmask);
     if (mi != 0)
-      for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
+      for (int v = lane; v < N; v += G) M_(0, v) = M_(mi, v);
 
     // Refinement hypotheses, :2449-2486.
     float nn[3];
@@ -470,36 +568,42 @@ __global__ void SMVS_SWEEP_BOUNDS SweepKernel(const Batch b, int colour) {
     float rn[3];
     RandomNormal(r, vd, rn);
     CorrectNormal(rn, vd, ivl);
-    hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
-    hyp[1][0] = nn[0]; hyp[1][1] = nn[1]; hyp[1][2] = nn[2]; hyp[1][3] = depth;
-    hyp[2][0] = normal[0]; hyp[2][1] = normal[1]; hyp[2][2] = normal[2]; hyp[2][3] = ndepth;
-    hyp[3][0] = rn[0]; hyp[3][1] = rn[1]; hyp[3][2] = rn[2]; hyp[3][3] = depth;
-    hyp[4][0] = normal[0]; hyp[4][1] = normal[1]; hyp[4][2] = normal[2]; hyp[4][3] = rdepth;
+    if (leader) {
+      HY_(0, 0) = normal[0]; HY_(0, 1) = normal[1]; HY_(0, 2) = normal[2]; HY_(0, 3) = depth;
+      HY_(1, 0) = nn[0]; HY_(1, 1) = nn[1]; HY_(1, 2) = nn[2]; HY_(1, 3) = depth;
+      HY_(2, 0) = normal[0]; HY_(2, 1) = normal[1]; HY_(2, 2) = normal[2]; HY_(2, 3) = ndepth;
+      HY_(3, 0) = rn[0]; HY_(3, 1) = rn[1]; HY_(3, 2) = rn[2]; HY_(3, 3) = depth;
+      HY_(4, 0) = normal[0]; HY_(4, 1) = normal[1]; HY_(4, 2) = normal[2]; HY_(4, 3) = rdepth;
+    }
+    __syncwarp(gmask);
     h_end = 5;
   }
   // :2488-2559: weighted refinement costs, argmin, write back.
+  int mi = -1;
+  float m = FLT_MAX;
   for (int h = 0; h < 5; ++h) {
     float cs = 0.f;
-    for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
-    costs[h] = cs;
-  }
-  int mi = -1;
-  {
-    float m = FLT_MAX;
-    for (int h = 0; h < 5; ++h)
-      if (costs[h] <= m) { m = costs[h]; mi = h; }
+    for (int v = 0; v < N; ++v) cs += VW_(v) * M_(h, v);
+    if (cs <= m) { m = cs; mi = h; }
   }
   if (mi != -1) {
-    p.conf[pix] = costs[mi];
-    p.depth[pix] = hyp[mi][3];
-    p.normal[pix] = hyp[mi][0]; p.normal[WH + pix] = hyp[mi][1]; p.normal[2 * WH + pix] = hyp[mi][2];
-    for (int v = 0; v < N; ++v) p.cost[(size_t)v * WH + pix] = M[mi][v];
+    if (leader) {
+      p.conf[pix] = m;
+      p.depth[pix] = HY_(mi, 3);
+      p.normal[pix] = HY_(mi, 0); p.normal[WH + pix] = HY_(mi, 1); p.normal[2 * WH + pix] = HY_(mi, 2);
+    }
+    for (int v = lane; v < N; v += G) p.cost[(size_t)v * WH + pix] = M_(mi, v);
   }
+#undef M_
+#undef HY_
+#undef VW_
+#undef PR_
 }
 
-// LocalOptimization, kernel_functions.cu:2736-2931.
-template <int R, int S, int NB>
-__global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
+// LocalOptimization, kernel_functions.cu:2736-2931, G threads per pixel; the
+// five hypotheses and their costs live in shared memory.
+template <int R, int S, int G>
+__global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) LocalOptKernel(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
@@ -509,16 +613,22 @@ __global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
   // Iterations > 2 only (patch_match_cuda.cu:861-880); block-uniform.
   if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
   const uint64_t skey = StageKey(p.seed, StageLocal(iter, colour));
-  const int kBX = blockDim.x, kBY = blockDim.y;
-  const int tw = RefTileW(kBX, R), th = RefTileH(kBX, R);
+  constexpr int P = kThreads / G;
+  const int bx = b.block_x, rows = P / bx, nb = b.NB;
+  const int tw = RefTileW(bx, R), th = rows + 2 * R;
   float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
   float* poses = tile + tw * th;
-  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, poses, &mbar)) return;  // block-uniform
+  float* Ms = poses + nb * SMVS_POSE_FLOATS;  // [5][nb][P]
+  const int col0 = (blk % p.blocks_x) * 2 * bx, row0 = (blk / p.blocks_x) * rows;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar)) return;  // block-uniform
   __syncthreads();
-  const int row = row0 + threadIdx.y;
-  const int col = col0 + 2 * threadIdx.x + ((row + colour) & 1);
+  const int g = threadIdx.x / G, lane = threadIdx.x % G;
+  const int row = row0 + g / bx;
+  const int col = col0 + 2 * (g % bx) + ((row + colour) & 1);
   if (col >= p.W || row >= p.H) return;
+  const unsigned gmask = GroupMask<G>();
+  const bool leader = lane == 0;
+#define M_(h, v) Ms[((h) * nb + (v)) * P + g]
   const int W = p.W, H = p.H, N = p.N;
   const size_t WH = (size_t)W * H;
   const size_t pix = (size_t)row * W + col;
@@ -549,18 +659,15 @@ __global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
   pr.rsum = p.ref_sum[pix];
   pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
   pr.ws = tw;
-  pr.win = tile + threadIdx.y * tw + (col - col0) + RefTileShift(R);
-  float M[5][NB];
-  float hyp[5][4];
+  pr.win = tile + (g / bx) * tw + (col - col0) + RefTileShift(R);
   int mi = -1;
   // Rounds 0..4 score five random hypotheses on the selected views; round 5
   // rescores the winner on the unselected views. One call site of the cost code.
   for (int it = 0; it < 6; ++it) {
     float hcur[4];
     if (it < 5) {
-      hyp[it][3] = r.Uniform() * (hi - lo) + lo;
-      PerturbNormalACMH(m, hyp[it], a1, a2, r);
-      hcur[0] = hyp[it][0]; hcur[1] = hyp[it][1]; hcur[2] = hyp[it][2]; hcur[3] = hyp[it][3];
+      hcur[3] = r.Uniform() * (hi - lo) + lo;
+      PerturbNormalACMH(m, hcur, a1, a2, r);
     } else {
       if (mi == -1) break;
       hcur[0] = normal[0]; hcur[1] = normal[1]; hcur[2] = normal[2]; hcur[3] = depth;
@@ -572,12 +679,12 @@ __global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
     for (int v = 0; v < N; ++v) {
       const bool selected = (sel >> v) & 1u;
       if (selected != (it < 5)) continue;
-      const float cost = ViewCost<R, S>(p, poses, v, row, col, hcur[3], hcur, np, pr, Kg);
+      const float cost = ViewCost<R, S, G>(p, poses, v, row, col, hcur[3], hcur, np, pr, Kg, lane, gmask);
       if (it < 5) {
-        M[it][v] = cost;
+        if (leader) M_(it, v) = cost;
         mconf += cost;
         mw += 1.f;
-      } else {
+      } else if (leader) {
         p.cost[(size_t)v * WH + pix] = cost;
       }
     }
@@ -586,53 +693,55 @@ __global__ void SMVS_SWEEP_BOUNDS LocalOptKernel(const Batch b, int colour) {
     mconf /= mw;
     if (mconf < conf) {
       conf = mconf;
-      depth = hyp[it][3];
-      normal[0] = hyp[it][0]; normal[1] = hyp[it][1]; normal[2] = hyp[it][2];
+      depth = hcur[3];
+      normal[0] = hcur[0]; normal[1] = hcur[1]; normal[2] = hcur[2];
       mi = it;
     }
   }
+  __syncwarp(gmask);
   if (mi != -1) {
-    p.conf[pix] = conf;
-    p.depth[pix] = depth;
-    p.normal[pix] = normal[0]; p.normal[WH + pix] = normal[1]; p.normal[2 * WH + pix] = normal[2];
-    for (int v = 0; v < N; ++v)
-      if ((sel >> v) & 1u) p.cost[(size_t)v * WH + pix] = M[mi][v];
+    if (leader) {
+      p.conf[pix] = conf;
+      p.depth[pix] = depth;
+      p.normal[pix] = normal[0]; p.normal[WH + pix] = normal[1]; p.normal[2 * WH + pix] = normal[2];
+    }
+    for (int v = lane; v < N; v += G)
+      if ((sel >> v) & 1u) p.cost[(size_t)v * WH + pix] = M_(mi, v);
   }
+#undef M_
 }
 
-template <int R, int S>
-size_t SweepSmem(int NB, int bx, int by) {
-  (void)by;
-  return 128 + sizeof(float) * (RefTileW(bx, R) * RefTileH(bx, R) + NB * SMVS_POSE_FLOATS);  // + alignment slack
-}
+static_assert(kSweepHyp == kMaxHyp, "hypotheses per pixel");
 
-template <int R, int S, int NB>
+template <int R, int S, int G>
 cudaError_t LaunchSweepT(const Batch& b, int colour, bool local, cudaStream_t stream) {
-  const int bx = b.block_x, by = kThreads / b.block_x;
-  const size_t smem = SweepSmem<R, S>(NB, bx, by);
   if (b.total_blocks <= 0) return cudaSuccess;
   if (local)
-    LocalOptKernel<R, S, NB><<<b.total_blocks, dim3(bx, by), smem, stream>>>(b, colour);
+    LocalOptKernel<R, S, G><<<b.total_blocks, kThreads, LocalKernelSmem(R, b.NB, b.block_x, G), stream>>>(b, colour);
   else
-    SweepKernel<R, S, NB><<<b.total_blocks, dim3(bx, by), smem, stream>>>(b, colour);
+    SweepKernel<R, S, G><<<b.total_blocks, kThreads, SweepKernelSmem(R, b.NB, b.block_x, G), stream>>>(b, colour);
   return cudaGetLastError();
 }
 
 template <int R, int S>
-cudaError_t LaunchSweepNB(const Batch& b, int colour, bool local, cudaStream_t stream) {
-  if (b.NB == 8) return LaunchSweepT<R, S, 8>(b, colour, local, stream);
-  if (b.NB == 16) return LaunchSweepT<R, S, 16>(b, colour, local, stream);
-  if (b.NB == SMVS_MAX_SRC) return LaunchSweepT<R, S, SMVS_MAX_SRC>(b, colour, local, stream);
+cudaError_t LaunchSweepG(const Batch& b, int colour, bool local, cudaStream_t stream) {
+  if (b.tpp == 1) return LaunchSweepT<R, S, 1>(b, colour, local, stream);
+  if (b.tpp == 2) return LaunchSweepT<R, S, 2>(b, colour, local, stream);
+  if (b.tpp == 4) return LaunchSweepT<R, S, 4>(b, colour, local, stream);
   return cudaErrorInvalidValue;
 }
 
 template <int R, int S>
 cudaError_t LaunchInitConfT(const Batch& b, cudaStream_t stream) {
-  const int bx = 32, by = kThreads / 32;
-  const size_t smem = sizeof(float) * ((bx + 2 * R) * (by + 2 * R) + b.NB * SMVS_POSE_FLOATS);
   if (b.total_conf_blocks <= 0) return cudaSuccess;
-  InitConfKernel<R, S><<<b.total_conf_blocks, dim3(bx, by), smem, stream>>>(b);
+  InitConfKernel<R, S><<<b.total_conf_blocks, dim3(32, kThreads / 32), InitConfKernelSmem(R, b.NB), stream>>>(b);
   return cudaGetLastError();
+}
+
+// Let kernel k request up to kMaxDynamicSmem bytes of dynamic shared memory.
+template <typename Kernel>
+cudaError_t AllowLargeSmem(Kernel k) {
+  return cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kMaxDynamicSmem);
 }
 
 }  // namespace
@@ -641,7 +750,21 @@ cudaError_t LaunchInitConfT(const Batch& b, cudaStream_t stream) {
 template <int R, int S>
 cudaError_t LaunchWindow(const Batch& b, int op, int colour, cudaStream_t stream) {
   if (op == 0) return LaunchInitConfT<R, S>(b, stream);
-  return LaunchSweepNB<R, S>(b, colour, op == 2, stream);
+  return LaunchSweepG<R, S>(b, colour, op == 2, stream);
+}
+
+// Opt this window's kernels into large dynamic shared memory (current device).
+template <int R, int S>
+cudaError_t ConfigureWindow() {
+  cudaError_t e = cudaSuccess;
+  if (e == cudaSuccess) e = AllowLargeSmem(InitConfKernel<R, S>);
+  if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 1>);
+  if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 2>);
+  if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 4>);
+  if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 1>);
+  if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 2>);
+  if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 4>);
+  return e;
 }
 
 }  // namespace detail

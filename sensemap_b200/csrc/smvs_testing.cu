@@ -130,6 +130,8 @@ __global__ void TexKernel(cudaTextureObject_t tex, int iters, float* out) {
 
 }  // namespace
 
+extern "C" int smvs_test_take_cuda_error(void) { return (int)cudaGetLastError(); }
+
 extern "C" int smvs_test_calibrate(int kind, double seconds, double* rate) {
   if (!rate || (kind != 0 && kind != 1)) {
     smvs_internal_set_error("smvs_test_calibrate: bad arguments");

@@ -31,9 +31,9 @@ PFN_cuTensorMapEncodeTiled_v12000 Encoder() {
 
 }  // namespace
 
-bool EncodeRefMap(CUtensorMap* map, const float* ref, int W, int H, int bx, int R) {
-  if (!map || !ref || bx <= 0 || 256 % bx) return false;
-  const int box_w = RefTileW(bx, R), box_h = RefTileH(bx, R);
+bool EncodeRefMap(CUtensorMap* map, const float* ref, int W, int H, int bx, int tpp, int R) {
+  if (!map || !ref || !ValidSweepShape(bx, tpp)) return false;
+  const int box_w = RefTileW(bx, R), box_h = RefTileH(bx, tpp, R);
   // Row pitch and base must be multiples of 16 bytes; the box must fit the
   // descriptor's limits (<= 256 per dimension, inner extent a multiple of 16
   // bytes) and the image.

@@ -4,5 +4,6 @@
 namespace smvs {
 namespace detail {
 template cudaError_t LaunchWindow<7, 1>(const Batch& b, int op, int colour, cudaStream_t stream);
+template cudaError_t ConfigureWindow<7, 1>();
 }  // namespace detail
 }  // namespace smvs

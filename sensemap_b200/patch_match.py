@@ -285,15 +285,17 @@ class PatchMatchACMMCuda:
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_launch_count(self._h))
 
-    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True) -> None:
-        t = N.smvs_tuning(sweep_block_x=sweep_block_x, ref_tile_tma=int(ref_tile_tma))
+    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 2) -> None:
+        t = N.smvs_tuning(sweep_block_x=sweep_block_x, ref_tile_tma=int(ref_tile_tma),
+                          threads_per_pixel=int(threads_per_pixel))
         N.check(N.lib().smvs_set_tuning(self._h, C.byref(t)))
 
     def Tuning(self) -> dict:
         """Launch shape in use and whether the last Run staged reference tiles with TMA."""
         t = N.smvs_tuning()
         N.check(N.lib().smvs_get_tuning(self._h, C.byref(t)))
-        return {"sweep_block_x": t.sweep_block_x, "ref_tile_tma": bool(t.ref_tile_tma)}
+        return {"sweep_block_x": t.sweep_block_x, "ref_tile_tma": bool(t.ref_tile_tma),
+                "threads_per_pixel": t.threads_per_pixel}
 
     def SetProfiling(self, enable: bool = True) -> None:
         N.check(N.lib().smvs_set_profiling(self._h, int(enable)))
@@ -331,12 +333,15 @@ def autotune(options: PatchMatchOptions, problem: Problem, stream=None, repeats:
     this problem, with every candidate's ms per sweep launch."""
     prob, keep = _problem_struct(problem)
     best = N.smvs_tuning()
-    tried = (N.smvs_tuning * 16)()
-    ms = (C.c_double * 16)()
+    cap = 32
+    tried = (N.smvs_tuning * cap)()
+    ms = (C.c_double * cap)()
     n = C.c_int()
     stream_ptr = C.c_void_p(int(stream)) if stream is not None else None
     N.check(N.lib().smvs_autotune(C.byref(options.to_c()), C.byref(prob), stream_ptr, int(repeats), C.byref(best),
-                                  tried, ms, 16, C.byref(n)))
+                                  tried, ms, cap, C.byref(n)))
     return {"sweep_block_x": best.sweep_block_x, "ref_tile_tma": bool(best.ref_tile_tma),
+            "threads_per_pixel": best.threads_per_pixel,
             "candidates": [{"sweep_block_x": tried[i].sweep_block_x, "ref_tile_tma": bool(tried[i].ref_tile_tma),
-                            "ms_per_sweep": ms[i]} for i in range(min(n.value, 16))]}
+                            "threads_per_pixel": tried[i].threads_per_pixel, "ms_per_sweep": ms[i]}
+                           for i in range(min(n.value, cap))]}

@@ -1,14 +1,18 @@
 """The no-allocation geometric-consistency filter (smvs_filter_depth_map_noalloc).
 
-It exists for callers that cannot allocate device memory — a process working
-inside a device-memory budget it reserved at start-up, or work issued on a
-stream that is being captured into a CUDA graph — so it takes every input and
-output as a caller-owned device buffer and keeps its scratch in a fixed device
-array. This checks it through the C ABI against the allocating entry point
-(smvs_run_filter) on the same inputs, for two calls in a row (the second call
-reuses the scratch the first one left behind), and that it rejects more source
-views than its scratch holds. Collected last so a failure here cannot stop the
-other tests from running.
+Some callers of this library cannot allocate device memory: a serving process
+that reserved its whole device budget at start-up and may not grow it per
+request, or a host whose framework owns every device allocation. For them the
+filter takes every input and output as a caller-owned device buffer and keeps
+its only scratch (the source views' pose records) in a fixed device array.
+
+These tests call it through the C ABI and compare it with the allocating entry
+point (smvs_create + smvs_run_filter) on the same inputs, for two calls in a
+row whose problems differ (another reference view and fewer source views), so
+that a second call reading the first call's leftover scratch would fail. They
+also check that it rejects more source views than its scratch holds and options
+the engine rejects. Collected last, so a failure here cannot stop the other
+tests from running.
 """
 import ctypes as C
 
@@ -16,17 +20,21 @@ import numpy as np
 import pytest
 
 from sensemap_b200 import _native as N
-from sensemap_b200.patch_match import PatchMatchACMMCuda
-from tests.helpers import photometric_options, problem_from_scene, small_planes
+from sensemap_b200.patch_match import PatchMatchACMMCuda, Problem, View
+from tests.helpers import photometric_options, small_planes
 
 pytestmark = pytest.mark.gpu
 
+# Keep/drop decisions may differ where a reprojection error lies within the
+# texture unit's 1/256 position grid of the limit: the allocating filter samples
+# through hardware textures, this one with the same 8-bit weights in software.
+MAX_DECISION_MISMATCH = 1e-3
 
-def _device_problem(scene, depth_tensors):
+
+def _device_problem(scene, ref, srcs, depth_tensors):
     """smvs_problem over device depth maps (pixels are not read by the filter)."""
-    prob = N.smvs_problem()
-    views = []
-    for i, v in enumerate(scene.views):
+    def view(i):
+        v = scene.views[i]
         cv = N.smvs_view()
         cv.width, cv.height, cv.pixel_format = v.image.shape[1], v.image.shape[0], N.PIX_F32
         cv.pixels = None
@@ -35,57 +43,78 @@ def _device_problem(scene, depth_tensors):
         cv.T[:] = list(np.asarray(v.T, np.float64).reshape(3))
         cv.scale = 1.0
         cv.depth = depth_tensors[i].data_ptr()
-        views.append(cv)
-    ref = scene.ref_index
-    prob.ref = views[ref]
-    srcs = (N.smvs_view * (len(views) - 1))(*[v for i, v in enumerate(views) if i != ref])
-    prob.src = srcs
-    prob.num_src = len(views) - 1
+        return cv
+
+    prob = N.smvs_problem()
+    prob.ref = view(ref)
+    arr = (N.smvs_view * len(srcs))(*[view(i) for i in srcs])
+    prob.src = arr
+    prob.num_src = len(srcs)
     prob.memory = N.MEM_DEVICE
-    return prob, srcs
+    return prob, arr
 
 
-def test_noalloc_filter_matches_allocating_entry_point():
-    import torch
-    scene = small_planes(seed=31)
-    rng = np.random.default_rng(7)
+def _noisy_maps(scene, seed):
+    rng = np.random.default_rng(seed)
     maps = []
     for v in scene.views:
         d = v.depth_gt * (1 + rng.normal(0, 0.01, v.depth_gt.shape)).astype(np.float32)
         d[rng.random(d.shape) < 0.1] = 0
         maps.append(d.astype(np.float32))
-    opt = photometric_options(scene, filter_min_num_consistent=2)
+    return maps
 
-    # Existing (allocating) entry point.
-    with PatchMatchACMMCuda(opt, problem_from_scene(scene, depth_maps=maps)) as pm:
+
+def _allocating_filter(scene, opt, ref, srcs, maps):
+    views = [View(v.image, v.K, v.R, v.T, depth=maps[i]) for i, v in enumerate(scene.views)]
+    with PatchMatchACMMCuda(opt, Problem(ref, list(srcs), views)) as pm:
         pm.RunFilter(False)
-        expected = pm.GetDepthMap()
+        return pm.GetDepthMap()
 
-    dev = [torch.from_numpy(m).cuda() for m in maps]
-    prob, keep = _device_problem(scene, dev)
+
+def test_noalloc_filter_matches_allocating_entry_point():
+    import torch
+    N.lib().smvs_test_take_cuda_error()  # start from a clean thread state
+    scene = small_planes(seed=31)
+    maps = _noisy_maps(scene, 7)
+    opt = photometric_options(scene, filter_min_num_consistent=2)
     copt = opt.to_c()
-    for call in range(2):
-        out = torch.full_like(dev[scene.ref_index], -1.0)
+    dev = [torch.from_numpy(m).cuda() for m in maps]
+    # Two calls in a row on the same stream; the second one filters another
+    # reference view against fewer source views.
+    calls = [(0, [1, 2, 3, 4]), (2, [0, 3])]
+    for k, (ref, srcs) in enumerate(calls):
+        expected = _allocating_filter(scene, opt, ref, srcs, maps)
+        prob, keep = _device_problem(scene, ref, srcs, dev)
+        out = torch.full_like(dev[ref], -1.0)
         N.check(N.lib().smvs_filter_depth_map_noalloc(C.byref(copt), C.byref(prob), C.c_void_p(out.data_ptr()), 0,
                                                       None))
         torch.cuda.synchronize()
         got = out.cpu().numpy()
-        assert np.mean((got > 0) == (expected > 0)) > 0.999, f"call {call}"
-        both = (got > 0) & (expected > 0)
-        np.testing.assert_array_equal(got[both], expected[both])
-        assert (got >= 0).all()  # every pixel written
+        d_in = maps[ref]
+        # Every pixel is written, with the input depth or with 0.
+        assert ((got == d_in) | (got == 0)).all(), f"call {k}"
+        mismatch = float(np.mean((got > 0) != (expected > 0)))
+        assert mismatch <= MAX_DECISION_MISMATCH, f"call {k}: keep/drop decisions differ on {mismatch:.5f}"
+        # The problem is not trivial: the filter drops some pixels and keeps most.
+        assert 0.05 < float(np.mean(expected > 0)) < 0.99
 
 
-def test_noalloc_filter_rejects_too_many_views():
+def test_noalloc_filter_rejects_too_many_views_and_bad_options():
     import torch
     scene = small_planes(seed=32)
     d = torch.ones((scene.views[0].image.shape[0], scene.views[0].image.shape[1]), device="cuda")
-    prob, _ = _device_problem(scene, [d] * len(scene.views))
+    prob, _ = _device_problem(scene, 0, [1, 2, 3, 4], [d] * len(scene.views))
     many = (N.smvs_view * (N.SMVS_MAX_SRC + 1))(*([prob.src[0]] * (N.SMVS_MAX_SRC + 1)))
     prob.src = many
     prob.num_src = N.SMVS_MAX_SRC + 1
     out = torch.zeros_like(d)
-    st = N.lib().smvs_filter_depth_map_noalloc(C.byref(photometric_options(scene).to_c()), C.byref(prob),
-                                               C.c_void_p(out.data_ptr()), 0, None)
+    opt = photometric_options(scene)
+    st = N.lib().smvs_filter_depth_map_noalloc(C.byref(opt.to_c()), C.byref(prob), C.c_void_p(out.data_ptr()), 0,
+                                               None)
     assert st == N.SMVS_EINVAL
     assert "32" in N.last_error()
+    prob2, _ = _device_problem(scene, 0, [1, 2], [d] * len(scene.views))
+    bad = photometric_options(scene, filter_min_num_consistent=-1)
+    st = N.lib().smvs_filter_depth_map_noalloc(C.byref(bad.to_c()), C.byref(prob2), C.c_void_p(out.data_ptr()), 0,
+                                               None)
+    assert st == N.SMVS_EINVAL
