@@ -222,9 +222,10 @@ typedef struct smvs_tuning {
   int ref_tile_tma;  /* 1 (default): stage the reference tile with a TMA load where the image
                         qualifies (rows a multiple of 16 bytes, image at least one tile);
                         0: plain loads */
-  int threads_per_pixel; /* 1, 2 (default) or 4 threads share one pixel's NCC windows; the
-                            smallest value >= this whose shared memory fits the view count
-                            is used. Maps do not depend on it. */
+  int threads_per_pixel; /* 1 (default), 2 or 4 threads share one pixel's NCC windows (1:
+                            the pixel's state in registers and local memory; 2, 4: in
+                            shared memory, the smallest value >= this whose shared memory
+                            fits the view count is used). Maps do not depend on it. */
 } smvs_tuning;
 int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 /* The launch shape in use and whether the last smvs_run staged its reference
@@ -457,6 +458,30 @@ int smvs_init_depth_from_mesh(const smvs_view* view, const double* vertices, siz
 int smvs_init_depth_from_dense_points(const smvs_view* view, const float* xyz, const float* normals,
                                       size_t num_points, int level, int memory, float* depth, float* normal,
                                       float* depth_range, void* stream);
+
+/* ---- coarse-to-fine pyramid --------------------------------------------- */
+/* Size of pyramid level `level` of a width x height image: the factor
+ * 1 / 2^level, but never below 320 pixels on the longer side, and the rounded
+ * sizes (PatchMatchController::ProcessProblem, patch_match_controller.cc:
+ * 4407-4410; Image::Rescale, src/mvs/image.cc:51-52). `factor` may be NULL. */
+int smvs_pyramid_level_size(int width, int height, int level, int* out_width, int* out_height, float* factor);
+/* Image::Rescale / Bitmap::Rescale (src/mvs/image.cc:44-70, src/util/bitmap.cc:
+ * 705-708, FreeImage's bilinear filter) on the device: a grey float image
+ * (0..255) resampled to out_width x out_height with the triangle filter
+ * widened by the inverse scale, rounded to integer grey levels. Device
+ * buffers: `in` width*height, `out` out_width*out_height, `scratch`
+ * out_width*height floats. Enqueued on `stream`. The caller scales K by the
+ * size ratios as Image::Rescale does (image.cc:58-63). */
+int smvs_rescale_image(const float* in, int width, int height, float* out, int out_width, int out_height,
+                       void* scratch, void* stream);
+/* DepthMap::Rescale and NormalMap::Rescale (src/mvs/depth_map.cc:32-55,
+ * src/mvs/normal_map.cc:27-72: InterpolateImage -> ResampleImageBilinear,
+ * src/util/mat.cc:18-58, then the normals re-normalised) on the device, to
+ * out_width x out_height. Device buffers; `normal`/`out_normal` are planar
+ * 3 x H x W and may be NULL, as may depth/out_depth (one of the two pairs must
+ * be given). Enqueued on `stream`. */
+int smvs_resample_maps(const float* depth, const float* normal, int width, int height, float* out_depth,
+                       float* out_normal, int out_width, int out_height, void* stream);
 
 /* ---- view selection and depth ranges from the sparse model (host) -------- */
 /* One image of mvs::Model (src/mvs/model.h): the world-to-camera pose and

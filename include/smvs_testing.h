@@ -24,6 +24,36 @@ int smvs_test_sample_texture(const float* image, int w, int h, int storage, cons
  * test start from a clean thread state after other tests. */
 int smvs_test_take_cuda_error(void);
 
+/* Benchmark inputs: render one view of the synthetic aerial scene (a terrain
+ * of num_hills Gaussian hills {cx, cy, amplitude, sigma} in metres, with
+ * num_boxes box buildings {x0, y0, x1, y1, roof height}) by ray casting on the
+ * GPU, marching `step` metres along each ray (to at most max_dist metres from
+ * the camera, 65536 steps) before bisecting the crossing.
+ * K, R, T: intrinsics (3x3 row-major), world-to-camera rotation and
+ * translation. Outputs are W*H device buffers: albedo in [0, 1] (seeded value
+ * noise with lattice spacing `texel` metres), depth (camera z, 0 where the ray
+ * misses) and a planar 3*W*H camera-frame normal facing the camera.
+ * Synchronous. */
+int smvs_synth_render_aerial(const float* hills, int num_hills, const float* boxes, int num_boxes, uint32_t salt,
+                             float texel, float step, float max_dist, const double* K, const double* R,
+                             const double* T, int width, int height, float* albedo, float* depth, float* normal,
+                             void* stream);
+
+/* Fusion replay waits for the next smvs_fusion_run calls on this thread: each
+ * wait for a predecessor gives up after limit_seconds (0 restores the 20 s
+ * default) and, if withhold_seed >= 0, that seed never releases its
+ * successors (-2: no seed does), so their waits run out and the run returns
+ * SMVS_ETIMEDOUT
+ * (nothing faults or hangs: every wait is bounded and the kernel finishes). */
+int smvs_test_fusion_waits(double limit_seconds, long long withhold_seed);
+
+/* Reference-tile waits of the next smvs_run calls of engine `eng`: each block's
+ * wait for its TMA tile gives up after `polls` mbarrier polls (0 restores the
+ * default bound), and with skip_copy = 1 the copy is never issued, so every
+ * wait runs out; smvs_run's maps are then incomplete and the next
+ * smvs_synchronize or getter returns SMVS_ETIMEDOUT. */
+int smvs_test_tile_waits(smvs_engine* eng, int polls, int skip_copy);
+
 /* Throughput calibration on the current device, used as roofline denominators
  * for this path's bounds: kind 0 = FP32 FMA rate (flop/s, FMA = 2 flop),
  * kind 1 = bilinear texture samples/s from an 8-bit texture with warp-coherent

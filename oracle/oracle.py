@@ -73,6 +73,10 @@ def lib():
         h.orc_fusion_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
         h.orc_fusion_free.restype = None
         h.orc_fusion_free.argtypes = [C.c_void_p]
+        h.orc_resample_maps.restype = C.c_int
+        h.orc_resample_maps.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
+        h.orc_rescale_image.restype = C.c_int
+        h.orc_rescale_image.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
         h.orc_cross_filter_poses.restype = C.c_int
         h.orc_cross_filter_poses.argtypes = [vp, C.c_int, pp, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = h
@@ -346,3 +350,24 @@ def fusion_run(options, images, overlapping_images, max_images: int = 0, masks: 
         return out
     finally:
         lib().orc_fusion_free(h)
+
+
+def resample_maps(planes: np.ndarray, new_h: int, new_w: int, renormalise: bool) -> np.ndarray:
+    """ResampleImageBilinear of a (P, H, W) float32 stack (+ normal re-normalisation)."""
+    a = np.ascontiguousarray(planes, np.float32)
+    P, H, W = a.shape
+    out = np.zeros((P, new_h, new_w), np.float32)
+    if lib().orc_resample_maps(a.ctypes.data, H, W, P, int(renormalise), out.ctypes.data, new_h, new_w) != 0:
+        raise ValueError("orc_resample_maps rejected its arguments")
+    return out
+
+
+def rescale_image(image: np.ndarray, new_h: int, new_w: int) -> np.ndarray:
+    """The bilinear-filter image rescale (grey 0..255 float32)."""
+    a = np.ascontiguousarray(image, np.float32)
+    H, W = a.shape
+    tmp = np.zeros((H, new_w), np.float32)
+    out = np.zeros((new_h, new_w), np.float32)
+    if lib().orc_rescale_image(a.ctypes.data, W, H, tmp.ctypes.data, out.ctypes.data, new_w, new_h) != 0:
+        raise ValueError("orc_rescale_image rejected its arguments")
+    return out

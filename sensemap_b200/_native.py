@@ -251,6 +251,17 @@ _SIGNATURES = {
                                            C.c_void_p]),
     "smvs_test_calibrate": (C.c_int, [C.c_int, C.c_double, C.POINTER(C.c_double)]),
     "smvs_test_take_cuda_error": (C.c_int, []),
+    "smvs_test_fusion_waits": (C.c_int, [C.c_double, C.c_longlong]),
+    "smvs_test_tile_waits": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "smvs_pyramid_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                          C.POINTER(C.c_float)]),
+    "smvs_rescale_image": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,
+                                     C.c_void_p]),
+    "smvs_resample_maps": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int,
+                                     C.c_int, C.c_void_p]),
+    "smvs_synth_render_aerial": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_uint32, C.c_float,
+                                           C.c_float, C.c_float, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                                           C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_test_fusion_caps": (C.c_int, [C.c_int, C.c_int, C.c_int]),
     "smvs_test_fusion_chains": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "smvs_test_fusion_image_ms": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),

@@ -161,6 +161,7 @@ struct smvs_engine {
   bool tma_active = false;        // the last run staged reference tiles with TMA
   int tpp_used = 0;               // threads per pixel of the last run
   int tma_polls = 0;              // TMA tile wait bound (0 = default; a test hook shortens it)
+  int tma_skip_copy = 0;          // test hook: issue no tile copy, so the waits run out
   float* d_ggrad = nullptr;     // W*H (median_filter)
   bool has_init = false;
   bool has_src_depth = false;
@@ -259,7 +260,7 @@ int smvs_internal_prepare_job(smvs::JobParams* p, const smvs_options* o) {
   p->conf_blocks_x = (p->W + 31) / 32;
   // Threads per pixel: the requested value, raised until the block's cost
   // matrices fit in shared memory (maps do not depend on it).
-  const int tpp = smvs::FitThreadsPerPixel(p->R, smvs::ViewBucket(p->N), p->block_x, p->tpp > 0 ? p->tpp : 2);
+  const int tpp = smvs::FitThreadsPerPixel(p->R, smvs::ViewBucket(p->N), p->block_x, p->tpp > 0 ? p->tpp : 1);
   if (!tpp)
     return Fail(SMVS_EINVAL, "no launch shape with sweep_block_x=%d fits %d source views in shared memory",
                 p->block_x, p->N);
@@ -416,7 +417,7 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   p.geom = opt->geom_consistency;
   p.thk = opt->thk < N ? opt->thk : N;  // patch_match_cuda.cu:949-950
   p.block_x = 32;
-  p.tpp = 2;
+  p.tpp = 1;
   p.geom_reg = (float)opt->geom_consistency_regularizer;
   p.geom_max = (float)opt->geom_consistency_max_cost;
   const float* K = prob->ref.K;
@@ -597,6 +598,7 @@ int smvs_run(smvs_engine* e) {
     b.ref_maps = e->d_tmap;
     b.status = e->d_status;
     b.tma_polls = e->tma_polls;
+    b.tma_skip_copy = e->tma_skip_copy;
   }
   if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(b, e->stream); }))) return st;
   int* iters = const_cast<int*>(b.iters);
@@ -751,6 +753,13 @@ int smvs_get_profile(smvs_engine* e, int kind, int* count, double* total_ms) {
   return SMVS_OK;
 }
 void smvs_destroy(smvs_engine* e) { delete e; }
+
+int smvs_test_tile_waits(smvs_engine* e, int polls, int skip_copy) {
+  if (!e || polls < 0) return Fail(SMVS_EINVAL, "tile waits: bad arguments");
+  e->tma_polls = polls;
+  e->tma_skip_copy = skip_copy ? 1 : 0;
+  return SMVS_OK;
+}
 
 // Launch-shape autotuner: times the checkerboard sweep of one iteration of
 // `prob` for every candidate launch shape (threads per block in x, reference

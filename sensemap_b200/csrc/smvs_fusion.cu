@@ -67,6 +67,10 @@ constexpr int kEdgeSh = 1024;          // push-list entries of a record staged i
 constexpr int kStackSh = 512;          // replay stack entries kept in shared memory per warp
 constexpr int kScanItems = 4096;       // items per scan block (256 threads x 16)
 constexpr unsigned long long kWaitLimitNs = 20ull * 1000 * 1000 * 1000;  // bounded waits: 20 s
+// Test hooks (smvs_test_fusion_waits): a shorter wait bound and a seed whose
+// successors are never released, for this thread's next runs.
+thread_local unsigned long long t_wait_limit_ns = 0;  // 0: kWaitLimitNs
+thread_local long long t_withhold = -1;
 
 // Status bits written by the kernels.
 constexpr uint32_t kStTimeout = 1u, kStPool = 2u, kStBad = 4u, kStBig = 8u;
@@ -821,6 +825,8 @@ struct FReplay {
   uint32_t* level;            // with profiling: dependency depth of each seed (else null)
   uint32_t* chain;            // with profiling: the image's longest dependency chain
   unsigned long long* times;  // with profiling: summed ns [waiting, after the wait until release], seeds
+  unsigned long long wait_limit_ns;  // bound of a predecessor wait
+  long long withhold;         // test hook: this seed's successors are never released (-1: none, -2: all)
 };
 
 struct WarpShared {
@@ -875,7 +881,7 @@ __device__ float WarpMedian(const float* vals, int n, float* med, int lane) {
 // Waits until *flag is set: a short spin, then a growing back-off (fewer loads
 // for L2 to serve while most warps wait), bounded in time (status bit on
 // timeout).
-__device__ __forceinline__ void WaitDone(const uint32_t* flag, uint32_t* stats) {
+__device__ __forceinline__ void WaitDone(const uint32_t* flag, uint32_t* stats, unsigned long long limit_ns) {
   unsigned long long t0 = 0;
   unsigned ns = 0;
   for (uint32_t it = 0; LoadAcquire(flag) == 0u; ++it) {
@@ -883,7 +889,7 @@ __device__ __forceinline__ void WaitDone(const uint32_t* flag, uint32_t* stats) 
     if (ns == 0) t0 = GlobalTimer();
     ns = ns < 256 ? ns + 32 : 256;
     __nanosleep(ns);
-    if (GlobalTimer() - t0 > kWaitLimitNs) {
+    if (GlobalTimer() - t0 > limit_ns) {
       atomicOr(&stats[2], kStTimeout);
       return;
     }
@@ -1002,12 +1008,12 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
         latest = max(latest, p);
       }
       for (int o = 16; o > 0; o >>= 1) latest = max(latest, __shfl_xor_sync(0xffffffffu, latest, o));
-      if (lane == 0 && latest >= 0) WaitDone(rp.done + latest, r.stats);
+      if (lane == 0 && latest >= 0) WaitDone(rp.done + latest, r.stats, rp.wait_limit_ns);
       __syncwarp();
       for (int k = lane; k < cnt; k += 32) {
         const int32_t p = v.pred[k];
         if (p < 0) break;
-        WaitDone(rp.done + p, r.stats);
+        WaitDone(rp.done + p, r.stats, rp.wait_limit_ns);
       }
     }
     // The acquires above order the predecessors' mask writes before these
@@ -1150,7 +1156,7 @@ __global__ void __launch_bounds__(32 * kReplayWarps) ReplayKernel(FMaps m, FCons
     // Release the successors: the barrier orders every lane's mask writes
     // before lane 0's release store.
     __syncwarp();
-    if (lane == 0) StoreRelease(&rp.done[s], 1u);
+    if (lane == 0 && rp.withhold != -2 && (long long)s != rp.withhold) StoreRelease(&rp.done[s], 1u);
     if (rp.times && lane == 0) {
       const unsigned long long tw2 = GlobalTimer();
       atomicAdd(rp.times, tw1 - tw0);
@@ -1824,6 +1830,8 @@ int FuseImage(smvs_fusion* f, int image) {
     rp.level = nullptr;
     rp.chain = nullptr;
     rp.times = nullptr;
+    rp.wait_limit_ns = t_wait_limit_ns ? t_wait_limit_ns : kWaitLimitNs;
+    rp.withhold = t_withhold;
     if (f->profiling) {
       if (nseeds > f->level_cap) {
         Free(f, f->d_level);
@@ -1870,7 +1878,7 @@ int CheckStatus(smvs_fusion* f) {
   uint32_t stats[3];
   FU_CUDA(cudaMemcpyAsync(stats, f->d_stats, sizeof(stats), cudaMemcpyDeviceToHost, f->stream));
   FU_CUDA(cudaStreamSynchronize(f->stream));
-  if (stats[2] & kStTimeout) return Fail(SMVS_ETIMEDOUT, "fusion: a replay wait gave up after 20 s");
+  if (stats[2] & kStTimeout) return Fail(SMVS_ETIMEDOUT, "fusion: a replay wait gave up (predecessor never released)");
   if (stats[2] & kStBad) return Fail(SMVS_ECUDA, "fusion: inconsistent replay state");
   return SMVS_OK;
 }
@@ -2241,6 +2249,13 @@ int smvs_test_fusion_caps(int closure_cap, int replay_cap, int replay_stack) {
   t_cap_closure = closure_cap;
   t_cap_replay = replay_cap;
   t_cap_stack = replay_stack;
+  return SMVS_OK;
+}
+
+int smvs_test_fusion_waits(double limit_seconds, long long withhold_seed) {
+  if (limit_seconds < 0 || withhold_seed < -2) return Fail(SMVS_EINVAL, "fusion waits: bad values");
+  t_wait_limit_ns = (unsigned long long)(limit_seconds * 1e9);
+  t_withhold = withhold_seed;
   return SMVS_OK;
 }
 

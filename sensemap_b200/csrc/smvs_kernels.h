@@ -68,6 +68,7 @@ struct Batch {
   const CUtensorMap* ref_maps;  // per job: reference image for TMA tile loads (jobs with tma_box_w > 0)
   int* status;                  // set to 1 when a bounded wait of a kernel gave up
   int tma_polls;                // mbarrier polls before a TMA tile wait gives up (0 = the default bound)
+  int tma_skip_copy;            // test hook: arm the tile barrier but issue no copy (its waits run out)
 };
 
 // Checkerboard blocks: 256 threads, tpp threads per pixel, bx pixels per
@@ -89,13 +90,13 @@ constexpr size_t kMaxDynamicSmem = 227 * 1024 - 2048;
 // alignment slack for the TMA destination), nb pose records, and per pixel the
 // cost matrix, hypotheses, view weights and view probabilities.
 __host__ __device__ inline size_t SweepKernelSmem(int R, int nb, int bx, int tpp) {
-  const size_t P = 256 / tpp;
+  const size_t P = tpp == 1 ? 0 : 256 / tpp;  // tpp == 1 keeps the per-pixel state in registers and local memory
   const size_t tile = (size_t)RefTileW(bx, R) * RefTileH(bx, tpp, R);
   return 128 + sizeof(float) * (tile + (size_t)nb * SMVS_POSE_FLOATS + P * (kSweepHyp * nb + kSweepHyp * 4 + 2 * nb));
 }
 // Same for a local-optimisation block (per pixel: five hypotheses' costs).
 __host__ __device__ inline size_t LocalKernelSmem(int R, int nb, int bx, int tpp) {
-  const size_t P = 256 / tpp;
+  const size_t P = tpp == 1 ? 0 : 256 / tpp;
   const size_t tile = (size_t)RefTileW(bx, R) * RefTileH(bx, tpp, R);
   return 128 + sizeof(float) * (tile + (size_t)nb * SMVS_POSE_FLOATS + P * (5 * nb));
 }

@@ -154,6 +154,7 @@ struct PoolJob {
   void* block = nullptr;   // one allocation for every per-job buffer
   size_t block_bytes = 0;
   double t_submit = 0, t_admit = 0, t_done = 0;
+  cudaEvent_t done_ev = nullptr;  // recorded after the job's last iteration was enqueued
 };
 
 size_t Align256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -184,14 +185,53 @@ struct smvs_pool {
   uint64_t clock = 0;
   size_t bytes_used = 0;
   Arena arena;
-  // Batch arrays on the device and their pinned host staging.
+  // Batch arrays on the device and their pinned host staging (two sets, used
+  // in turn, so that building a batch never waits for the previous upload).
   smvs::JobParams* d_jobs = nullptr;
   int* d_ints = nullptr;   // [iters (cap) | prefix (cap+32) | conf prefix (cap+32)]
   smvs::JobParams* h_jobs = nullptr;
   int* h_ints = nullptr;
   CUtensorMap* d_maps = nullptr;  // per job, as d_jobs
   CUtensorMap* h_maps = nullptr;
+  smvs::JobParams* h_jobs_set[2] = {nullptr, nullptr};
+  int* h_ints_set[2] = {nullptr, nullptr};
+  CUtensorMap* h_maps_set[2] = {nullptr, nullptr};
+  cudaEvent_t staged_ev[2] = {nullptr, nullptr};  // last upload from each set
+  int cur_set = 0;
   int* d_status = nullptr;        // bounded waits of the kernels that gave up
+  int* h_status = nullptr;        // pinned copy of d_status, refreshed after every step
+  // Pose records of admitted jobs go through a pinned ring (no host sync).
+  float* h_poses = nullptr;
+  size_t poses_cap = 0, poses_off = 0;
+  // Views uploaded from host memory: converted on copy_stream straight from
+  // pinned staging slots (the compute stream waits for upload_ev before its
+  // next launches), so uploads overlap the running iteration.
+  cudaStream_t copy_stream = nullptr;
+  struct Staging {
+    void* host = nullptr;
+    size_t bytes = 0;
+    cudaEvent_t done = nullptr;
+  };
+  Staging staging[4];
+  int staging_next = 0;
+  cudaEvent_t upload_ev = nullptr;
+  bool upload_pending = false;
+  // Completion tracking without host synchronisation: jobs whose last
+  // iteration is enqueued hold an event; the host keeps at most
+  // kMaxStepsInFlight steps queued ahead of the GPU.
+  std::vector<int64_t> finishing;
+  std::deque<cudaEvent_t> step_events;
+  std::vector<cudaEvent_t> free_events;
+  cudaEvent_t GetEvent() {
+    if (!free_events.empty()) {
+      cudaEvent_t e = free_events.back();
+      free_events.pop_back();
+      return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return e;
+  }
   int capacity = 0;
   // Graph of the current batch's step (valid while the batch is unchanged).
   cudaGraphExec_t graph = nullptr;
@@ -203,8 +243,27 @@ struct smvs_pool {
   int64_t steps = 0;
 
   ~smvs_pool() {
+    if (copy_stream) cudaStreamSynchronize(copy_stream);
     if (stream) cudaStreamSynchronize(stream);
     if (graph) cudaGraphExecDestroy(graph);
+    for (auto& kv : jobs)
+      if (kv.second.done_ev) cudaEventDestroy(kv.second.done_ev);
+    for (cudaEvent_t e : step_events) cudaEventDestroy(e);
+    for (cudaEvent_t e : free_events) cudaEventDestroy(e);
+    for (int i = 0; i < 2; ++i) {
+      if (staged_ev[i]) cudaEventDestroy(staged_ev[i]);
+      if (h_jobs_set[i] != h_jobs) cudaFreeHost(h_jobs_set[i]);
+      if (h_ints_set[i] != h_ints) cudaFreeHost(h_ints_set[i]);
+      if (h_maps_set[i] != h_maps) cudaFreeHost(h_maps_set[i]);
+    }
+    for (auto& st : staging) {
+      if (st.done) cudaEventDestroy(st.done);
+      cudaFreeHost(st.host);
+    }
+    if (upload_ev) cudaEventDestroy(upload_ev);
+    cudaFreeHost(h_status);
+    cudaFreeHost(h_poses);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
     for (auto& kv : jobs)
       if (kv.second.block) cudaFree(kv.second.block);
     for (auto& kv : views) ReleaseView(kv.second);
@@ -274,17 +333,25 @@ int EnsureCapacity(smvs_pool* P, int n) {
   cudaFree(P->d_jobs);
   cudaFree(P->d_ints);
   cudaFree(P->d_maps);
-  cudaFreeHost(P->h_jobs);
-  cudaFreeHost(P->h_ints);
-  cudaFreeHost(P->h_maps);
+  for (int i = 0; i < 2; ++i) {
+    cudaFreeHost(P->h_jobs_set[i]);
+    cudaFreeHost(P->h_ints_set[i]);
+    cudaFreeHost(P->h_maps_set[i]);
+    P->h_jobs_set[i] = nullptr; P->h_ints_set[i] = nullptr; P->h_maps_set[i] = nullptr;
+  }
   P->d_jobs = nullptr; P->d_ints = nullptr; P->h_jobs = nullptr; P->h_ints = nullptr;
   P->d_maps = nullptr; P->h_maps = nullptr;
   POOL_CUDA(cudaMalloc(&P->d_jobs, sizeof(smvs::JobParams) * cap));
   POOL_CUDA(cudaMalloc(&P->d_ints, sizeof(int) * IntsSize(cap)));
   POOL_CUDA(cudaMalloc(&P->d_maps, sizeof(CUtensorMap) * cap));
-  POOL_CUDA(cudaMallocHost(&P->h_jobs, sizeof(smvs::JobParams) * cap));
-  POOL_CUDA(cudaMallocHost(&P->h_ints, sizeof(int) * IntsSize(cap)));
-  POOL_CUDA(cudaMallocHost(&P->h_maps, sizeof(CUtensorMap) * cap));
+  for (int i = 0; i < 2; ++i) {
+    POOL_CUDA(cudaMallocHost(&P->h_jobs_set[i], sizeof(smvs::JobParams) * cap));
+    POOL_CUDA(cudaMallocHost(&P->h_ints_set[i], sizeof(int) * IntsSize(cap)));
+    POOL_CUDA(cudaMallocHost(&P->h_maps_set[i], sizeof(CUtensorMap) * cap));
+  }
+  P->h_jobs = P->h_jobs_set[P->cur_set];
+  P->h_ints = P->h_ints_set[P->cur_set];
+  P->h_maps = P->h_maps_set[P->cur_set];
   P->capacity = cap;
   P->batch_dirty = true;
   return SMVS_OK;
@@ -304,7 +371,7 @@ int smvs_pool_options_default(smvs_pool_options* o) {
   o->use_graphs = 1;
   o->ref_tile_tma = 1;
   o->gpu_index = -1;
-  o->sweep_threads_per_pixel = 2;
+  o->sweep_threads_per_pixel = 1;
   return SMVS_OK;
 }
 
@@ -341,9 +408,18 @@ int smvs_pool_create(const smvs_pool_options* o, void* stream, smvs_pool** out) 
   int st = EnsureCapacity(P, o->max_active_jobs);
   if (st) { delete P; return st; }
   if (cudaMalloc(&P->d_status, sizeof(int)) != cudaSuccess ||
-      cudaMemsetAsync(P->d_status, 0, sizeof(int), P->stream) != cudaSuccess) {
+      cudaMemsetAsync(P->d_status, 0, sizeof(int), P->stream) != cudaSuccess ||
+      cudaMallocHost(&P->h_status, sizeof(int)) != cudaSuccess) {
     delete P;
     return Fail(SMVS_ENOMEM, "pool status word");
+  }
+  *P->h_status = 0;
+  P->poses_cap = (size_t)64 * 1024;
+  if (cudaMallocHost(&P->h_poses, P->poses_cap * sizeof(float)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&P->copy_stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&P->upload_ev, cudaEventDisableTiming) != cudaSuccess) {
+    delete P;
+    return Fail(SMVS_ENOMEM, "pool staging");
   }
   *out = P;
   return SMVS_OK;
@@ -369,24 +445,40 @@ int smvs_pool_add_view(smvs_pool* P, int64_t view_id, const smvs_view* v, int me
   pv.meta.pixels = nullptr; pv.meta.depth = nullptr; pv.meta.normal = nullptr;
   cudaError_t e = cudaMallocPitch(&pv.img, &pv.pitch, (size_t)w * StorageBytes(P->opt.image_storage), h);
   if (e == cudaSuccess) e = cudaMalloc((void**)&pv.ref, (size_t)w * h * 4);
-  void* staged = const_cast<void*>(v->pixels);
-  void* tmp = nullptr;
-  if (e == cudaSuccess && memory != SMVS_MEM_DEVICE) {
-    e = cudaMalloc(&tmp, stride * h);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(tmp, v->pixels, stride * h, cudaMemcpyHostToDevice, P->stream);
-    staged = tmp;
+  if (e == cudaSuccess && memory == SMVS_MEM_DEVICE) {
+    // Device pixels: convert on the compute stream (ordered before every job).
+    e = smvs::LaunchConvertImage(v->pixels, v->pixel_format, stride, w, h, pv.img, P->opt.image_storage, pv.pitch, 1,
+                                 P->stream);
+    if (e == cudaSuccess)
+      e = smvs::LaunchConvertImage(v->pixels, v->pixel_format, stride, w, h, pv.ref, 3, (size_t)w * 4, 1, P->stream);
+  } else if (e == cudaSuccess) {
+    // Host pixels: copy them into a pinned staging slot (the caller's buffer
+    // is only guaranteed during this call), then convert on the copy stream,
+    // reading the slot over the bus, while the compute stream keeps running.
+    smvs_pool::Staging& slot = P->staging[P->staging_next];
+    P->staging_next = (P->staging_next + 1) % 4;
+    if (slot.done) e = cudaEventSynchronize(slot.done);  // its previous upload has been converted
+    if (e == cudaSuccess && slot.bytes < stride * h) {
+      cudaFreeHost(slot.host);
+      slot.host = nullptr;
+      slot.bytes = 0;
+      e = cudaHostAlloc(&slot.host, stride * h, cudaHostAllocMapped | cudaHostAllocPortable);
+      if (e == cudaSuccess) slot.bytes = stride * h;
+    }
+    if (e == cudaSuccess && !slot.done) e = cudaEventCreateWithFlags(&slot.done, cudaEventDisableTiming);
+    if (e == cudaSuccess) {
+      memcpy(slot.host, v->pixels, stride * h);
+      e = smvs::LaunchConvertImage(slot.host, v->pixel_format, stride, w, h, pv.img, P->opt.image_storage, pv.pitch,
+                                   1, P->copy_stream);
+    }
+    if (e == cudaSuccess)
+      e = smvs::LaunchConvertImage(slot.host, v->pixel_format, stride, w, h, pv.ref, 3, (size_t)w * 4, 1,
+                                   P->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(slot.done, P->copy_stream);
+    if (e == cudaSuccess) e = cudaEventRecord(P->upload_ev, P->copy_stream);
+    if (e == cudaSuccess) P->upload_pending = true;
   }
-  if (e == cudaSuccess)
-    e = smvs::LaunchConvertImage(staged, v->pixel_format, stride, w, h, pv.img, P->opt.image_storage, pv.pitch, 1, P->stream);
-  if (e == cudaSuccess)
-    e = smvs::LaunchConvertImage(staged, v->pixel_format, stride, w, h, pv.ref, 3, (size_t)w * 4, 1, P->stream);
   if (e == cudaSuccess) e = MakeTexture(pv.img, P->opt.image_storage, w, h, pv.pitch, &pv.tex);
-  if (tmp) {
-    cudaStreamSynchronize(P->stream);
-    cudaFree(tmp);
-  } else if (e == cudaSuccess && memory != SMVS_MEM_DEVICE) {
-    e = cudaStreamSynchronize(P->stream);
-  }
   if (e != cudaSuccess) {
     P->ReleaseView(pv);
     return Fail(SMVS_ECUDA, "add_view: %s", cudaGetErrorString(e));
@@ -548,10 +640,17 @@ int Admit(smvs_pool* P, PoolJob& J) {
     P->bytes_used += J.block_bytes;
   }
   CarveJob(J, W, H, N);
-  std::vector<float> poses((size_t)N * SMVS_POSE_FLOATS);
+  const size_t nposes = (size_t)N * SMVS_POSE_FLOATS;
+  if (P->poses_off + nposes > P->poses_cap) {
+    // Ring wrap: every earlier record copy must have completed.
+    POOL_CUDA(cudaStreamSynchronize(P->stream));
+    P->poses_off = 0;
+  }
+  float* poses = P->h_poses + P->poses_off;
+  P->poses_off += nposes;
   for (int i = 0; i < N; ++i)
-    smvs_internal_pose_record(&rv.meta, &P->views[J.srcs[i]].meta, poses.data() + (size_t)i * SMVS_POSE_FLOATS);
-  POOL_CUDA(cudaMemcpyAsync((void*)p.poses, poses.data(), poses.size() * 4, cudaMemcpyHostToDevice, P->stream));
+    smvs_internal_pose_record(&rv.meta, &P->views[J.srcs[i]].meta, poses + (size_t)i * SMVS_POSE_FLOATS);
+  POOL_CUDA(cudaMemcpyAsync((void*)p.poses, poses, nposes * 4, cudaMemcpyHostToDevice, P->stream));
   POOL_CUDA(smvs::LaunchPrepRef(p, (float*)p.ref_sum, (float*)p.ref_sqsum, (float*)p.grad, P->stream));
   if (!o.init_depth_random) {
     const size_t WH = (size_t)W * H;
@@ -560,8 +659,6 @@ int Admit(smvs_pool* P, PoolJob& J) {
   }
   p.stage_key = smvs::StageKey(o.random_seed, smvs::kStageInit);
   POOL_CUDA(smvs::LaunchInit(p, o.init_depth_random, (float)o.depth_min, (float)o.depth_max, P->stream));
-  // The host copy of `poses` must survive the async copy.
-  POOL_CUDA(cudaStreamSynchronize(P->stream));
   P->launches += 2;
   J.state = kActive;
   J.iter = 0;
@@ -574,8 +671,12 @@ int Admit(smvs_pool* P, PoolJob& J) {
 int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs::Batch>& groups) {
   groups.clear();
   if (ids.empty()) return SMVS_OK;
-  // The staging buffers may still feed the previous upload.
-  POOL_CUDA(cudaStreamSynchronize(P->stream));
+  // Use the other staging set; it may still feed the upload before last.
+  P->cur_set ^= 1;
+  if (P->staged_ev[P->cur_set]) POOL_CUDA(cudaEventSynchronize(P->staged_ev[P->cur_set]));
+  P->h_jobs = P->h_jobs_set[P->cur_set];
+  P->h_ints = P->h_ints_set[P->cur_set];
+  P->h_maps = P->h_maps_set[P->cur_set];
   std::map<std::tuple<int, int, int, int, int>, std::vector<int64_t>> by_key;
   for (int64_t id : ids) {
     const smvs::JobParams& p = P->jobs[id].p;
@@ -599,6 +700,7 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
     b.block_x = std::get<3>(kv.first);
     b.tpp = std::get<4>(kv.first);
     b.tma_polls = 0;
+    b.tma_skip_copy = 0;
     const int by = smvs::SweepRows(b.block_x, b.tpp);
     int tot = 0, ctot = 0;
     for (int k = 0; k < n; ++k) {
@@ -635,6 +737,8 @@ int Upload(smvs_pool* P, int njobs) {
   POOL_CUDA(cudaMemcpyAsync(P->d_maps, P->h_maps, sizeof(CUtensorMap) * njobs, cudaMemcpyHostToDevice, P->stream));
   POOL_CUDA(cudaMemcpyAsync(P->d_ints, P->h_ints, sizeof(int) * IntsSize(P->capacity), cudaMemcpyHostToDevice,
                             P->stream));
+  if (!P->staged_ev[P->cur_set]) POOL_CUDA(cudaEventCreateWithFlags(&P->staged_ev[P->cur_set], cudaEventDisableTiming));
+  POOL_CUDA(cudaEventRecord(P->staged_ev[P->cur_set], P->stream));
   return SMVS_OK;
 }
 
@@ -650,13 +754,59 @@ int EnqueueIteration(smvs_pool* P, const std::vector<smvs::Batch>& groups) {
 
 }  // namespace
 
+// Retire finishing jobs whose last iteration has completed on the GPU (wait
+// for them with `block`). A kernel's bounded wait that gave up shows in the
+// status word copied back after every step.
+static int PollFinishing(smvs_pool* P, bool block) {
+  std::vector<int64_t> still;
+  int st = SMVS_OK;
+  for (int64_t id : P->finishing) {
+    PoolJob& J = P->jobs[id];
+    cudaError_t e = block ? cudaEventSynchronize(J.done_ev) : cudaEventQuery(J.done_ev);
+    if (e == cudaErrorNotReady) {
+      (void)cudaGetLastError();
+      still.push_back(id);
+      continue;
+    }
+    if (e != cudaSuccess) {
+      st = Fail(SMVS_ECUDA, "pool step: %s", cudaGetErrorString(e));
+      still.push_back(id);
+      continue;
+    }
+    if (*P->h_status) st = Fail(SMVS_ETIMEDOUT, "a reference-tile copy did not complete; active jobs' maps are incomplete");
+    P->free_events.push_back(J.done_ev);
+    J.done_ev = nullptr;
+    J.state = kDone;
+    J.t_done = NowSeconds();
+    P->views[J.ref].refs--;
+    for (int64_t sid : J.srcs) P->views[sid].refs--;
+  }
+  P->finishing.swap(still);
+  return st;
+}
+
+// Wait until `job` is no longer finishing (its maps are final).
+static int SettleJob(smvs_pool* P, PoolJob& J) {
+  if (!J.done_ev) return SMVS_OK;
+  POOL_CUDA(cudaEventSynchronize(J.done_ev));
+  return PollFinishing(P, false);
+}
+
 int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
   if (!P) return Fail(SMVS_EINVAL, "null pool");
   cudaSetDevice(P->device);
   (void)cudaGetLastError();
+  int pst = PollFinishing(P, false);
+  if (pst) return pst;
+  // Uploads of views from host memory run on the copy stream: the compute
+  // stream's next launches wait for them.
+  if (P->upload_pending) {
+    POOL_CUDA(cudaStreamWaitEvent(P->stream, P->upload_ev, 0));
+    P->upload_pending = false;
+  }
   // 1. Admit queued jobs while slots and memory allow.
   std::vector<int64_t> admitted;
-  while (!P->queue.empty() && (int)P->active.size() < P->opt.max_active_jobs) {
+  while (!P->queue.empty() && (int)(P->active.size() + P->finishing.size()) < P->opt.max_active_jobs) {
     PoolJob& J = P->jobs[P->queue.front()];
     int st = Admit(P, J);
     if (st == SMVS_ENOMEM) {
@@ -664,7 +814,8 @@ int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
         P->arena.Put(J.block, J.block_bytes);
         J.block = nullptr;
       }
-      if (P->active.empty()) return Fail(SMVS_ENOMEM, "job %lld does not fit the memory budget", (long long)J.id);
+      if (P->active.empty() && P->finishing.empty())
+        return Fail(SMVS_ENOMEM, "job %lld does not fit the memory budget", (long long)J.id);
       break;  // wait for active jobs to finish
     }
     if (st) return st;
@@ -714,34 +865,42 @@ int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
       if (st) return st;
     }
     P->launches += 5 * (int64_t)P->groups.size();
-  }
-  P->steps++;
-  POOL_CUDA(cudaStreamSynchronize(P->stream));
-  {
-    int status = 0;
-    POOL_CUDA(cudaMemcpy(&status, P->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-    if (status) return Fail(SMVS_ETIMEDOUT, "a reference-tile copy did not complete; active jobs' maps are incomplete");
-  }
-  // 4. Retire jobs that finished their iterations.
-  const double now = NowSeconds();
-  std::vector<int64_t> still;
-  for (int64_t id : P->active) {
-    PoolJob& J = P->jobs[id];
-    J.iter++;
-    if (J.iter >= J.opt.num_iterations) {
-      J.state = kDone;
-      J.t_done = now;
-      P->views[J.ref].refs--;
-      for (int64_t s : J.srcs) P->views[s].refs--;
-      P->batch_dirty = true;
-    } else {
-      still.push_back(id);
+    POOL_CUDA(cudaMemcpyAsync(P->h_status, P->d_status, sizeof(int), cudaMemcpyDeviceToHost, P->stream));
+    // 4. Jobs whose last iteration is now enqueued leave the batch; they are
+    // done once the GPU has run it.
+    std::vector<int64_t> still;
+    for (int64_t id : P->active) {
+      PoolJob& J = P->jobs[id];
+      J.iter++;
+      if (J.iter >= J.opt.num_iterations) {
+        J.done_ev = P->GetEvent();
+        POOL_CUDA(cudaEventRecord(J.done_ev, P->stream));
+        P->finishing.push_back(id);
+        P->batch_dirty = true;
+      } else {
+        still.push_back(id);
+      }
     }
+    P->active.swap(still);
+    P->steps++;
+    // Keep at most two steps queued ahead of the GPU.
+    cudaEvent_t ev = P->GetEvent();
+    POOL_CUDA(cudaEventRecord(ev, P->stream));
+    P->step_events.push_back(ev);
+    while (P->step_events.size() > 2) {
+      POOL_CUDA(cudaEventSynchronize(P->step_events.front()));
+      P->free_events.push_back(P->step_events.front());
+      P->step_events.pop_front();
+    }
+  } else if (!P->finishing.empty()) {
+    // Nothing to enqueue: wait for the oldest finishing job.
+    POOL_CUDA(cudaEventSynchronize(P->jobs[P->finishing.front()].done_ev));
   }
-  P->active.swap(still);
+  pst = PollFinishing(P, false);
+  if (pst) return pst;
   if (stats) {
     stats->queued = (int)P->queue.size();
-    stats->active = (int)P->active.size();
+    stats->active = (int)(P->active.size() + P->finishing.size());
     int done = 0;
     for (auto& kv : P->jobs) done += kv.second.state == kDone;
     stats->done = done;
@@ -760,6 +919,10 @@ int smvs_pool_job_state(smvs_pool* P, int64_t job_id, int* state, double* latenc
   if (!P || !state) return Fail(SMVS_EINVAL, "null argument");
   auto it = P->jobs.find(job_id);
   if (it == P->jobs.end()) return Fail(SMVS_EINVAL, "unknown job %lld", (long long)job_id);
+  if (it->second.done_ev) {
+    const int st = PollFinishing(P, false);
+    if (st) return st;
+  }
   *state = it->second.state;
   if (latency_s) *latency_s = it->second.state == kDone ? it->second.t_done - it->second.t_submit : -1.0;
   return SMVS_OK;
@@ -770,6 +933,10 @@ int smvs_pool_get_map(smvs_pool* P, int64_t job_id, int which, void* out) {
   auto it = P->jobs.find(job_id);
   if (it == P->jobs.end()) return Fail(SMVS_EINVAL, "unknown job %lld", (long long)job_id);
   PoolJob& J = it->second;
+  {
+    const int st = SettleJob(P, J);
+    if (st) return st;
+  }
   if (J.state != kDone || !J.block) return Fail(SMVS_ESTATE, "job %lld has no results", (long long)job_id);
   const size_t WH = (size_t)J.p.W * J.p.H;
   const void* src = nullptr;
@@ -792,6 +959,10 @@ int smvs_pool_keep_maps(smvs_pool* P, int64_t job_id) {
   auto it = P->jobs.find(job_id);
   if (it == P->jobs.end()) return Fail(SMVS_EINVAL, "unknown job %lld", (long long)job_id);
   PoolJob& J = it->second;
+  {
+    const int st = SettleJob(P, J);
+    if (st) return st;
+  }
   if (J.state != kDone || !J.block) return Fail(SMVS_ESTATE, "job %lld has no results", (long long)job_id);
   auto vit = P->views.find(J.ref);
   if (vit == P->views.end()) return Fail(SMVS_ESTATE, "reference view of job %lld was evicted", (long long)job_id);
@@ -803,6 +974,10 @@ int smvs_pool_release(smvs_pool* P, int64_t job_id) {
   auto it = P->jobs.find(job_id);
   if (it == P->jobs.end()) return Fail(SMVS_EINVAL, "unknown job %lld", (long long)job_id);
   PoolJob& J = it->second;
+  {
+    const int st = SettleJob(P, J);
+    if (st) return st;
+  }
   if (J.state == kActive) return Fail(SMVS_ESTATE, "job %lld is running", (long long)job_id);
   if (J.state == kQueued) {
     for (auto q = P->queue.begin(); q != P->queue.end(); ++q)
@@ -811,7 +986,8 @@ int smvs_pool_release(smvs_pool* P, int64_t job_id) {
     for (int64_t s : J.srcs) P->views[s].refs--;
   }
   if (J.block) {
-    cudaStreamSynchronize(P->stream);
+    // Its kernels have completed (SettleJob); copies enqueued from it since
+    // (keep_maps) precede, in stream order, any kernel of a job that reuses it.
     P->arena.Put(J.block, J.block_bytes);  // kept as cached memory (still counted in bytes_used)
     J.block = nullptr;
   }

@@ -92,7 +92,7 @@ __device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity, uint32_t
 // a bounded wait (`polls`). Returns false after setting *status if the copy
 // did not land; the caller then leaves the block's pixels unchanged.
 __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile, int x, int y, uint32_t bytes,
-                                             uint64_t* mbar, int* status, uint32_t polls) {
+                                             uint64_t* mbar, int* status, uint32_t polls, bool skip_copy) {
   const uint32_t bar = SmemAddr(mbar);
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
   if (leader) {
@@ -103,15 +103,18 @@ __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile
   __syncthreads();
   if (leader) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
-        ::"r"(SmemAddr(tile)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
+    if (!skip_copy)
+      asm volatile(
+          "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+          ::"r"(SmemAddr(tile)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+          : "memory");
   }
   const bool landed = MbarWait(bar, 0, polls);
   if (!__syncthreads_or(!landed)) return true;  // block-uniform outcome
   if (leader) atomicExch(status, 1);
-  MbarWait(bar, 0, kTmaWaitPolls);  // let a late copy land before the block's shared memory is released
+  // Let a late copy land before the block's shared memory is released (no
+  // copy is in flight when the test hook skipped it).
+  if (!skip_copy) MbarWait(bar, 0, kTmaWaitPolls);
   return false;
 }
 
@@ -132,7 +135,7 @@ __device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobP
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += blockDim.x * blockDim.y) poses[i] = __ldg(p.poses + i);
   return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, b.status,
-                      b.tma_polls > 0 ? (uint32_t)b.tma_polls : kTmaWaitPolls);
+                      b.tma_polls > 0 ? (uint32_t)b.tma_polls : kTmaWaitPolls, b.tma_skip_copy != 0);
 }
 
 // Batched launches: find this block's job (binary search over the block
@@ -355,6 +358,328 @@ struct SweepSmem {
 
 // SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
 // propagate_depth): one checkerboard colour, G threads per pixel.
+// Threads-per-pixel 1: the thread-per-pixel form of SweepFromCheckerBoardOpt
+// (kernel_functions.cu:2136-2560) and LocalOptimization (:2736-2931). The
+// pixel's cost matrix M[kMaxHyp][NB], its hypotheses and view weights are
+// per-thread arrays (NB = the view bucket): the compiler keeps them in the
+// thread's local frame, which lives in the L1 next to the texture cache the
+// cost windows read. Measured on the 1600x1200, 10-view workload this is the
+// fastest layout: keeping those arrays in shared memory shrinks the L1 that the
+// texture fetches need (the G = 2 / 4 kernels below), and keeping them in an
+// L2-resident global scratch makes the scalar phases wait on L2 latency. The
+// arithmetic is the same as the G-lane kernels (NccCost<R,S,1> sums the window
+// in the same canonical order), so maps are identical for every
+// threads-per-pixel value.
+template <int R, int S, int NB>
+__global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colour) {
+  extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  __shared__ uint64_t mbar;
+  int job, blk, iter;
+  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  const JobParams& p = sp;
+  if (iter >= p.num_iterations) return;  // finished job of the batch (block-uniform)
+  const float th_mc = p.th_tab[iter];
+  const uint64_t skey = StageKey(p.seed, StageSweep(iter, colour));
+  const int kBX = b.block_x, kBY = kThreads / b.block_x;
+  const int tw = RefTileW(kBX, R), th = kBY + 2 * R;
+  float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
+  float* poses = tile + tw * th;
+  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, &mbar)) return;  // block-uniform
+  __syncthreads();
+  const int tx = threadIdx.x % kBX, ty = threadIdx.x / kBX;
+  const int row = row0 + ty;
+  const int col = col0 + 2 * tx + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;
+  const int W = p.W, H = p.H, N = p.N;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  const unsigned gmask = GroupMask<1>();
+  Rng r(skey, (uint32_t)pix);
+  float depth = p.depth[pix];
+  float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const float grad = p.grad[pix];
+  const float depth_min = p.depth_min;
+  const float depth_max = (float)(1.2 * (double)p.depth_max);  // [quirk] :2213
+  const float a1 = fminf(p.rand_a1, (float)(180.0 * 0.0174532925199432));
+  const float a2 = fminf(p.rand_a2, (float)(90.0 * 0.0174532925199432));
+  const float* iK = p.refiK;
+  const float vd[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
+  const float ivl = rsqrtf(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
+
+  float hyp[kMaxHyp][4];
+  int ns = 0;
+  hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
+  ns = 1;
+  if (grad >= 1.0f) {  // :2237-2276
+    float nconf[4], O[4];
+    int nvalid = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      O[i] = (float)i;
+      const int u = kNeighborOffs[i][1] + col, v = kNeighborOffs[i][0] + row;
+      if (u < 0 || u >= W || v < 0 || v >= H) { nconf[i] = FLT_MAX; continue; }
+      nvalid++;
+      nconf[i] = p.conf[(size_t)v * W + u];
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+      for (int j = 0; j < 3 - i; ++j)
+        if (nconf[j] > nconf[j + 1]) {
+          float t = nconf[j]; nconf[j] = nconf[j + 1]; nconf[j + 1] = t;
+          t = O[j]; O[j] = O[j + 1]; O[j + 1] = t;
+        }
+    nvalid = min(nvalid, 2);
+    for (int i = 0; i < nvalid; ++i) {
+      const int idx = (int)O[i];
+      const int u = kNeighborOffs[idx][1] + col, v = kNeighborOffs[idx][0] + row;
+      const size_t q = (size_t)v * W + u;
+      float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
+      CorrectNormal(nn, vd, ivl);
+      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, v, u, vd);
+      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      ns++;
+    }
+  }
+  for (int k = 0; k < 8; ++k) {  // :2278-2327
+    int br = 0, bc = 0;
+    float best = FLT_MAX;
+#pragma unroll
+    for (int s = 0; s < 10; ++s) {
+      const int nr = row + kDirSamples[k][2 * s], nc = col + kDirSamples[k][2 * s + 1];
+      if (nr < 0 || nr >= H || nc < 0 || nc >= W) continue;
+      const float nconf = p.conf[(size_t)nr * W + nc];
+      if (best > nconf) { br = nr; bc = nc; best = nconf; }
+    }
+    if (best < FLT_MAX) {
+      const size_t q = (size_t)br * W + bc;
+      float nn[3] = {p.normal[q], p.normal[WH + q], p.normal[2 * WH + q]};
+      CorrectNormal(nn, vd, ivl);
+      hyp[ns][3] = PropagateDepth(p.depth[q], nn, iK, br, bc, vd);
+      hyp[ns][0] = nn[0]; hyp[ns][1] = nn[1]; hyp[ns][2] = nn[2];
+      ns++;
+    }
+  }
+
+  PixRef pr;
+  pr.center = p.ref[pix];
+  pr.rsum = p.ref_sum[pix];
+  pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
+  pr.ws = tw;
+  pr.win = tile + ty * tw + (col - col0) + RefTileShift(R);
+  float M[kMaxHyp][NB];
+  for (int v = 0; v < N; ++v) M[0][v] = p.cost[(size_t)v * WH + pix];
+  float vw[NB];
+  float costs[kMaxHyp];
+  // Two evaluation phases share one call site of the cost code: phase 0 scores
+  // the propagated hypotheses 1..ns-1, phase 1 the refinement hypotheses 1..4.
+  int h_end = ns;
+  for (int phase = 0; phase < 2; ++phase) {
+    for (int h = 1; h < h_end; ++h)
+      for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S, 1>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr, p.refK, 0, gmask);
+    if (phase == 1) break;
+
+    // ACMM view selection, :2364-2427.
+    uint32_t flags = 0;
+    float probs[NB];
+    for (int v = 0; v < N; ++v) {
+      unsigned n1 = 0, n2 = 0;
+      float pv = 0.f;
+      for (int h = 0; h < ns; ++h) {
+        const float cst = M[h][v];
+        pv += __expf(-cst * cst * p.inv_beta2);
+        n1 += (cst < th_mc);
+        n2 += (cst > p.max_mc);
+      }
+      probs[v] = pv;
+      if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
+    }
+    if (flags == 0) return;
+    for (int v = 0; v < N; ++v)
+      if (!((flags >> v) & 1u)) probs[v] = 0.f;
+    {
+      float sum = 0.f;
+      for (int v = 0; v < N; ++v) sum += probs[v];
+      const float inv = 1.0f / sum;
+      float cum = 0.f;
+      for (int v = 0; v < N; ++v) { cum += probs[v] * inv; probs[v] = cum; }
+    }
+    for (int v = 0; v < N; ++v) vw[v] = 0.f;
+    for (int s = 0; s < p.num_samples; ++s) {
+      const float rp = r.Uniform() - FLT_EPSILON;
+      for (int v = 0; v < N; ++v)
+        if (probs[v] > rp) {
+          if (p.random_opt) vw[v] = 1.0f; else vw[v] += 1.0f;
+          break;
+        }
+    }
+    float wn = 0.f;
+    for (int v = 0; v < N; ++v) wn += vw[v];
+    if (wn <= 1e-5f) return;
+    const float iwn = 1.0f / wn;
+    uint32_t sel = 0;
+    for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
+    for (int h = 0; h < ns; ++h) {
+      float cs = 0.f;
+      for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
+      costs[h] = cs;
+    }
+    p.view_sel[pix] = sel;
+    int mi = -1;
+    {
+      float m = FLT_MAX;
+      for (int h = 0; h < ns; ++h)
+        if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
+    }
+    if (mi < 0) return;
+    depth = hyp[mi][3];
+    normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
+    if (mi != 0)
+      for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
+
+    // Refinement hypotheses, :2449-2486.
+    float nn[3];
+    const float pd_min = (1.0f - p.rand_depth_ratio) * depth, pd_max = (1.0f + p.rand_depth_ratio) * depth;
+    const float ndepth = r.Uniform() * (pd_max - pd_min) + pd_min;  // PerturbDepth :141-147
+    PerturbNormalACMH(normal, nn, a1, a2, r);
+    CorrectNormal(nn, vd, ivl);
+    const float rdepth = r.Uniform() * (depth_max - depth_min) + depth_min;
+    float rn[3];
+    RandomNormal(r, vd, rn);
+    CorrectNormal(rn, vd, ivl);
+    hyp[0][0] = normal[0]; hyp[0][1] = normal[1]; hyp[0][2] = normal[2]; hyp[0][3] = depth;
+    hyp[1][0] = nn[0]; hyp[1][1] = nn[1]; hyp[1][2] = nn[2]; hyp[1][3] = depth;
+    hyp[2][0] = normal[0]; hyp[2][1] = normal[1]; hyp[2][2] = normal[2]; hyp[2][3] = ndepth;
+    hyp[3][0] = rn[0]; hyp[3][1] = rn[1]; hyp[3][2] = rn[2]; hyp[3][3] = depth;
+    hyp[4][0] = normal[0]; hyp[4][1] = normal[1]; hyp[4][2] = normal[2]; hyp[4][3] = rdepth;
+    h_end = 5;
+  }
+  // :2488-2559: weighted refinement costs, argmin, write back.
+  for (int h = 0; h < 5; ++h) {
+    float cs = 0.f;
+    for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
+    costs[h] = cs;
+  }
+  int mi = -1;
+  {
+    float m = FLT_MAX;
+    for (int h = 0; h < 5; ++h)
+      if (costs[h] <= m) { m = costs[h]; mi = h; }
+  }
+  if (mi != -1) {
+    p.conf[pix] = costs[mi];
+    p.depth[pix] = hyp[mi][3];
+    p.normal[pix] = hyp[mi][0]; p.normal[WH + pix] = hyp[mi][1]; p.normal[2 * WH + pix] = hyp[mi][2];
+    for (int v = 0; v < N; ++v) p.cost[(size_t)v * WH + pix] = M[mi][v];
+  }
+}
+
+template <int R, int S, int NB>
+__global__ void __launch_bounds__(kThreads) LocalOptKernelL(const Batch b, int colour) {
+  extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  __shared__ uint64_t mbar;
+  int job, blk, iter;
+  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  const JobParams& p = sp;
+  // Iterations > 2 only (patch_match_cuda.cu:861-880); block-uniform.
+  if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
+  const uint64_t skey = StageKey(p.seed, StageLocal(iter, colour));
+  const int kBX = b.block_x, kBY = kThreads / b.block_x;
+  const int tw = RefTileW(kBX, R), th = kBY + 2 * R;
+  float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
+  float* poses = tile + tw * th;
+  const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, &mbar)) return;  // block-uniform
+  __syncthreads();
+  const int tx = threadIdx.x % kBX, ty = threadIdx.x / kBX;
+  const int row = row0 + ty;
+  const int col = col0 + 2 * tx + ((row + colour) & 1);
+  if (col >= p.W || row >= p.H) return;
+  const int W = p.W, H = p.H, N = p.N;
+  const size_t WH = (size_t)W * H;
+  const size_t pix = (size_t)row * W + col;
+  const unsigned gmask = GroupMask<1>();
+  Rng r(skey, (uint32_t)pix);
+  float conf = p.conf[pix];
+  float depth = p.depth[pix];
+  float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
+  const uint32_t sel = p.view_sel[pix];
+  const float a1 = (float)(4.0 * 0.0174532925199432), a2 = (float)(2.0 * 0.0174532925199432);
+  const float* iK = p.refiK;
+  const float np[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
+  float m[3] = {normal[0], normal[1], normal[2]};
+  float lo = depth, hi = depth;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int u = kNeighborOffs[i][1] + col, v = kNeighborOffs[i][0] + row;
+    if (u < 0 || u >= W || v < 0 || v >= H) continue;
+    const size_t q = (size_t)v * W + u;
+    const float nd = p.depth[q];
+    m[0] += p.normal[q]; m[1] += p.normal[WH + q]; m[2] += p.normal[2 * WH + q];
+    if (nd <= lo) lo = nd;
+    if (nd > hi) hi = nd;
+  }
+  const float inv_norm = rsqrtf(m[0] * m[0] + m[1] * m[1] + m[2] * m[2]);
+  m[0] *= inv_norm; m[1] *= inv_norm; m[2] *= inv_norm;
+  PixRef pr;
+  pr.center = p.ref[pix];
+  pr.rsum = p.ref_sum[pix];
+  pr.rvar = p.ref_sqsum[pix] - pr.rsum * pr.rsum;
+  pr.ws = tw;
+  pr.win = tile + ty * tw + (col - col0) + RefTileShift(R);
+  float M[5][NB];
+  float hyp[5][4];
+  int mi = -1;
+  // Rounds 0..4 score five random hypotheses on the selected views; round 5
+  // rescores the winner on the unselected views. One call site of the cost code.
+  for (int it = 0; it < 6; ++it) {
+    float hcur[4];
+    if (it < 5) {
+      hyp[it][3] = r.Uniform() * (hi - lo) + lo;
+      PerturbNormalACMH(m, hyp[it], a1, a2, r);
+      hcur[0] = hyp[it][0]; hcur[1] = hyp[it][1]; hcur[2] = hyp[it][2]; hcur[3] = hyp[it][3];
+    } else {
+      if (mi == -1) break;
+      hcur[0] = normal[0]; hcur[1] = normal[1]; hcur[2] = normal[2]; hcur[3] = depth;
+    }
+    // [quirk] :2916-2919 passes the inverse intrinsics where K is expected when
+    // rescoring the unselected views.
+    const float* Kg = (it < 5) ? p.refK : p.refiK;
+    float mconf = 0.f, mw = 0.f;
+    for (int v = 0; v < N; ++v) {
+      const bool selected = (sel >> v) & 1u;
+      if (selected != (it < 5)) continue;
+      const float cost = ViewCost<R, S, 1>(p, poses, v, row, col, hcur[3], hcur, np, pr, Kg, 0, gmask);
+      if (it < 5) {
+        M[it][v] = cost;
+        mconf += cost;
+        mw += 1.f;
+      } else {
+        p.cost[(size_t)v * WH + pix] = cost;
+      }
+    }
+    if (it == 5) break;
+    if (mw <= 0.f) return;
+    mconf /= mw;
+    if (mconf < conf) {
+      conf = mconf;
+      depth = hyp[it][3];
+      normal[0] = hyp[it][0]; normal[1] = hyp[it][1]; normal[2] = hyp[it][2];
+      mi = it;
+    }
+  }
+  if (mi != -1) {
+    p.conf[pix] = conf;
+    p.depth[pix] = depth;
+    p.normal[pix] = normal[0]; p.normal[WH + pix] = normal[1]; p.normal[2 * WH + pix] = normal[2];
+    for (int v = 0; v < N; ++v)
+      if ((sel >> v) & 1u) p.cost[(size_t)v * WH + pix] = M[mi][v];
+  }
+}
+
 // Blocks per SM the register allocation must allow: shared memory holds one
 // block per SM at G = 1 (10 views), two at G = 2 and three at G = 4.
 template <int G>
@@ -723,9 +1048,25 @@ cudaError_t LaunchSweepT(const Batch& b, int colour, bool local, cudaStream_t st
   return cudaGetLastError();
 }
 
+template <int R, int S, int NB>
+cudaError_t LaunchSweepL(const Batch& b, int colour, bool local, cudaStream_t stream) {
+  if (b.total_blocks <= 0) return cudaSuccess;
+  const size_t smem = SweepKernelSmem(R, b.NB, b.block_x, 1);
+  if (local)
+    LocalOptKernelL<R, S, NB><<<b.total_blocks, kThreads, smem, stream>>>(b, colour);
+  else
+    SweepKernelL<R, S, NB><<<b.total_blocks, kThreads, smem, stream>>>(b, colour);
+  return cudaGetLastError();
+}
+
 template <int R, int S>
 cudaError_t LaunchSweepG(const Batch& b, int colour, bool local, cudaStream_t stream) {
-  if (b.tpp == 1) return LaunchSweepT<R, S, 1>(b, colour, local, stream);
+  if (b.tpp == 1) {
+    if (b.NB <= 8) return LaunchSweepL<R, S, 8>(b, colour, local, stream);
+    if (b.NB <= 12) return LaunchSweepL<R, S, 12>(b, colour, local, stream);
+    if (b.NB <= 16) return LaunchSweepL<R, S, 16>(b, colour, local, stream);
+    return LaunchSweepL<R, S, SMVS_MAX_SRC>(b, colour, local, stream);
+  }
   if (b.tpp == 2) return LaunchSweepT<R, S, 2>(b, colour, local, stream);
   if (b.tpp == 4) return LaunchSweepT<R, S, 4>(b, colour, local, stream);
   return cudaErrorInvalidValue;
@@ -758,10 +1099,8 @@ template <int R, int S>
 cudaError_t ConfigureWindow() {
   cudaError_t e = cudaSuccess;
   if (e == cudaSuccess) e = AllowLargeSmem(InitConfKernel<R, S>);
-  if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 1>);
   if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 2>);
   if (e == cudaSuccess) e = AllowLargeSmem(SweepKernel<R, S, 4>);
-  if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 1>);
   if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 2>);
   if (e == cudaSuccess) e = AllowLargeSmem(LocalOptKernel<R, S, 4>);
   return e;

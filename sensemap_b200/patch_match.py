@@ -285,7 +285,7 @@ class PatchMatchACMMCuda:
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_launch_count(self._h))
 
-    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 2) -> None:
+    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 1) -> None:
         t = N.smvs_tuning(sweep_block_x=sweep_block_x, ref_tile_tma=int(ref_tile_tma),
                           threads_per_pixel=int(threads_per_pixel))
         N.check(N.lib().smvs_set_tuning(self._h, C.byref(t)))

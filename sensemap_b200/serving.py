@@ -28,9 +28,11 @@ def poisson_arrivals(rate_per_s: float, count: int, seed: int = 0) -> np.ndarray
     return np.cumsum(rng.exponential(1.0 / rate_per_s, size=count))
 
 
-def serve(pool, specs, arrivals, on_done=None, time_fn=time.perf_counter) -> dict:
+def serve(pool, specs, arrivals, on_done=None, time_fn=time.perf_counter, before_submit=None) -> dict:
     """Run `specs[i]` arriving at `arrivals[i]` seconds; returns latency stats.
-    `on_done(i, job_id)` is called for each finished job (e.g. to read maps)."""
+    `on_done(i, job_id)` is called for each finished job (e.g. to read maps);
+    `before_submit(spec)` before a job is submitted (e.g. to make its views
+    resident)."""
     t0 = time_fn()
     pending = 0
     i = 0
@@ -41,6 +43,8 @@ def serve(pool, specs, arrivals, on_done=None, time_fn=time.perf_counter) -> dic
         now = time_fn() - t0
         while i < len(specs) and arrivals[i] <= now:
             s = specs[i]
+            if before_submit is not None:
+                before_submit(s)
             live[pool.submit(s.options, s.ref_view, s.src_views)] = i
             i += 1
         if not live:

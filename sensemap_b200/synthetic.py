@@ -533,3 +533,190 @@ def fusion_inputs(scene: Scene, seed: int = 0, rel_noise: float = 0.002, outlier
         order = [int(i) for i in np.argsort(dist, kind="stable") if i != k]
         overlaps.append(order)
     return images, overlaps
+
+
+# ---------------------------------------------------------------------------
+# Aerial scene: terrain heightfield with box buildings (GPU ray-caster)
+# ---------------------------------------------------------------------------
+@dataclass
+class DeviceView:
+    """A view whose image and ground truth stay on the GPU (large view sets)."""
+    image: torch.Tensor        # H x W float32 on the device, integer grey 0..255
+    K: np.ndarray
+    R: np.ndarray
+    T: np.ndarray
+    depth_gt: torch.Tensor     # H x W float32 on the device
+    normal_gt: object = None   # 3 x H x W float32 on the device, or None
+    kind: str = "nadir"
+
+    @property
+    def centre(self) -> np.ndarray:
+        return -np.asarray(self.R, np.float64).T @ np.asarray(self.T, np.float64)
+
+    @property
+    def axis(self) -> np.ndarray:
+        return np.asarray(self.R, np.float64)[2]
+
+
+@dataclass
+class AerialTerrain:
+    hills: np.ndarray          # k x 4 float32: centre x, centre y, amplitude, sigma (m)
+    boxes: np.ndarray          # m x 5 float32: x0, y0, x1, y1, roof height (m)
+    salt: int
+    texel: float               # albedo lattice spacing (m)
+    step: float = 0.25         # ray-march step (m)
+    max_dist: float = 400.0    # rays end this far from the camera (m)
+
+
+def aerial_terrain(seed: int = 0, extent=(600.0, 500.0), num_hills: int = 24, num_boxes: int = 260,
+                   texel: float = 0.15, max_height: float = 20.0) -> AerialTerrain:
+    """Seeded terrain (a sum of Gaussian hills 30..120 m wide, scaled so that
+    the highest point over the extent is `max_height` m) centred on the origin,
+    with box buildings (footprints 8..30 m, 5..40 m tall above the terrain at
+    their centre, not overlapping)."""
+    gen = np.random.default_rng(seed)
+    ex, ey = extent
+    hills = np.stack([gen.uniform(-ex / 2, ex / 2, num_hills), gen.uniform(-ey / 2, ey / 2, num_hills),
+                      gen.uniform(2.0, 15.0, num_hills), gen.uniform(30.0, 120.0, num_hills)], 1)
+    gx, gy = np.meshgrid(np.linspace(-ex / 2, ex / 2, 121), np.linspace(-ey / 2, ey / 2, 101))
+    peak = np.max(np.sum(hills[:, 2, None, None] * np.exp(-((gx[None] - hills[:, 0, None, None]) ** 2 +
+                                                            (gy[None] - hills[:, 1, None, None]) ** 2)
+                                                          / (2 * hills[:, 3, None, None] ** 2)), 0))
+    hills[:, 2] *= max_height / max(peak, 1e-6)
+
+    def terrain(x, y):
+        return float(np.sum(hills[:, 2] * np.exp(-((x - hills[:, 0]) ** 2 + (y - hills[:, 1]) ** 2)
+                                                  / (2 * hills[:, 3] ** 2))))
+
+    boxes = []
+    tries = 0
+    while len(boxes) < num_boxes and tries < 50 * num_boxes:
+        tries += 1
+        w, h = gen.uniform(8.0, 30.0, 2)
+        cx, cy = gen.uniform(-ex / 2 + w, ex / 2 - w), gen.uniform(-ey / 2 + h, ey / 2 - h)
+        b = (cx - w / 2, cy - h / 2, cx + w / 2, cy + h / 2)
+        if any(b[0] < o[2] + 2 and o[0] < b[2] + 2 and b[1] < o[3] + 2 and o[1] < b[3] + 2 for o in boxes):
+            continue
+        boxes.append((*b, terrain(cx, cy) + gen.uniform(5.0, 40.0)))
+    return AerialTerrain(hills.astype(np.float32), np.array(boxes, np.float32).reshape(-1, 5),
+                         int(gen.integers(1, 1 << 30)), texel)
+
+
+def nadir_rotation() -> np.ndarray:
+    """World-to-camera rotation of a camera looking straight down (image x along
+    world x, image y along world -y)."""
+    return np.array([[1.0, 0.0, 0.0], [0.0, -1.0, 0.0], [0.0, 0.0, -1.0]])
+
+
+def render_aerial(terrain: AerialTerrain, K, R, T, width: int, height: int, stream=None):
+    """(albedo in [0, 1], depth, normal) of one view as device tensors."""
+    from . import _native as N
+    import ctypes as C
+    dev = torch.device("cuda")
+    albedo = torch.empty((height, width), dtype=torch.float32, device=dev)
+    depth = torch.empty_like(albedo)
+    normal = torch.empty((3, height, width), dtype=torch.float32, device=dev)
+    Kd = (C.c_double * 9)(*np.asarray(K, np.float64).reshape(9))
+    Rd = (C.c_double * 9)(*np.asarray(R, np.float64).reshape(9))
+    Td = (C.c_double * 3)(*np.asarray(T, np.float64).reshape(3))
+    hills = np.ascontiguousarray(terrain.hills, np.float32)
+    boxes = np.ascontiguousarray(terrain.boxes, np.float32)
+    N.check(N.lib().smvs_synth_render_aerial(
+        hills.ctypes.data, len(hills), boxes.ctypes.data if len(boxes) else None, len(boxes), terrain.salt,
+        float(terrain.texel), float(terrain.step), float(terrain.max_dist), Kd, Rd, Td, width, height, albedo.data_ptr(), depth.data_ptr(), normal.data_ptr(),
+        C.c_void_p(int(stream)) if stream is not None else None))
+    return albedo, depth, normal
+
+
+def _finish_image_device(albedo: torch.Tensor, gen: np.random.Generator, gain_range, noise_sigma) -> torch.Tensor:
+    g = albedo * 255.0
+    if gain_range is not None:
+        g = g * float(gen.uniform(*gain_range))
+    if noise_sigma:
+        t = torch.Generator(device=g.device)
+        t.manual_seed(int(gen.integers(0, 1 << 62)))
+        g = g + noise_sigma * torch.randn(g.shape, generator=t, device=g.device, dtype=g.dtype)
+    return torch.clamp(torch.round(g), 0, 255)
+
+
+def aerial_grid_cameras(stations=(20, 20), altitude: float = 100.0, width: int = 2000, height: int = 1500,
+                        focal: float = 2000.0, overlap: float = 0.8, tilt_deg: float = 45.0):
+    """An aerial survey: a grid of stations at `altitude` spaced for `overlap`
+    between neighbouring nadir footprints; at each station the camera is nadir
+    or tilted by `tilt_deg` towards +x, +y, -x or -y, cycling over the five
+    kinds. Returns [(K, R, T, kind)]."""
+    K = intrinsics(focal, width, height)
+    fx = width * altitude / focal
+    fy = height * altitude / focal
+    sx, sy = (1 - overlap) * fx, (1 - overlap) * fy
+    nx, ny = stations
+    cams = []
+    kinds = ["nadir", "+x", "+y", "-x", "-y"]
+    t = math.radians(tilt_deg)
+    for j in range(ny):
+        for i in range(nx):
+            pos = np.array([(i - (nx - 1) / 2) * sx, (j - (ny - 1) / 2) * sy, altitude])
+            kind = kinds[(i + 2 * j) % 5]
+            if kind == "nadir":
+                R = nadir_rotation()
+            else:
+                a = {"+x": 0.0, "+y": math.pi / 2, "-x": math.pi, "-y": -math.pi / 2}[kind]
+                fwd = np.array([math.cos(a) * math.sin(t), math.sin(a) * math.sin(t), -math.cos(t)])
+                R, _ = look_at(pos, pos + fwd)
+            cams.append((K.copy(), R, -R @ pos, kind))
+    return cams
+
+
+def aerial_views(terrain: AerialTerrain, cams, seed: int = 0, gain_range=(0.8, 1.2), noise_sigma: float = 2.0,
+                 normals: bool = False, stream=None) -> list:
+    """Render cameras [(K, R, T, kind)] into DeviceViews."""
+    gen = np.random.default_rng(seed)
+    out = []
+    for K, R, T, kind in cams:
+        H_, W_ = int(round(2 * K[1, 2] + 1)), int(round(2 * K[0, 2] + 1))
+        albedo, depth, normal = render_aerial(terrain, K, R, T, W_, H_, stream)
+        img = _finish_image_device(albedo, gen, gain_range, noise_sigma)
+        del albedo
+        out.append(DeviceView(img, K, R, T, depth, normal if normals else None, kind))
+    return out
+
+
+def nearest_sources(views, ref: int, k: int, max_angle_deg: float = 50.0) -> list:
+    """The k cameras nearest to view `ref` (camera centres) among those whose
+    viewing directions are within max_angle_deg of its own."""
+    c0, a0 = views[ref].centre, views[ref].axis
+    cos_lim = math.cos(math.radians(max_angle_deg))
+    cand = [i for i in range(len(views)) if i != ref and float(views[i].axis @ a0) >= cos_lim]
+    cand.sort(key=lambda i: (float(np.linalg.norm(views[i].centre - c0)), i))
+    return cand[:k]
+
+
+def depth_range_of(view: DeviceView) -> tuple:
+    d = view.depth_gt
+    valid = d[d > 0]
+    return float(valid.min()) * 0.9, float(valid.max()) * 1.1
+
+
+def ring_terrain(seed: int = 0) -> AerialTerrain:
+    """The heightfield of ``heightfield_scene`` (20 seeded Gaussians over a
+    plane, extent 6 m) as a terrain for the GPU ray-caster, no buildings."""
+    gen = np.random.default_rng(seed)
+    cx, cy, amp, sig = _gaussians(gen)
+    hills = np.stack([cx, cy, amp, sig], 1).astype(np.float32)
+    return AerialTerrain(hills, np.zeros((0, 5), np.float32), int(gen.integers(1, 1 << 30)), 0.06, 0.02, 60.0)
+
+
+def ring_cameras(num_cameras: int = 200, radius: float = 20.0, seed: int = 0):
+    """Cameras on a ring (radius 20 m, heights 2..6 m) looking at the origin,
+    each of one of three sizes (800x600, 1600x1200, 3000x2000; focal 0.75 x
+    width). Returns [(K, R, T, kind)]."""
+    gen = np.random.default_rng(seed + 1)
+    sizes = [(800, 600), (1600, 1200), (3000, 2000)]
+    cams = []
+    for i in range(num_cameras):
+        a = 2 * math.pi * i / num_cameras
+        pos = np.array([radius * math.cos(a), radius * math.sin(a), float(gen.uniform(2.0, 6.0))])
+        w, h = sizes[int(gen.integers(0, len(sizes)))]
+        R, T = look_at(pos, (0.0, 0.0, 0.0))
+        cams.append((intrinsics(0.75 * w, w, h), R, T, f"{w}x{h}"))
+    return cams

@@ -1,0 +1,164 @@
+"""Parity at the benchmark configurations, against both oracles.
+
+Config 1: the planes scene at 640x480, 1 reference + 4 source views (f = 500,
+30-degree arc, 0.3 m baseline), window radius 5 step 1, 6 iterations,
+photometric only, FP32. Config 2: the heightfield scene at 1600x1200 with 10
+source views (gain 0.8-1.2, noise sigma 2), photometric then geometric pass.
+
+The oracles are the reference's own kernels (oracle/_ref, run on this GPU) and
+the CPU transcription of the reference kernel logic. Their random number
+generators differ from the engine's (cuRAND XORWOW vs a counter-based
+generator), so maps are compared statistically:
+* ground-truth accuracy (fraction of pixels within 1 % of the analytic depth)
+  must agree within 0.5 points, the north star's tolerance;
+* the fraction of pixels whose depth is within 1 % and normal within 10 degrees
+  of the oracle's map is stated in each test and must be reached.
+"""
+import numpy as np
+import pytest
+
+import oracle.oracle as orc
+import oracle.ref_oracle as ref
+from sensemap_b200 import STORE_F32
+from sensemap_b200 import synthetic as syn
+from sensemap_b200.patch_match import PatchMatchACMMCuda, PatchMatchOptions, Problem, View
+
+pytestmark = pytest.mark.gpu
+
+GT_GAP = 0.005  # 0.5 points of the within-1 % fraction
+# Agreement with an oracle's map: fraction of pixels within 1 % depth / 10
+# degrees normal. The planes scene of config 1 has large weakly textured areas
+# where both solvers settle on different normals of equal cost.
+CFG1_DEPTH_AGREE, CFG1_NORMAL_AGREE = 0.95, 0.80
+CFG2_DEPTH_AGREE, CFG2_NORMAL_AGREE = 0.97, 0.90
+
+
+def _engine(opt, prob):
+    with PatchMatchACMMCuda(opt, prob) as pm:
+        pm.Run()
+        return {"depth": pm.GetDepthMap(), "normal": pm.GetNormalMap()}
+
+
+def _agreement(a, b, mask):
+    """Fractions of `mask` pixels with depth within 1 % and normal within 10 degrees of b."""
+    d = float(np.mean(np.abs(a["depth"][mask] - b["depth"][mask]) <= 0.01 * np.abs(b["depth"][mask])))
+    nb = b["normal"] / np.maximum(np.linalg.norm(b["normal"], axis=0, keepdims=True), 1e-12)
+    n = syn.normal_accuracy(a["normal"], nb, 10.0, mask=mask)
+    return d, n
+
+
+def _opts(scene, geometric=False, seed=0, **kw):
+    o = PatchMatchOptions(depth_min=scene.depth_min, depth_max=scene.depth_max, window_radius=5, window_step=1,
+                          sigma_spatial=5, num_iterations=6, geom_consistency=geometric,
+                          init_depth_random=not geometric, geom_consistency_regularizer=0.1,
+                          image_storage=STORE_F32, random_seed=seed)
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def _problem(scene, ref_idx, maps=None):
+    views = [View(v.image, v.K, v.R, v.T, depth=None if maps is None else maps[i][0],
+                  normal=None if maps is None else maps[i][1]) for i, v in enumerate(scene.views)]
+    return Problem(ref_idx, [i for i in range(len(views)) if i != ref_idx], views)
+
+
+@pytest.fixture(scope="module", params=[0, 1])
+def config1(request):
+    return syn.planes_scene(seed=request.param, width=640, height=480, focal=500.0, num_src=4)
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_config1_matches_reference_kernels(config1):
+    sc = config1
+    prob = _problem(sc, sc.ref_index)
+    opt = _opts(sc)
+    poses = orc.run(_opts(sc, num_iterations=0), prob)["poses"]
+    r = ref.run(opt, prob, poses)
+    g = _engine(opt, prob)
+    gt = sc.views[sc.ref_index].depth_gt
+    m = gt > 0
+    acc_g, acc_r = syn.depth_accuracy(g["depth"], gt), syn.depth_accuracy(r["depth"], gt)
+    agree_d, agree_n = _agreement(g, r, m)
+    print(f"config1 vs reference kernels: GT {acc_g:.4f} vs {acc_r:.4f}; agreement depth {agree_d:.4f} "
+          f"normal {agree_n:.4f}")
+    assert abs(acc_g - acc_r) <= GT_GAP
+    assert agree_d >= CFG1_DEPTH_AGREE and agree_n >= CFG1_NORMAL_AGREE
+
+
+def test_config1_matches_cpu_transcription(config1):
+    sc = config1
+    prob = _problem(sc, sc.ref_index)
+    opt = _opts(sc)
+    o = orc.run(opt, prob)
+    g = _engine(opt, prob)
+    gt = sc.views[sc.ref_index].depth_gt
+    m = gt > 0
+    acc_g, acc_o = syn.depth_accuracy(g["depth"], gt), syn.depth_accuracy(o["depth"], gt)
+    agree_d, agree_n = _agreement(g, o, m)
+    print(f"config1 vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
+          f"normal {agree_n:.4f}")
+    assert abs(acc_g - acc_o) <= GT_GAP
+    assert agree_d >= CFG1_DEPTH_AGREE and agree_n >= CFG1_NORMAL_AGREE
+
+
+@pytest.fixture(scope="module")
+def config2():
+    import torch
+    return syn.heightfield_scene(seed=0, width=1600, height=1200, num_src=10,
+                                 device="cuda" if torch.cuda.is_available() else "cpu")
+
+
+@pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
+def test_config2_both_passes_match_reference_kernels(config2):
+    """Photometric maps of every view, then view 0's geometric pass against the
+    others' photometric maps, by the engine and by the reference kernels, each
+    from its own maps."""
+    sc = config2
+    V = len(sc.views)
+    fviews = [orc.FilterView(v.K, v.R, v.T, v.depth_gt, v.normal_gt) for v in sc.views]
+    ours, theirs = [], []
+    for r in range(V):
+        prob = _problem(sc, r)
+        poses = orc.cross_filter_poses(fviews, (r, [i for i in range(V) if i != r]))[2]  # 43-float records
+        ours.append(_engine(_opts(sc, seed=r), prob))
+        res = ref.run(_opts(sc, seed=r), prob, poses)
+        theirs.append({"depth": res["depth"], "normal": res["normal"]})
+        if r == 0:
+            poses0 = poses
+    g = _engine(_opts(sc, True, seed=1000), _problem(sc, 0, [(x["depth"], x["normal"]) for x in ours]))
+    res = ref.run(_opts(sc, True, seed=1000), _problem(sc, 0, [(x["depth"], x["normal"]) for x in theirs]), poses0)
+    gt = sc.views[0].depth_gt
+    m = gt > 0
+    out = {}
+    for name, a, b in (("photometric", ours[0], theirs[0]), ("geometric", g, res)):
+        acc_g, acc_r = syn.depth_accuracy(a["depth"], gt), syn.depth_accuracy(b["depth"], gt)
+        out[name] = (acc_g, acc_r) + _agreement(a, b, m)
+    print("config2 vs reference kernels (GT ours, GT reference, agreement depth, normal):", out)
+    for name, (acc_g, acc_r, agree_d, agree_n) in out.items():
+        assert abs(acc_g - acc_r) <= GT_GAP, name
+        assert agree_d >= CFG2_DEPTH_AGREE and agree_n >= CFG2_NORMAL_AGREE, name
+
+
+def test_config2_photometric_band_matches_cpu_transcription(config2):
+    """The CPU transcription on a 64-row band of view 0 (its sweeps read rows
+    outside the band that it does not update, so only the band's 16 central
+    rows are compared) against the engine's full photometric map."""
+    sc = config2
+    prob = _problem(sc, 0)
+    opt = _opts(sc)
+    Hh = sc.views[0].image.shape[0]
+    r0 = Hh // 2 - 32
+    o = orc.run(opt, prob, rows=(r0, r0 + 64))
+    g = _engine(opt, prob)
+    gt = sc.views[0].depth_gt
+    band = np.zeros_like(gt, dtype=bool)
+    band[r0 + 24:r0 + 40] = True
+    m = band & (gt > 0)
+    acc_g = float(np.mean(np.abs(g["depth"][m] - gt[m]) <= 0.01 * gt[m]))
+    acc_o = float(np.mean(np.abs(o["depth"][m] - gt[m]) <= 0.01 * gt[m]))
+    agree_d, agree_n = _agreement(g, o, m)
+    print(f"config2 band vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
+          f"normal {agree_n:.4f}")
+    assert abs(acc_g - acc_o) <= GT_GAP
+    assert agree_d >= CFG2_DEPTH_AGREE and agree_n >= CFG2_NORMAL_AGREE
