@@ -283,7 +283,9 @@ typedef enum smvs_map_kind {
 int smvs_pool_options_default(smvs_pool_options* opt);
 int smvs_pool_create(const smvs_pool_options* opt, void* stream, smvs_pool** out);
 /* Make a view resident (image only; K/R/T as in smvs_view). Re-adding a
- * resident id only refreshes its LRU position. `memory`: smvs_memory of pixels. */
+ * resident id only refreshes its LRU position. `memory`: smvs_memory of pixels.
+ * Host pixels are copied into a pinned staging slot before the call returns
+ * and converted on the pool's copy stream, overlapping the running step. */
 int smvs_pool_add_view(smvs_pool* pool, int64_t view_id, const smvs_view* view, int memory);
 int smvs_pool_has_view(smvs_pool* pool, int64_t view_id, int* resident);
 /* Resident depth (W*H) and normal (3*W*H, may be NULL) maps of a view: the
@@ -295,8 +297,11 @@ int smvs_pool_set_view_maps(smvs_pool* pool, int64_t view_id, const float* depth
  * pool jobs (rejected with SMVS_EINVAL); use smvs_create for those. */
 int smvs_pool_submit(smvs_pool* pool, const smvs_options* opt, int64_t ref_view, const int64_t* src_views,
                      int num_src, int64_t* job_id);
-/* Admit, advance every active job one iteration, retire finished jobs; waits
- * for the step's GPU work. */
+/* Admit, advance every active job one iteration, retire finished jobs. Does
+ * not wait for the step's GPU work: a job whose last iteration has been
+ * enqueued is done once the GPU has run it (smvs_pool_job_state polls; the map
+ * getters wait), and the host stays at most two steps ahead of the GPU. A CUDA
+ * error pending on the calling thread from earlier work is cleared first. */
 int smvs_pool_step(smvs_pool* pool, smvs_pool_stats* stats);
 /* smvs_job_state; latency_s (may be NULL) = completion - submission for done jobs, else -1. */
 int smvs_pool_job_state(smvs_pool* pool, int64_t job_id, int* state, double* latency_s);
