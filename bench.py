@@ -42,9 +42,9 @@ FLOP_PER_TAP = 25           # incremental warp, 1/z, bilinear, 4 moment updates
 METRIC = "depth maps/s (1.6MP,10 src)"
 CPU_BAND_ROWS = 16         # rows of the CPU oracle's band sample (both passes)
 # DRAM bytes (read + write) of one sweep launch of the bench workload per source
-# storage, from ncu (dram__bytes_read.sum + dram__bytes_write.sum); None until
-# captured for the current kernels.
-SWEEP_DRAM_BYTES: dict = {}
+# storage, from ncu (dram__bytes_read.sum + dram__bytes_write.sum of one
+# SweepKernelL<5,1,12> launch, profiles/sweep_kernel_1600x1200_n10_f16.md).
+SWEEP_DRAM_BYTES: dict = {"f16": 0.548e9 + 0.587e9}
 
 
 def log(*a):
@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--serving-jobs", type=int, default=200, help="jobs per rate of --workload serving")
     ap.add_argument("--single", action="store_true",
                     help="profiling mode: run one photometric pass of view 0 per step (for ncu captures)")
+    ap.add_argument("--single-step", type=int, default=STEP,
+                    help="window step of the --single profiling pass (1 = the plain path's, 2 = the autotuned one)")
     ap.add_argument("--workload", default="patchmatch",
                     choices=["patchmatch", "cross-filter", "fusion", "large", "batched", "serving"],
                     help="patchmatch: the depth-map stage (default); cross-filter: CrossFilterCuda::Run + "
@@ -823,7 +825,7 @@ def run_single(args, wl, sptr):
     import torch
     from sensemap_b200.patch_match import PatchMatchACMMCuda
     views = wl.views(wl.dev)
-    opt = make_options(wl.scene, wl.storage, False)
+    opt = make_options(wl.scene, wl.storage, False, step=args.single_step)
     for i in range(args.warmup + args.steps):
         with PatchMatchACMMCuda(opt, wl.problem(0, views), stream=sptr) as pm:
             pm.Run()

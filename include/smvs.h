@@ -101,8 +101,21 @@ typedef struct smvs_options {
   int conf_filter;                         /* :234 */
   float depth_diff_threshold;              /* :231 */
   float conf_threshold;                    /* :237 */
-  int has_prior_depth;                     /* :250 — prior paths not built: must be 0 */
-  int propagate_depth;                     /* :288 — prior paths not built: must be 0 */
+  int has_prior_depth;                     /* :250 — the reference view's given depth and
+                                              normal maps (ref.depth, ref.normal) are a prior:
+                                              costs are weighted by agreement with it
+                                              (ComputeNCCWeightFromPrior, kernel_functions.cu:316-340),
+                                              the first argmin of a sweep keeps to a band
+                                              around it (:2431-2442) and local optimisation
+                                              is off (patch_match_cuda.cu:861) */
+  int propagate_depth;                     /* :288 — with init_depth_random == 0: pixels without a
+                                              given depth start from the source views' depth maps
+                                              projected into the reference view (src[i].depth; a
+                                              source without one is skipped), the median of
+                                              consistent projections becomes a prior depth, and
+                                              normals are fitted to the result
+                                              (patch_match_cuda.cu:603-659); excludes
+                                              has_prior_depth and geom_consistency */
   /* ---- fields with no counterpart in the reference ---- */
   uint64_t random_seed;  /* seed of the counter-based RNG (replaces cuRAND XORWOW,
                             gpu_mat_prng.cu:10-37); results are a pure function of
@@ -140,7 +153,11 @@ typedef struct smvs_problem {
   int num_src;           /* 1..SMVS_MAX_SRC */
   const uint8_t* ref_mask; /* optional W*H mask; depth is zeroed where 0
                               (MaskDepthMapKernel, kernel_functions.cu:3080-3093) */
-  int memory;            /* smvs_memory of pixels/depth/normal/ref_mask */
+  int memory;            /* smvs_memory of pixels/depth/normal/ref_mask/ref_prior_wgt */
+  const float* ref_prior_wgt; /* optional W*H prior weights of the reference view
+                              (Problem::prior_wgt_maps, patch_match_options.h:333; read
+                              by has_prior_depth, InitPriorDepthAndNormalInfo
+                              patch_match_cuda.cu:715-746); NULL = all 0 */
 } smvs_problem;
 
 typedef struct smvs_engine smvs_engine;
@@ -451,6 +468,18 @@ int smvs_cross_filter_release_cache(int gpu_index);
  * lands in a 7x7 window at its truncated pixel, nearest depth kept, normal 0. */
 int smvs_init_depth_from_sparse_points(const smvs_view* view, const float* xyz, size_t num_points, int memory,
                                        float* depth, float* normal, float* depth_range, void* stream);
+/* InitDepthMap with init_from_delaunay (:1205-1307, :1290-1291) +
+ * InitDepthMapFromDelaunay (:398-474): the same sparse points, each at its
+ * truncated pixel (a repeated pixel keeps its first point, as CGAL keeps the
+ * first vertex at a position), are triangulated (2-D Delaunay over the pixel
+ * positions, on the host) and every triangle's plane through its three
+ * back-projected points is written to the pixels inside it: depth and the
+ * camera-frame unit normal. A pixel on an edge shared by two triangles takes
+ * the triangle with the largest vertex indices (the reference takes the later
+ * face in CGAL's face order); on four co-circular points the triangulation's
+ * diagonal may differ from CGAL's. At most 2^21 - 1 points. */
+int smvs_init_depth_from_delaunay(const smvs_view* view, const float* xyz, size_t num_points, int memory,
+                                  float* depth, float* normal, float* depth_range, void* stream);
 /* Model2Depth (:520-642): TriangleMesh vertices_ (n x 3 double), faces_
  * (m x 3 int32) and face_normals_ (m x 3 double), rasterised with back-face
  * and field-of-view culling; normals are the camera-frame face normals. */
@@ -590,6 +619,24 @@ int smvs_fusion_get_points(smvs_fusion* f, smvs_fused_point* points, uint64_t* v
 /* Device addresses of the same arrays (valid until destroy). */
 int smvs_fusion_get_device_points(smvs_fusion* f, const smvs_fused_point** points, const uint64_t** vis_offsets,
                                   const uint32_t** vis_images);
+/* StereoFusion::RemoveDuplicatePoints (fusion.cc:2184-2266; Run calls it after
+ * the image loop when Options::remove_duplicate_pnts, the default, fusion.cc:
+ * 1271-1274): in fusion order each point claims the pixel it projects to in each
+ * of its images; a point that meets an occupant seen by more images is dropped
+ * (and visits no further image), otherwise it takes the pixel and the occupant
+ * is dropped. A point's images are visited in ascending order (the reference
+ * iterates its std::unordered_set). The cloud is compacted in place (order kept);
+ * *num_removed (may be NULL) receives the number of points dropped. */
+int smvs_fusion_remove_duplicate_points(smvs_fusion* f, size_t* num_removed);
+/* StereoFusion::RemoveOutliers (fusion.cc:2542-2611; Run calls it when
+ * Options::outlier_removal, off by default, :1277-1279) with the spacing of
+ * ComputeAverageDistance (patch_match_controller.cc:115-228): each point's mean
+ * distance to its nb_neighbors nearest points (exact k-nearest neighbours on the
+ * GPU) is blended into its score as score * 0.6 + spacing / (max_spacing_factor *
+ * mean spacing) * 0.4, the scores are histogrammed over 256 bins between their
+ * minimum and maximum, and points in a bin holding under 1 % of the cloud whose
+ * cumulative share is at least 90 % are dropped. Scores are updated in place. */
+int smvs_fusion_remove_outliers(smvs_fusion* f, int nb_neighbors, double max_spacing_factor, size_t* num_removed);
 /* The images in the order they were fused (count <= num_views). */
 int smvs_fusion_get_image_order(smvs_fusion* f, int* order, int* count);
 /* fused_pixel_masks_ of a view after run: W*H bytes, 1 = fused. */

@@ -54,6 +54,18 @@ int smvs_test_fusion_waits(double limit_seconds, long long withhold_seed);
  * smvs_synchronize or getter returns SMVS_ETIMEDOUT. */
 int smvs_test_tile_waits(smvs_engine* eng, int polls, int skip_copy);
 
+/* The propagate-depth initial maps of an engine created with propagate_depth:
+ * the given reference maps with the projected source depths composited in
+ * (depth W*H, normal 3*W*H planar) and the prior depth (W*H), before random
+ * hypotheses fill the pixels still without a depth. Host buffers; synchronous. */
+int smvs_test_propagate_init(smvs_engine* eng, float* depth, float* normal, float* prior);
+
+/* The 2-D Delaunay triangulation the Delaunay initial map uses, on n integer
+ * points xy[2i], xy[2i + 1] (repeated positions after the first are skipped):
+ * *num_tris triangles, their counter-clockwise vertex indices into xy in
+ * tris[3k..3k+2] (up to `capacity` triangles written). Host only. */
+int smvs_test_delaunay(const int32_t* xy, int n, int32_t* tris, int capacity, int* num_tris);
+
 /* Throughput calibration on the current device, used as roofline denominators
  * for this path's bounds: kind 0 = FP32 FMA rate (flop/s, FMA = 2 flop),
  * kind 1 = bilinear texture samples/s from an 8-bit texture with warp-coherent

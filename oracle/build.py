@@ -19,7 +19,8 @@ SOURCES = [(ORACLE_DIR / "smvs_oracle.c", []),
            (ORACLE_DIR / "smvs_oracle_filter.c", ["-ffp-contract=off"]),
            (ORACLE_DIR / "smvs_oracle_init.c", ["-ffp-contract=off"]),
            (ORACLE_DIR / "smvs_oracle_fusion.c", ["-ffp-contract=off"]),
-           (ORACLE_DIR / "smvs_oracle_pyramid.c", ["-ffp-contract=off"])]
+           (ORACLE_DIR / "smvs_oracle_pyramid.c", ["-ffp-contract=off"]),
+           (ORACLE_DIR / "smvs_oracle_prior.c", ["-ffp-contract=off"])]
 DEPS = [src for src, _ in SOURCES] + [ORACLE_DIR / "smvs_oracle.h", ORACLE_DIR / "orc_pose.h",
                                       ORACLE_DIR.parent / "include" / "smvs.h", Path(__file__)]
 CFLAGS = ["-std=c11", "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-Wall", "-Wextra"]

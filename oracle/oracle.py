@@ -71,12 +71,26 @@ def lib():
         h.orc_fusion_copy.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_fusion_mask.restype = C.c_int
         h.orc_fusion_mask.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        h.orc_fusion_duplicate_keep.restype = C.c_int
+        h.orc_fusion_duplicate_keep.argtypes = [C.POINTER(N.smvs_fusion_view), C.c_int, C.c_void_p, C.c_size_t,
+                                                C.c_void_p, C.c_void_p, C.c_void_p]
+        h.orc_fusion_outlier_keep.restype = C.c_int
+        h.orc_fusion_outlier_keep.argtypes = [C.c_void_p, C.c_size_t, C.c_int, C.c_double, C.c_void_p, C.c_void_p,
+                                              C.c_void_p]
         h.orc_fusion_free.restype = None
         h.orc_fusion_free.argtypes = [C.c_void_p]
+        h.orc_delaunay_points.restype = C.c_int
+        h.orc_delaunay_points.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.POINTER(C.c_size_t)]
+        h.orc_init_from_delaunay.restype = C.c_int
+        h.orc_init_from_delaunay.argtypes = [C.POINTER(N.smvs_view), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
+                                             C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_resample_maps.restype = C.c_int
         h.orc_resample_maps.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
         h.orc_rescale_image.restype = C.c_int
         h.orc_rescale_image.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int]
+        h.orc_propagate_init_problem.restype = C.c_int
+        h.orc_propagate_init_problem.argtypes = [C.POINTER(N.smvs_problem), C.c_void_p, C.c_void_p, C.c_void_p]
         h.orc_cross_filter_poses.restype = C.c_int
         h.orc_cross_filter_poses.argtypes = [vp, C.c_int, pp, C.c_void_p, C.c_void_p, C.c_void_p]
         _LIB = h
@@ -123,8 +137,28 @@ def _problem_struct(problem: Problem):
         m = np.ascontiguousarray(problem.mask, dtype=np.uint8)
         keep.append(m)
         prob.ref_mask = m.ctypes.data
+    if problem.prior_wgt is not None:
+        w = np.ascontiguousarray(problem.prior_wgt, dtype=np.float32)
+        keep.append(w)
+        prob.ref_prior_wgt = w.ctypes.data
     prob.memory = N.MEM_HOST
     return prob, keep
+
+
+def propagate_init(problem: Problem) -> dict:
+    """The oracle's propagate-depth initial maps (InitWorkspace,
+    patch_match_cuda.cu:603-659) from the problem's given reference maps and
+    source depth maps: depth, normal (3 x H x W) and prior depth."""
+    prob, keep = _problem_struct(problem)
+    ref = problem.images[problem.ref_image_idx]
+    out = {"depth": np.zeros((ref.height, ref.width), np.float32),
+           "normal": np.zeros((3, ref.height, ref.width), np.float32),
+           "prior": np.zeros((ref.height, ref.width), np.float32)}
+    rc = lib().orc_propagate_init_problem(C.byref(prob), out["depth"].ctypes.data, out["normal"].ctypes.data,
+                                          out["prior"].ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"oracle propagate init failed ({rc})")
+    return out
 
 
 def run(options: PatchMatchOptions, problem: Problem, rows=None) -> dict:
@@ -295,6 +329,33 @@ def init_from_sparse_points(width, height, K, R, T, xyz):
     return d, n, (r[0], r[1])
 
 
+def delaunay_points(width, height, K, R, T, xyz):
+    """The projected points that land in the view (input order): (uv (m, 2)
+    int32 truncated pixel positions, z (m,), input indices (m,))."""
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    uv = np.zeros((max(len(x), 1), 2), np.int32)
+    z = np.zeros(max(len(x), 1), np.float32)
+    idx = np.zeros(max(len(x), 1), np.int32)
+    m = C.c_size_t()
+    if lib().orc_delaunay_points(C.byref(_init_view(width, height, K, R, T)), x.ctypes.data, len(x), uv.ctypes.data,
+                                 z.ctypes.data, idx.ctypes.data, C.byref(m)):
+        raise RuntimeError("orc_delaunay_points failed")
+    return uv[:m.value], z[:m.value], idx[:m.value]
+
+
+def init_from_delaunay(width, height, K, R, T, xyz, tris):
+    """InitDepthMapFromDelaunay over a given triangulation (index triples into
+    the delaunay_points list)."""
+    x = np.ascontiguousarray(xyz, np.float32).reshape(-1, 3)
+    t = np.ascontiguousarray(tris, np.int32).reshape(-1, 3)
+    d, n, r = _init_out(width, height)
+    if lib().orc_init_from_delaunay(C.byref(_init_view(width, height, K, R, T)), x.ctypes.data, len(x),
+                                    t.ctypes.data if len(t) else None, len(t), d.ctypes.data, n.ctypes.data,
+                                    r.ctypes.data):
+        raise RuntimeError("orc_init_from_delaunay failed")
+    return d, n, (r[0], r[1])
+
+
 def init_from_mesh(width, height, K, R, T, vertices, faces, face_normals):
     v = np.ascontiguousarray(vertices, np.float64).reshape(-1, 3)
     f = np.ascontiguousarray(faces, np.int32).reshape(-1, 3)
@@ -350,6 +411,47 @@ def fusion_run(options, images, overlapping_images, max_images: int = 0, masks: 
         return out
     finally:
         lib().orc_fusion_free(h)
+
+
+def _compact(pts, off, vis, keep):
+    keep = keep.astype(bool)
+    counts = np.diff(off.astype(np.int64))
+    new_off = np.zeros(int(keep.sum()) + 1, dtype=np.uint64)
+    new_off[1:] = np.cumsum(counts[keep])
+    vmask = np.repeat(keep, counts)
+    return pts[keep].copy(), new_off, vis[:len(vmask)][vmask].copy()
+
+
+def fusion_remove_duplicates(images, pts, off, vis):
+    """RemoveDuplicatePoints (smvs_oracle_fusion.c) over a fused cloud: the
+    kept (points, offsets, images) and the number dropped."""
+    from sensemap_b200.fusion import fusion_structs
+    views, _, _, _, alive = fusion_structs(images, [[] for _ in images])
+    pts = np.ascontiguousarray(pts)
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    vis = np.ascontiguousarray(vis, dtype=np.uint32)
+    keep = np.zeros(len(pts), dtype=np.uint8)
+    if lib().orc_fusion_duplicate_keep(views, len(images), pts.ctypes.data, len(pts), off.ctypes.data,
+                                       vis.ctypes.data, keep.ctypes.data) != 0:
+        raise ValueError("orc_fusion_duplicate_keep rejected its arguments")
+    return _compact(pts, off, vis, keep) + (int(len(pts) - keep.sum()),)
+
+
+def fusion_remove_outliers(pts, off, vis, nb_neighbors=6, max_spacing_factor=6.0):
+    """RemoveOutliers (smvs_oracle_fusion.c, brute-force neighbours): the kept
+    (points with updated scores, offsets, images), the number dropped and the
+    per-point spacings."""
+    pts = np.ascontiguousarray(pts).copy()
+    scores = np.ascontiguousarray(pts["score"], dtype=np.float32).copy()
+    keep = np.zeros(len(pts), dtype=np.uint8)
+    spacing = np.zeros(len(pts), dtype=np.float32)
+    if lib().orc_fusion_outlier_keep(pts.ctypes.data, len(pts), int(nb_neighbors), float(max_spacing_factor),
+                                     scores.ctypes.data, keep.ctypes.data, spacing.ctypes.data) != 0:
+        raise ValueError("orc_fusion_outlier_keep rejected its arguments")
+    pts["score"] = scores
+    kp, ko, kv = _compact(pts, np.ascontiguousarray(off, dtype=np.uint64), np.ascontiguousarray(vis, dtype=np.uint32),
+                          keep)
+    return kp, ko, kv, int(len(pts) - keep.sum()), spacing
 
 
 def resample_maps(planes: np.ndarray, new_h: int, new_w: int, renormalise: bool) -> np.ndarray:

@@ -7,6 +7,7 @@
 // with textures configured as InitRefImage / InitSourceImages / InitTransforms /
 // Preprocess configure them (patch_match_cuda.cu:110-580, 448-491). The host
 // pose records are supplied by the caller (the 43-float layout of :516-559).
+#include <cfloat>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -39,7 +40,9 @@ struct RefJob {
   float geom_reg, geom_max, rand_depth_ratio, a1, a2, init_mc, max_mc, alpha, beta;
   const float* init_depth;
   const float* init_normal;
-  const float* const* src_depth;
+  const float* const* src_depth;  // per source; an entry may be NULL (propagate_depth: no map)
+  int prior_mode;                 // 0 none, 1 has_prior_depth, 2 propagate_depth
+  const float* prior_wgt;         // W*H or NULL (has_prior_depth)
 };
 
 struct RefOut {
@@ -110,10 +113,11 @@ void SetupTextures(const RefJob& j, Textures& t, bool with_images) {
     t.src_tex = MakeArrayTexture(t.src_dev->GetPtr(), cudaFilterModeLinear, cudaReadModeNormalizedFloat);
   }
   if (j.src_depth) {
-    // InitSourceImages geometric branch, patch_match_cuda.cu:318-367.
+    // InitSourceImages geometric branch, patch_match_cuda.cu:318-367, and the
+    // propagate-depth branch :377-417 (a source without a map stays 0).
     std::vector<float> packed(max_w * max_h * j.N, 0.f);
     for (int i = 0; i < j.N; ++i)
-      for (int r = 0; r < j.src_h[i]; ++r)
+      for (int r = 0; j.src_depth[i] && r < j.src_h[i]; ++r)
         memcpy(packed.data() + max_w * max_h * i + r * max_w, j.src_depth[i] + (size_t)r * j.src_w[i],
                sizeof(float) * j.src_w[i]);
     t.src_depth_dev.reset(new CudaArrayWrapper<float>(max_w, max_h, j.N));
@@ -128,11 +132,60 @@ void SetupTextures(const RefJob& j, Textures& t, bool with_images) {
   t.poses_tex = MakeArrayTexture(t.poses_dev->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
 }
 
+// The propagate-depth initial maps in the reference's order
+// (patch_match_cuda.cu:603-659): GenerateProjectDepthMaps per source with a
+// map, CompositeInitDepthMap, CompositeInitNormalMap. The reference launches
+// them with 32x32 blocks; the driver uses 32x16 (every kernel indexes pixels
+// from blockDim and the projections combine by atomicMin, so results do not
+// depend on the block shape) and checks every launch.
+// The reference starts the projections from composite_depth_map.FillWithScalar
+// (FLT_MAX), a byte cudaMemset of the float converted to int (gpu_mat.h:240-243):
+// its fill byte is 0xff (every float NaN, which the atomicMin and the
+// (0, FLT_MAX) test treat like FLT_MAX) when the host compiler folds the
+// conversion, and 0x00 (no projection is ever stored, the mode does nothing)
+// when it converts at run time. The driver fills FLT_MAX itself: the intended
+// result.
+int PropagateInit(const RefJob& j, const Textures& t, GpuMatPRNG& rand_state, GpuMat<float>& depth_map,
+                  GpuMat<float>& normal_map, GpuMat<float>& prior_depth) {
+  size_t max_w = 0, max_h = 0;
+  for (int i = 0; i < j.N; ++i) {
+    max_w = std::max<size_t>(max_w, j.src_w[i]);
+    max_h = std::max<size_t>(max_h, j.src_h[i]);
+  }
+  const dim3 b(THREADS_PER_BLOCK, THREADS_PER_BLOCK / 2);
+  GpuMat<float> composite(j.W, j.H, j.N);
+  {
+    std::vector<float> init((size_t)j.W * j.H * j.N, FLT_MAX);
+    composite.CopyToDevice(init.data(), j.W * sizeof(float));
+  }
+  for (int i = 0; i < j.N; ++i) {
+    if (!j.src_depth || !j.src_depth[i]) continue;
+    const dim3 g((max_w - 1) / b.x + 1, (max_h - 1) / b.y + 1);
+    GenerateProjectDepthMaps<<<g, b>>>(max_w, max_h, i, j.N, composite, t.src_depth_tex, t.poses_tex, 0);
+    if (cudaGetLastError() != cudaSuccess) return 20;
+  }
+  CUDA_SYNC_AND_CHECK();
+  prior_depth.FillWithScalar(0);
+  const dim3 g((j.W - 1) / b.x + 1, (j.H - 1) / b.y + 1);
+  CompositeInitDepthMap<<<g, b>>>(rand_state, depth_map, prior_depth, composite, j.depth_min, j.depth_max);
+  if (cudaGetLastError() != cudaSuccess) return 21;
+  CUDA_SYNC_AND_CHECK();
+  CompositeInitNormalMap<<<g, b>>>(depth_map, normal_map, 0);
+  if (cudaGetLastError() != cudaSuccess) return 22;
+  CUDA_SYNC_AND_CHECK();
+  return 0;
+}
+
 }  // namespace
 
 extern "C" int ref_run(const RefJob* jp, RefOut* out) {
   const RefJob& j = *jp;
   if (j.N > MAX_NUM_SRC_IMAGE) return 1;
+  // The reference's sweep with a prior (prior_depth_ncc) reads hypotheses[-1]
+  // and M[-1] when FindMinCostWithin finds no hypothesis in the prior's band
+  // (kernel_functions.cu:2431-2446, 2488-2493), before its local arrays; a test
+  // process ended inside that run. Only the cost level (no iterations) is run.
+  if (j.prior_mode == 1 && j.num_iterations > 0) return 31;
   Textures t;
   SetupTextures(j, t, true);
   const int W = j.W, H = j.H;
@@ -140,7 +193,24 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
   // InitWorkspace, patch_match_cuda.cu:582-698.
   GpuMatPRNG rand_state(W, H);
   GpuMat<float> conf_map(W, H), depth_map(W, H), normal_map(W, H, 3);
-  GpuMat<float> prior_depth(0, 0, 0), prior_normal(0, 0, 0), prior_wgt(0, 0, 0);
+  // Prior maps: InitPriorDepthAndNormalInfo (patch_match_cuda.cu:715-746) for
+  // has_prior_depth; for propagate_depth the reference's sweep reads normal and
+  // weight maps that stay 0 x 0 (:588-591), which the driver replaces by zero
+  // maps of the image's size (the reading this library defines).
+  const bool prior = j.prior_mode != 0;
+  GpuMat<float> prior_depth(prior ? W : 0, prior ? H : 0, prior ? 1 : 0);
+  GpuMat<float> prior_normal(prior ? W : 0, prior ? H : 0, prior ? 3 : 0);
+  GpuMat<float> prior_wgt(prior ? W : 0, prior ? H : 0, prior ? 1 : 0);
+  if (j.prior_mode == 1) {
+    if (!j.init_depth || !j.init_normal) return 30;
+    prior_depth.CopyToDevice(j.init_depth, W * sizeof(float));
+    prior_normal.CopyToDevice(j.init_normal, W * sizeof(float));
+    if (j.prior_wgt) prior_wgt.CopyToDevice(j.prior_wgt, W * sizeof(float));
+    else prior_wgt.FillWithScalar(0);
+  } else if (j.prior_mode == 2) {
+    prior_normal.FillWithScalar(0);
+    prior_wgt.FillWithScalar(0);
+  }
   dim3 eb(THREADS_PER_BLOCK, THREADS_PER_BLOCK), eg((W - 1) / THREADS_PER_BLOCK + 1, (H - 1) / THREADS_PER_BLOCK + 1);
   // The reference launches InitDepthMap / InitNormalMap with 32x32 blocks
   // (patch_match_cuda.cu:93-100, 662-671). On sm_100a they need 96 / 72
@@ -155,6 +225,10 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
   if (!j.init_depth_random) {
     depth_map.CopyToDevice(j.init_depth, W * sizeof(float));
     normal_map.CopyToDevice(j.init_normal, W * sizeof(float));
+    if (j.prior_mode == 2) {
+      const int st = PropagateInit(j, t, rand_state, depth_map, normal_map, prior_depth);
+      if (st) return st;
+    }
     InitDepthMap<<<ig, ib>>>(depth_map, normal_map, rand_state, j.depth_min, j.depth_max, 0);
   } else {
     depth_map.FillWithRandomNumbers(j.depth_min, j.depth_max, rand_state);
@@ -201,8 +275,8 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
   so.num_samples = j.num_samples;
   so.geom_consistency = j.geom != 0;
   so.random_optimization = j.random_opt != 0;
-  so.propagate_depth = false;
-  so.prior_depth_ncc = false;
+  so.propagate_depth = j.prior_mode == 2;
+  so.prior_depth_ncc = j.prior_mode == 1;
 
   const int BW = THREADS_PER_BLOCK, BH = THREADS_PER_BLOCK / 2;
   {  // InitConfMapKernel launch, patch_match_cuda.cu:963-981.
@@ -229,7 +303,7 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
                                           t.sum_tex, t.sqsum_tex, t.src_tex, t.src_depth_tex, t.poses_tex);
       if (cudaGetLastError() != cudaSuccess) return 6;
       CUDA_SYNC_AND_CHECK();
-      if (j.local_opt && iter > 2) {
+      if (j.local_opt && iter > 2 && j.prior_mode != 1) {  // patch_match_cuda.cu:861
         BlackPixelLocalOptimization<<<g, b, shared>>>(rand_state, depth_map, normal_map, conf_map, cost_map, view_sel,
                                                       j.N, so, weight_computer, t.ref_tex, t.sum_tex, t.sqsum_tex,
                                                       t.src_tex, t.src_depth_tex, t.poses_tex);
@@ -247,6 +321,29 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
   if (out->conf) conf_map.CopyToHost(out->conf, W * sizeof(float));
   if (out->cost) cost_map.CopyToHost(out->cost, W * sizeof(float));
   if (out->view_sel) view_sel.CopyToHost(out->view_sel, W * sizeof(uint32_t));
+  CUDA_SYNC_AND_CHECK();
+  return 0;
+}
+
+// The propagate-depth initial maps alone (before InitDepthMap draws random
+// hypotheses for the pixels still without a depth): depth and normal hold the
+// given maps on entry and the composited maps on return; prior receives the
+// consistent medians.
+extern "C" int ref_propagate_init(const RefJob* jp, float* depth, float* normal, float* prior) {
+  const RefJob& j = *jp;
+  if (j.N > MAX_NUM_SRC_IMAGE || !j.src_depth || !j.init_depth || !j.init_normal) return 1;
+  Textures t;
+  SetupTextures(j, t, false);
+  GpuMatPRNG rand_state(j.W, j.H);
+  if (cudaGetLastError() != cudaSuccess) return 2;
+  GpuMat<float> depth_map(j.W, j.H), normal_map(j.W, j.H, 3), prior_depth(j.W, j.H);
+  depth_map.CopyToDevice(j.init_depth, j.W * sizeof(float));
+  normal_map.CopyToDevice(j.init_normal, j.W * sizeof(float));
+  const int st = PropagateInit(j, t, rand_state, depth_map, normal_map, prior_depth);
+  if (st) return st;
+  depth_map.CopyToHost(depth, j.W * sizeof(float));
+  normal_map.CopyToHost(normal, j.W * sizeof(float));
+  prior_depth.CopyToHost(prior, j.W * sizeof(float));
   CUDA_SYNC_AND_CHECK();
   return 0;
 }

@@ -33,7 +33,8 @@ class RefJob(C.Structure):
                 ("geom_reg", C.c_float), ("geom_max", C.c_float), ("rand_depth_ratio", C.c_float),
                 ("a1", C.c_float), ("a2", C.c_float), ("init_mc", C.c_float), ("max_mc", C.c_float),
                 ("alpha", C.c_float), ("beta", C.c_float),
-                ("init_depth", C.c_void_p), ("init_normal", C.c_void_p), ("src_depth", C.POINTER(C.c_void_p))]
+                ("init_depth", C.c_void_p), ("init_normal", C.c_void_p), ("src_depth", C.POINTER(C.c_void_p)),
+                ("prior_mode", C.c_int), ("prior_wgt", C.c_void_p)]
 
 
 class RefOut(C.Structure):
@@ -64,6 +65,8 @@ def lib():
         h.ref_filter.restype = C.c_int
         h.ref_filter.argtypes = [C.POINTER(RefJob), C.c_void_p, C.c_int, C.c_float, C.c_void_p]
         h.ref_max_num_src.restype = C.c_int
+        h.ref_propagate_init.restype = C.c_int
+        h.ref_propagate_init.argtypes = [C.POINTER(RefJob), C.c_void_p, C.c_void_p, C.c_void_p]
         h.ref_cross_filter.restype = C.c_int
         h.ref_cross_filter.argtypes = [C.c_int, C.POINTER(RefCfView), C.c_int, C.POINTER(RefCfProblem), C.c_float,
                                        C.c_float, C.c_float, C.c_int, C.c_void_p]
@@ -122,12 +125,17 @@ def _job(options: PatchMatchOptions, problem: Problem, poses: np.ndarray, keep: 
         n = np.ascontiguousarray(ref.normal, np.float32)
         keep.append(n)
         j.init_normal = n.ctypes.data
-    if all(v.depth is not None for v in srcs):
-        ds = [np.ascontiguousarray(v.depth, np.float32) for v in srcs]
+    if any(v.depth is not None for v in srcs):  # a source without a map is NULL (propagate_depth)
+        ds = [None if v.depth is None else np.ascontiguousarray(v.depth, np.float32) for v in srcs]
         keep.extend(ds)
-        da = (C.c_void_p * len(srcs))(*[a.ctypes.data for a in ds])
+        da = (C.c_void_p * len(srcs))(*[None if a is None else a.ctypes.data for a in ds])
         keep.append(da)
         j.src_depth = C.cast(da, C.POINTER(C.c_void_p))
+    j.prior_mode = 1 if o.has_prior_depth else (2 if o.propagate_depth else 0)
+    if problem.prior_wgt is not None:
+        w = np.ascontiguousarray(problem.prior_wgt, np.float32)
+        keep.append(w)
+        j.prior_wgt = w.ctypes.data
     return j
 
 
@@ -142,6 +150,21 @@ def run(options: PatchMatchOptions, problem: Problem, poses: np.ndarray) -> dict
     rc = lib().ref_run(C.byref(j), C.byref(ro))
     if rc != 0:
         raise RuntimeError(f"reference run failed (driver status {rc})")
+    return out
+
+
+def propagate_init(options: PatchMatchOptions, problem: Problem, poses: np.ndarray) -> dict:
+    """The reference's propagate-depth initial maps (GenerateProjectDepthMaps,
+    CompositeInitDepthMap, CompositeInitNormalMap) from the problem's given
+    reference maps and source depth maps."""
+    keep = []
+    j = _job(options, problem, poses, keep)
+    out = {"depth": np.zeros((j.H, j.W), np.float32), "normal": np.zeros((3, j.H, j.W), np.float32),
+           "prior": np.zeros((j.H, j.W), np.float32)}
+    rc = lib().ref_propagate_init(C.byref(j), out["depth"].ctypes.data, out["normal"].ctypes.data,
+                                  out["prior"].ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"reference propagate init failed (driver status {rc})")
     return out
 
 

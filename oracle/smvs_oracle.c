@@ -153,6 +153,12 @@ typedef struct {
   int sw[SMVS_MAX_SRC], sh[SMVS_MAX_SRC];
   int src_half;                  /* FP16 source storage: filtered values are FP16 */
   float* sdepth[SMVS_MAX_SRC];   /* geometric pass only */
+  /* Prior maps (SweepOptions::prior_depth_ncc / propagate_depth): mode 1 =
+   * has_prior_depth, 2 = propagate_depth; NULL normal/weight maps read as 0. */
+  int prior_mode;
+  const float* prior_depth;
+  const float* prior_normal;
+  const float* prior_wgt;
   /* state */
   float *depth, *normal, *conf, *cost;
   uint32_t* view_sel;
@@ -313,11 +319,48 @@ static float geom_cost(const ctx_t* c, int v, float row, float col, float depth,
   return fminf(c->geom_max, sqrtf(dc * dc + dr * dr));
 }
 
-/* ComputeMultiViewCostVector, kernel_functions.cu:1447-1495 (no prior). */
+/* A pixel's prior: normal xyz, depth w and weight (kernel_functions.cu:
+ * 1533-1543, 2188-2200). */
+typedef struct { float x, y, z, w, wgt; } prior_t;
+
+static prior_t load_prior(const ctx_t* c, size_t pix) {
+  prior_t pi = {0, 0, 0, 0, 0};
+  if (c->prior_mode == 0) return pi;
+  const size_t WH = (size_t)c->W * c->H;
+  pi.w = c->prior_depth[pix];
+  if (c->prior_normal) {
+    pi.x = c->prior_normal[pix]; pi.y = c->prior_normal[WH + pix]; pi.z = c->prior_normal[2 * WH + pix];
+  }
+  if (c->prior_wgt) pi.wgt = c->prior_wgt[pix];
+  return pi;
+}
+
+/* ComputeNCCWeightFromPrior (kernel_functions.cu:316-340) times the
+ * PRIOR_WGT_COST factor (:1470-1478), with the reference's float/double mix;
+ * 1 unless mode 1 and a prior depth above FLT_EPSILON. */
+static float prior_weight(const ctx_t* c, const prior_t* pi, const float h[3], float hd, float rvar) {
+  if (c->prior_mode != 1 || !(pi->w > FLT_EPSILON)) return 1.0f;
+  float regu = 1.0f;
+  const float sigma2 = (float)(0.5 - 0.4 * exp(-10000.0 * (double)fabsf(rvar)));
+  const float dd = hd - pi->w;
+  const float dd2 = fmaxf(dd * dd, 0.05f * 0.05f);
+  regu = (float)((double)regu * fmax(1.0 - 0.2 * (double)expf(-dd2 / sigma2), 0.01));
+  const float pn = pi->x * pi->x + pi->y * pi->y + pi->z * pi->z;
+  if ((double)pn > 0.8 && (double)pn < 1.25) {
+    const float ct = pi->x * h[0] + pi->y * h[1] + pi->z * h[2];
+    const float dt2 = (1.0f - ct) * (1.0f - ct);
+    regu = (float)((double)regu * fmax(1.0 - 0.54 * (double)expf(-dt2 / sigma2), 0.01));
+  }
+  if ((double)pi->wgt < 1.0 && (double)pi->wgt > 0.0) regu = (float)((double)regu * (1.0 - (double)pi->wgt * 0.3));
+  return regu;
+}
+
+/* ComputeMultiViewCostVector, kernel_functions.cu:1447-1495; pw = the prior
+ * factor of the hypothesis (1 without a prior). */
 static void cost_vector(const ctx_t* c, int row, int col, float depth, const float n[3],
-                        const float np[3], const pixref_t* pr, float* out) {
+                        const float np[3], const pixref_t* pr, float* out, float pw) {
   for (int v = 0; v < c->N; ++v) {
-    float cost = ncc_cost(c, v, row, col, depth, n, pr);
+    float cost = ncc_cost(c, v, row, col, depth, n, pr) * pw;
     if (c->geom) cost += c->geom_reg * geom_cost(c, v, (float)row, (float)col, depth, np, c->refK);
     out[v] = cost;
   }
@@ -479,7 +522,7 @@ static void init_workspace(ctx_t* c, int random_init, const float* init_depth, c
     }
 }
 
-/* InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior), over rows
+/* InitConfMapKernel, kernel_functions.cu:1497-1601, over rows
  * [row_begin, row_end). */
 static void init_conf(ctx_t* c, int row_begin, int row_end) {
   const int W = c->W, N = c->N;
@@ -494,7 +537,9 @@ static void init_conf(ctx_t* c, int row_begin, int row_end) {
       const float n[3] = {c->normal[pix], c->normal[WH + pix], c->normal[2 * WH + pix]};
       float costs[SMVS_MAX_SRC];
       int O[SMVS_MAX_SRC];
-      cost_vector(c, row, col, c->depth[pix], n, np, &pr, costs);
+      const prior_t pi = load_prior(c, pix);
+      cost_vector(c, row, col, c->depth[pix], n, np, &pr, costs,
+                  prior_weight(c, &pi, n, c->depth[pix], pr.rvar));
       for (int v = 0; v < N; ++v) { O[v] = v; c->cost[(size_t)v * WH + pix] = costs[v]; }
       /* BubbleSortByValue, utils.h:212-231 */
       for (int i = 0; i < N - 1; ++i)
@@ -513,8 +558,7 @@ static void init_conf(ctx_t* c, int row_begin, int row_end) {
   }
 }
 
-/* SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
- * propagate_depth), for one pixel. */
+/* SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560, for one pixel. */
 static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
   const int W = c->W, H = c->H, N = c->N;
   const size_t WH = (size_t)W * H;
@@ -523,11 +567,13 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
   float depth = c->depth[pix];
   float normal[3] = {c->normal[pix], c->normal[WH + pix], c->normal[2 * WH + pix]};
   const float grad = c->grad[pix];
+  const prior_t pri = load_prior(c, pix);
+  const float prf = (c->prior_mode == 1 && (double)pri.w > 1e-6) ? 0.1f : 1.0f; /* :2201-2203 */
   const float inv_beta2 = 0.5f / (c->beta * c->beta);
   const float depth_min = c->depth_min;
   const float depth_max = (float)(1.2 * (double)c->depth_max); /* [quirk] :2213 */
-  const float a1 = fminf(c->rand_a1, (float)DEG2RAD_D(180.0f));
-  const float a2 = fminf(c->rand_a2, (float)DEG2RAD_D(90.0f));
+  const float a1 = fminf(c->rand_a1 * prf, (float)DEG2RAD_D(180.0f));
+  const float a2 = fminf(c->rand_a2 * prf, (float)DEG2RAD_D(90.0f));
   const float* iK = c->refiK;
   const float vd[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
   const float ivl = 1.0f / sqrtf(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
@@ -571,7 +617,11 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
     for (int s = 0; s < 10; ++s) {
       const int nr = row + kDirSamples[k][2 * s], nc = col + kDirSamples[k][2 * s + 1];
       if (nr < 0 || nr >= H || nc < 0 || nc >= W) continue;
-      const float nconf = c->conf[(size_t)nr * W + nc];
+      float nconf = c->conf[(size_t)nr * W + nc];
+      if (c->prior_mode != 0 && c->prior_wgt) { /* PRIOR_WGT_PROGET :2292-2304 */
+        const float pws = c->prior_wgt[(size_t)nr * W + nc];
+        if ((double)pws > 1e-6) nconf = (float)((double)nconf * (1.0 - 0.2 * (double)pws));
+      }
       if (best > nconf) { br = nr; bc = nc; best = nconf; }
     }
     if (best < FLT_MAX) {
@@ -588,7 +638,8 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
   load_pixref(c, row, col, &pr);
   float M[ORC_MAX_HYP][SMVS_MAX_SRC];
   for (int v = 0; v < N; ++v) M[0][v] = c->cost[(size_t)v * WH + pix];
-  for (int h = 1; h < ns; ++h) cost_vector(c, row, col, hyp[h][3], hyp[h], np, &pr, M[h]);
+  for (int h = 1; h < ns; ++h)
+    cost_vector(c, row, col, hyp[h][3], hyp[h], np, &pr, M[h], prior_weight(c, &pri, hyp[h], hyp[h][3], pr.rvar));
 
   /* ACMM view selection, :2364-2427 */
   uint32_t flags = 0;
@@ -637,7 +688,16 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
     costs[h] = cs;
   }
   c->view_sel[pix] = sel;
-  int mi = find_min_cost(costs, ns);
+  int mi = -1;
+  if (c->prior_mode == 1 && pri.w > 0.0f) { /* FindMinCostWithin :661-671, band :2431-2437 */
+    const float lo = (float)fmin((double)(pri.w * 0.95f) - 0.05, 0.0);
+    const float hi = (float)((double)(pri.w * 1.05f) + 0.05);
+    float m = FLT_MAX;
+    for (int h = 0; h < ns; ++h)
+      if (costs[h] <= m && hyp[h][3] >= lo && hyp[h][3] <= hi) { m = costs[h]; mi = h; }
+  } else {
+    mi = find_min_cost(costs, ns);
+  }
   if (mi < 0) return;
   depth = hyp[mi][3];
   normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
@@ -648,7 +708,8 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
   const float ndepth = rng_uniform(&r) * (pd_max - pd_min) + pd_min; /* PerturbDepth :141-147 */
   perturb_normal_acmh(normal, nn, a1, a2, &r);
   correct_normal(nn, vd, ivl);
-  const float rdepth = rng_uniform(&r) * (depth_max - depth_min) + depth_min;
+  const int rand_depth = !(c->prior_mode == 2 && pri.w > 0.0f); /* :2467-2486 */
+  const float rdepth = rand_depth ? rng_uniform(&r) * (depth_max - depth_min) + depth_min : 0.0f;
   float rn[3];
   random_normal(&r, vd, rn);
   correct_normal(rn, vd, ivl);
@@ -661,13 +722,14 @@ static void sweep_pixel(ctx_t* c, int row, int col, float th_mc, uint64_t sk) {
   if (mi != 0)
     for (int v = 0; v < N; ++v) M[0][v] = M[mi][v];
   for (int v = 0; v < N; ++v) costs[0] += vw[v] * M[0][v];
-  for (int h = 1; h < 5; ++h) {
-    cost_vector(c, row, col, rh[h][3], rh[h], np, &pr, M[h]);
+  const int nh = rand_depth ? 5 : 4;
+  for (int h = 1; h < nh; ++h) {
+    cost_vector(c, row, col, rh[h][3], rh[h], np, &pr, M[h], prior_weight(c, &pri, rh[h], rh[h][3], pr.rvar));
     float cs = 0;
     for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
     costs[h] = cs;
   }
-  mi = find_min_cost(costs, 5);
+  mi = find_min_cost(costs, nh);
   if (mi != -1) {
     c->conf[pix] = costs[mi];
     c->depth[pix] = rh[mi][3];
@@ -1018,9 +1080,36 @@ int orc_run(const smvs_options* o, const smvs_problem* p, int row_begin, int row
   ctx_t c;
   int st = ctx_init(&c, o, p, 1);
   if (st != SMVS_OK) { ctx_free(&c); return st; }
-  if (o->has_prior_depth || o->propagate_depth) { ctx_free(&c); return SMVS_EINVAL; }
+  if (o->has_prior_depth && o->propagate_depth) { ctx_free(&c); return SMVS_EINVAL; }
+  if (o->propagate_depth && (o->init_depth_random || o->geom_consistency)) { ctx_free(&c); return SMVS_EINVAL; }
+  if (o->has_prior_depth && (!p->ref.depth || !p->ref.normal)) { ctx_free(&c); return SMVS_EINVAL; }
   if (!o->init_depth_random && (!p->ref.depth || !p->ref.normal)) { ctx_free(&c); return SMVS_EINVAL; }
-  init_workspace(&c, o->init_depth_random, p->ref.depth, p->ref.normal, (float)o->depth_min, (float)o->depth_max);
+  const size_t WH0 = (size_t)c.W * c.H;
+  float *pdepth = NULL, *pnormal = NULL, *pprior = NULL;
+  const float* init_depth = p->ref.depth;
+  const float* init_normal = p->ref.normal;
+  if (o->has_prior_depth) { /* InitPriorDepthAndNormalInfo, patch_match_cuda.cu:715-746 */
+    c.prior_mode = 1;
+    c.prior_depth = p->ref.depth;
+    c.prior_normal = p->ref.normal;
+    c.prior_wgt = p->ref_prior_wgt;
+  } else if (o->propagate_depth) { /* patch_match_cuda.cu:603-659 */
+    pdepth = (float*)malloc(sizeof(float) * WH0);
+    pnormal = (float*)malloc(sizeof(float) * 3 * WH0);
+    pprior = (float*)malloc(sizeof(float) * WH0);
+    if (!pdepth || !pnormal || !pprior) { free(pdepth); free(pnormal); free(pprior); ctx_free(&c); return SMVS_ENOMEM; }
+    memcpy(pdepth, p->ref.depth, sizeof(float) * WH0);
+    memcpy(pnormal, p->ref.normal, sizeof(float) * 3 * WH0);
+    st = orc_propagate_init(c.W, c.H, c.N, c.refK, c.refiK, c.poses, p->src, pdepth, pnormal, pprior);
+    if (st != SMVS_OK) { free(pdepth); free(pnormal); free(pprior); ctx_free(&c); return st; }
+    c.prior_mode = 2;
+    c.prior_depth = pprior;
+    init_depth = pdepth;
+    init_normal = pnormal;
+  }
+  init_workspace(&c, o->init_depth_random, init_depth, init_normal, (float)o->depth_min, (float)o->depth_max);
+  free(pdepth);
+  free(pnormal);
   int rb = 0, re = c.H;
   if (row_end > row_begin) { rb = row_begin < 0 ? 0 : row_begin; re = row_end > c.H ? c.H : row_end; }
   {
@@ -1068,6 +1157,7 @@ int orc_run(const smvs_options* o, const smvs_problem* p, int row_begin, int row
     if (out->curvature && curv) memcpy(out->curvature, curv, sizeof(uint16_t) * 2 * WH);
   }
   free(curv);
+  free(pprior);
   ctx_free(&c);
   return SMVS_OK;
 }

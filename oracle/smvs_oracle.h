@@ -46,6 +46,19 @@ typedef struct orc_outputs {
 int orc_run(const smvs_options* opt, const smvs_problem* prob, int row_begin, int row_end,
             orc_outputs* out);
 
+/* The propagate-depth initial maps (InitWorkspace, patch_match_cuda.cu:603-659):
+ * every source with a depth map (src[i].depth) is projected into the W x H
+ * reference view with its pose record (poses: N*43), pixels of `depth` that
+ * are <= 0 take the median (or the first / smaller of two) projected depth,
+ * `prior` (W*H) receives the medians that more than two projections agree
+ * with, and `normal` (3*W*H planar) is fitted to the result. depth and normal
+ * hold the given maps on entry. */
+int orc_propagate_init(int W, int H, int N, const float refK[4], const float refiK[4], const float* poses,
+                       const smvs_view* src, float* depth, float* normal, float* prior);
+/* The same for a PatchMatch problem (host memory): its pose records, with the
+ * given maps ref.depth / ref.normal copied into depth / normal first. */
+int orc_propagate_init_problem(const smvs_problem* prob, float* depth, float* normal, float* prior);
+
 /* PatchMatchACMMCuda::RunFilter(false): FilterDepthMapsKernel over the
  * problem's ref.depth using the source views' depth maps. Writes W*H. */
 int orc_run_filter(const smvs_options* opt, const smvs_problem* prob, float* depth_out);
@@ -87,6 +100,14 @@ int orc_encode_normal_map(const float* normal, int width, int height, uint32_t* 
  * InitDepthMapFromSparsePoint (:1205-1307, :483-518), Model2Depth (:520-642),
  * Ply2Depth (:643-750). `view` gives width, height, K, R, T; depth is W*H,
  * normal 3*W*H planar; range[2] is the returned depth range. */
+/* Delaunay initial map (InitDepthMapFromDelaunay, :398-474): the projected
+ * points that land in the view (input order; uv 2 per point, z, input index),
+ * and the map rasterised from a triangulation of them (counter-clockwise
+ * index triples into that list). */
+int orc_delaunay_points(const smvs_view* v, const float* xyz, size_t n, int32_t* uv, float* z, int32_t* idx,
+                        size_t* count);
+int orc_init_from_delaunay(const smvs_view* v, const float* xyz, size_t n, const int32_t* tris, size_t ntri,
+                           float* depth, float* normal, float* range);
 int orc_init_from_sparse_points(const smvs_view* view, const float* xyz, size_t n, float* depth, float* normal,
                                 float* range);
 int orc_init_from_mesh(const smvs_view* view, const double* vertices, size_t num_vertices, const int32_t* faces,
@@ -108,6 +129,16 @@ int orc_fusion_sizes(void* h, size_t* num_points, size_t* num_vis, int* order_co
 int orc_fusion_copy(void* h, smvs_fused_point* points, uint64_t* vis_offsets, uint32_t* vis_images, int* order);
 int orc_fusion_mask(void* h, int view, int width, int height, uint8_t* out);
 void orc_fusion_free(void* h);
+
+/* RemoveDuplicatePoints (fusion.cc:2184-2266) over a fused cloud: keep[i] = 0
+ * for the points it drops. */
+int orc_fusion_duplicate_keep(const smvs_fusion_view* views, int nv, const smvs_fused_point* pts, size_t n,
+                              const uint64_t* off, const uint32_t* vis, uint8_t* keep);
+/* RemoveOutliers (fusion.cc:2542-2611) with ComputeAverageDistance
+ * (patch_match_controller.cc:115-228) by brute-force neighbours: scores[n]
+ * updated in place, keep[n], spacing[n] (may be NULL). */
+int orc_fusion_outlier_keep(const smvs_fused_point* pts, size_t n, int nb, double max_spacing_factor, float* scores,
+                            uint8_t* keep, float* spacing);
 
 /* The generator shared with the engine: uniform in (0, 1]. */
 float orc_uniform(uint64_t seed, uint32_t stage, uint32_t pixel, uint32_t draw);

@@ -529,3 +529,125 @@ void orc_fusion_free(void* h) {
   free(o->order);
   free(o);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Clean-up passes after the image loop, over a fused cloud given as arrays.  */
+/* ------------------------------------------------------------------------ */
+
+/* RemoveDuplicatePoints, fusion.cc:2184-2266: keep[i] = 0 for the points it
+ * drops. The projection is Eigen's float K * (R * X + T) (3x3 products reduce
+ * as (p0 + p1) + p2) and std::round of proj / z; a point's images are visited
+ * in the order given (ascending in this library). */
+int orc_fusion_duplicate_keep(const smvs_fusion_view* views, int nv, const smvs_fused_point* pts, size_t n,
+                              const uint64_t* off, const uint32_t* vis, uint8_t* keep) {
+  if (!views || nv < 1 || (n && (!pts || !off || !vis)) || !keep) return SMVS_EINVAL;
+  int64_t** occ = (int64_t**)calloc((size_t)nv, sizeof(int64_t*));
+  uint8_t* removal = (uint8_t*)calloc(n ? n : 1, 1);
+  if (!occ || !removal) { free(occ); free(removal); return SMVS_ENOMEM; }
+  for (int v = 0; v < nv; ++v) {
+    const size_t plane = (size_t)views[v].width * views[v].height;
+    occ[v] = (int64_t*)malloc(sizeof(int64_t) * (plane ? plane : 1));
+    if (!occ[v]) {
+      for (int k = 0; k < v; ++k) free(occ[k]);
+      free(occ); free(removal);
+      return SMVS_ENOMEM;
+    }
+    for (size_t q = 0; q < plane; ++q) occ[v][q] = -1;
+  }
+  for (size_t i = 0; i < n; ++i) {
+    if (removal[i]) continue;
+    const uint64_t nvis = off[i + 1] - off[i];
+    const float X[3] = {pts[i].x, pts[i].y, pts[i].z};
+    for (uint64_t k = off[i]; k < off[i + 1]; ++k) {
+      const int img = (int)vis[k];
+      if (img < 0 || img >= nv) continue;
+      const smvs_fusion_view* v = &views[img];
+      float c[3], q[3];
+      for (int r = 0; r < 3; ++r) c[r] = ((v->R[3 * r] * X[0] + v->R[3 * r + 1] * X[1]) + v->R[3 * r + 2] * X[2]) + v->T[r];
+      for (int r = 0; r < 3; ++r) q[r] = (v->K[3 * r] * c[0] + v->K[3 * r + 1] * c[1]) + v->K[3 * r + 2] * c[2];
+      const int u = (int)roundf(q[0] / q[2]);
+      const int w = (int)roundf(q[1] / q[2]);
+      if (u < 0 || u >= v->width || w < 0 || w >= v->height) continue;
+      int64_t* o = &occ[img][(size_t)w * v->width + u];
+      if (*o == -1) { *o = (int64_t)i; continue; }
+      if (off[*o + 1] - off[*o] > nvis) { removal[i] = 1; break; }
+      removal[*o] = 1;
+      *o = (int64_t)i;
+    }
+  }
+  for (size_t i = 0; i < n; ++i) keep[i] = !removal[i];
+  for (int v = 0; v < nv; ++v) free(occ[v]);
+  free(occ);
+  free(removal);
+  return SMVS_OK;
+}
+
+/* ComputeAverageDistance (patch_match_controller.cc:115-228) by brute force:
+ * each point's K = nb + 1 nearest points (itself included) by squared distance
+ * in double (dx^2 + dy^2 + dz^2 summed in that order, CGAL's Euclidean
+ * distance), their square roots added nearest first into a float, over K - 1.
+ * Then RemoveOutliers (fusion.cc:2542-2611). scores (n) are updated in place;
+ * spacing (n, may be NULL) receives the per-point spacings. */
+int orc_fusion_outlier_keep(const smvs_fused_point* pts, size_t n, int nb, double max_spacing_factor, float* scores,
+                            uint8_t* keep, float* spacing) {
+  if ((n && (!pts || !scores || !keep)) || nb < 1 || nb > 63 || !(max_spacing_factor > 0)) return SMVS_EINVAL;
+  if (n == 0) return SMVS_OK;
+  const int K = nb + 1;
+  float* sp = (float*)malloc(sizeof(float) * n);
+  if (!sp) return SMVS_ENOMEM;
+#pragma omp parallel for schedule(dynamic, 64)
+  for (size_t i = 0; i < n; ++i) {
+    double best[64];
+    int cnt = 0;
+    const double qx = pts[i].x, qy = pts[i].y, qz = pts[i].z;
+    for (size_t j = 0; j < n; ++j) {
+      const double dx = qx - (double)pts[j].x, dy = qy - (double)pts[j].y, dz = qz - (double)pts[j].z;
+      double d = dx * dx;
+      d += dy * dy;
+      d += dz * dz;
+      if (cnt < K) {
+        int m = cnt++;
+        while (m > 0 && best[m - 1] > d) { best[m] = best[m - 1]; --m; }
+        best[m] = d;
+      } else if (d < best[K - 1]) {
+        int m = K - 1;
+        while (m > 0 && best[m - 1] > d) { best[m] = best[m - 1]; --m; }
+        best[m] = d;
+      }
+    }
+    float s = 0.0f;
+    for (int k = 0; k < cnt; ++k) s = (float)((double)s + sqrt(best[k]));
+    if (cnt > 1) s /= (float)(cnt - 1);
+    sp[i] = s;
+  }
+  float average = 0.0f;
+  for (size_t i = 0; i < n; ++i) average += sp[i];
+  average /= (float)n;
+  if (average > 1e-6) {
+    for (size_t i = 0; i < n; ++i) {
+      const float factor = (float)((double)sp[i] / (max_spacing_factor * (double)average));
+      scores[i] = (float)((double)scores[i] * 0.6 + (double)factor * 0.4);
+    }
+  }
+  float smin = scores[0], smax = scores[0];
+  for (size_t i = 0; i < n; ++i) {
+    if (scores[i] < smin) smin = scores[i];
+    if (scores[i] > smax) smax = scores[i];
+  }
+  const float range = smax - smin;
+  float ratios[256] = {0}, acc[256];
+  for (size_t i = 0; i < n; ++i) {
+    const int b = range > 0 ? (int)(((scores[i] - smin) / range) * 255) : 0;
+    ratios[b]++;
+  }
+  for (int k = 0; k < 256; ++k) ratios[k] /= (float)n;
+  float sum = 0.0f;
+  for (int k = 0; k < 256; ++k) { sum += ratios[k]; acc[k] = sum; }
+  for (size_t i = 0; i < n; ++i) {
+    const int b = range > 0 ? (int)(((scores[i] - smin) / range) * 255) : 0;
+    keep[i] = !((double)ratios[b] < 0.01 && (double)acc[b] >= 0.9);
+  }
+  if (spacing) memcpy(spacing, sp, sizeof(float) * n);
+  free(sp);
+  return SMVS_OK;
+}

@@ -241,3 +241,121 @@ int orc_init_from_dense_points(const smvs_view* v, const float* xyz, const float
   finish_range(lo, hi, range);
   return SMVS_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Delaunay initial map: InitDepthMap's projection (:1236-1256) and           */
+/* InitDepthMapFromDelaunay (:398-474) over a given triangulation.            */
+/* ------------------------------------------------------------------------ */
+
+/* The points that land in the view, in input order: their truncated pixel
+ * positions uv[2k], uv[2k + 1], camera depths z[k] and input indices idx[k]. */
+int orc_delaunay_points(const smvs_view* v, const float* xyz, size_t n, int32_t* uv, float* z, int32_t* idx,
+                        size_t* count) {
+  if (!v || (n && !xyz) || !uv || !z || !idx || !count) return SMVS_EINVAL;
+  size_t m = 0;
+  for (size_t i = 0; i < n; ++i) {
+    float Y[3], Xc[3];
+    mat3_apply_f(v->R, xyz + 3 * i, v->T, Y);
+    mat3_apply_f(v->K, Y, NULL, Xc);
+    if (!(Xc[2] > 0)) continue;
+    const float qu = Xc[0] / Xc[2], qv = Xc[1] / Xc[2];
+    if (!(qu > -1.0f && qu < (float)v->width && qv > -1.0f && qv < (float)v->height)) continue;
+    uv[2 * m] = (int)qu;
+    uv[2 * m + 1] = (int)qv;
+    z[m] = Xc[2];
+    idx[m] = (int32_t)i;
+    ++m;
+  }
+  *count = m;
+  return SMVS_OK;
+}
+
+static float dot3f(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+/* tris: counter-clockwise triples of indices into the orc_delaunay_points
+ * list. A pixel inside several triangles (on a shared edge) takes the one
+ * whose vertex indices, sorted, are largest. */
+int orc_init_from_delaunay(const smvs_view* v, const float* xyz, size_t n, const int32_t* tris, size_t ntri,
+                           float* depth, float* normal, float* range) {
+  if (!v || (n && !xyz) || (ntri && !tris) || !depth || !normal || !range) return SMVS_EINVAL;
+  const int W = v->width, H = v->height;
+  const size_t WH = (size_t)W * H;
+  int32_t* uv = (int32_t*)malloc(sizeof(int32_t) * 2 * (n ? n : 1));
+  float* z = (float*)malloc(sizeof(float) * (n ? n : 1));
+  int32_t* idx = (int32_t*)malloc(sizeof(int32_t) * (n ? n : 1));
+  unsigned long long* owner = (unsigned long long*)calloc(WH, sizeof(unsigned long long));
+  if (!uv || !z || !idx || !owner) { free(uv); free(z); free(idx); free(owner); return SMVS_ENOMEM; }
+  size_t m = 0;
+  orc_delaunay_points(v, xyz, n, uv, z, idx, &m);
+  /* The depth range covers every projected point (:1251-1254). */
+  float lo = FLT_MAX, hi = FLT_EPSILON;
+  for (size_t k = 0; k < m; ++k) { lo = fminf(lo, z[k]); hi = fmaxf(hi, z[k]); }
+  memset(depth, 0, sizeof(float) * WH);
+  memset(normal, 0, sizeof(float) * 3 * WH);
+  double Kd[9], Kid[9];
+  for (int k = 0; k < 9; ++k) Kd[k] = v->K[k];
+  inverse3d(Kd, Kid);
+  float kinv[9];
+  for (int k = 0; k < 9; ++k) kinv[k] = (float)Kid[k];
+  for (int pass = 0; pass < 2; ++pass)
+    for (size_t t = 0; t < ntri; ++t) {
+      double x[3], y[3];
+      float c[3][3];
+      int id[3];
+      for (int k = 0; k < 3; ++k) {
+        id[k] = tris[3 * t + k];
+        if (id[k] < 0 || (size_t)id[k] >= m) { free(uv); free(z); free(idx); free(owner); return SMVS_EINVAL; }
+        x[k] = (double)uv[2 * id[k]];
+        y[k] = (double)uv[2 * id[k] + 1];
+        const double zz = (double)z[id[k]];
+        const float q[3] = {(float)(x[k] * zz), (float)(y[k] * zz), (float)zz};
+        for (int r = 0; r < 3; ++r) c[k][r] = dot3f(kinv + 3 * r, q);
+      }
+      const float e1[3] = {c[1][0] - c[0][0], c[1][1] - c[0][1], c[1][2] - c[0][2]};
+      const float e2[3] = {c[2][0] - c[0][0], c[2][1] - c[0][1], c[2][2] - c[0][2]};
+      float nn[3] = {e2[1] * e1[2] - e2[2] * e1[1], e2[2] * e1[0] - e2[0] * e1[2], e2[0] * e1[1] - e2[1] * e1[0]};
+      const float sq = dot3f(nn, nn);
+      if (sq > 0.0f) {
+        const float nrm = sqrtf(sq);
+        nn[0] = nn[0] / nrm; nn[1] = nn[1] / nrm; nn[2] = nn[2] / nrm;
+      }
+      const float inv = 1.0f / dot3f(nn, c[0]);
+      const float np[3] = {nn[0] * inv, nn[1] * inv, nn[2] * inv};
+      int a = id[0], b = id[1], e = id[2], s;
+      if (a < b) { s = a; a = b; b = s; }
+      if (b < e) { s = b; b = e; e = s; }
+      if (a < b) { s = a; a = b; b = s; }
+      const unsigned long long key =
+          (((unsigned long long)a << 42) | ((unsigned long long)b << 21) | (unsigned long long)e) + 1ull;
+      double umin = x[0], umax = x[0], vmin = y[0], vmax = y[0];
+      for (int k = 1; k < 3; ++k) {
+        umin = fmin(umin, x[k]); umax = fmax(umax, x[k]);
+        vmin = fmin(vmin, y[k]); vmax = fmax(vmax, y[k]);
+      }
+      const int u0 = (int)umin > 0 ? (int)umin : 0, u1 = (int)umax < W - 1 ? (int)umax : W - 1;
+      const int v0 = (int)vmin > 0 ? (int)vmin : 0, v1 = (int)vmax < H - 1 ? (int)vmax : H - 1;
+      for (int vv = v0; vv <= v1; ++vv)
+        for (int uu = u0; uu <= u1; ++uu) {
+          const double m1 = (x[1] - x[0]) * ((double)vv - y[0]) - ((double)uu - x[0]) * (y[1] - y[0]);
+          const double m2 = (x[2] - x[1]) * ((double)vv - y[1]) - ((double)uu - x[1]) * (y[2] - y[1]);
+          const double m3 = (x[0] - x[2]) * ((double)vv - y[2]) - ((double)uu - x[2]) * (y[0] - y[2]);
+          if (!(m1 >= 0 && m2 >= 0 && m3 >= 0)) continue;
+          const size_t p = (size_t)vv * W + uu;
+          if (pass == 0) {
+            if (key > owner[p]) owner[p] = key;
+            continue;
+          }
+          if (owner[p] != key) continue;
+          const float q[3] = {(float)uu, (float)vv, 1.0f};
+          float xc[3];
+          for (int r = 0; r < 3; ++r) xc[r] = dot3f(kinv + 3 * r, q);
+          depth[p] = 1.0f / dot3f(np, xc);
+          normal[p] = nn[0];
+          normal[WH + p] = nn[1];
+          normal[2 * WH + p] = nn[2];
+        }
+    }
+  finish_range(lo, hi, range);
+  free(uv); free(z); free(idx); free(owner);
+  return SMVS_OK;
+}

@@ -79,7 +79,7 @@ class smvs_view(C.Structure):
 class smvs_problem(C.Structure):
     _fields_ = [
         ("ref", smvs_view), ("src", C.POINTER(smvs_view)), ("num_src", C.c_int),
-        ("ref_mask", C.c_void_p), ("memory", C.c_int),
+        ("ref_mask", C.c_void_p), ("memory", C.c_int), ("ref_prior_wgt", C.c_void_p),
     ]
 
 
@@ -208,6 +208,8 @@ _SIGNATURES = {
     "smvs_cross_filter_release_cache": (C.c_int, [C.c_int]),
     "smvs_init_depth_from_sparse_points": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_size_t, C.c_int,
                                                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_init_depth_from_delaunay": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_size_t, C.c_int,
+                                                     C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_init_depth_from_mesh": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t,
                                             C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_init_depth_from_dense_points": (C.c_int, [C.POINTER(smvs_view), C.c_void_p, C.c_void_p, C.c_size_t, C.c_int,
@@ -225,6 +227,8 @@ _SIGNATURES = {
     "smvs_fusion_get_device_points": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p),
                                                 C.POINTER(C.c_void_p)]),
     "smvs_fusion_get_image_order": (C.c_int, [C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]),
+    "smvs_fusion_remove_duplicate_points": (C.c_int, [C.c_void_p, C.POINTER(C.c_size_t)]),
+    "smvs_fusion_remove_outliers": (C.c_int, [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_size_t)]),
     "smvs_fusion_get_mask": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p]),
     "smvs_fusion_set_profiling": (C.c_int, [C.c_void_p, C.c_int]),
     "smvs_fusion_get_profile": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
@@ -253,6 +257,8 @@ _SIGNATURES = {
     "smvs_test_take_cuda_error": (C.c_int, []),
     "smvs_test_fusion_waits": (C.c_int, [C.c_double, C.c_longlong]),
     "smvs_test_tile_waits": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "smvs_test_propagate_init": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "smvs_test_delaunay": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "smvs_pyramid_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                           C.POINTER(C.c_float)]),
     "smvs_rescale_image": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_void_p,

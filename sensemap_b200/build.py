@@ -26,7 +26,7 @@ NVCC_FLAGS = COMMON_FLAGS + ["--use_fast_math"]
 # flush to zero): the cross-view filter's decisions and medians, and the
 # depth tests of the initial maps, the fusion's consistency tests and medians.
 EXACT_FLAGS = COMMON_FLAGS + ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"]
-EXACT_UNITS = {"smvs_cross_filter.cu", "smvs_init_maps.cu", "smvs_fusion.cu", "smvs_pyramid.cu"}
+EXACT_UNITS = {"smvs_cross_filter.cu", "smvs_init_maps.cu", "smvs_fusion.cu", "smvs_pyramid.cu", "smvs_prior.cu"}
 
 
 def _nvcc() -> str:

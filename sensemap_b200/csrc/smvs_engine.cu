@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/smvs.h"
+#include "../../include/smvs_testing.h"
 #include "smvs_device.cuh"
 #include "smvs_kernels.h"
 
@@ -153,6 +154,12 @@ struct smvs_engine {
   float* d_init_normal = nullptr;  // ref.normal as given
   uint8_t* d_mask = nullptr;
   uint16_t* d_curv = nullptr;   // 2*W*H (est_curvature && geom_consistency)
+  float* d_prior_wgt = nullptr;   // ref_prior_wgt as given (has_prior_depth)
+  float* d_prior = nullptr;       // W*H projected prior depth (propagate_depth)
+  float* d_composite = nullptr;   // N*W*H projected depths per source (propagate_depth)
+  std::vector<int> src_w, src_h;  // source sizes (the propagate-depth projection grid)
+  std::vector<const float*> src_depth;  // pitched device copies of the sources' depth maps (NULL = none)
+  std::vector<size_t> src_depth_pitch;
   // One-job batch for the checkerboard kernels: [JobParams | iters | prefix | conf prefix].
   void* d_batch = nullptr;
   CUtensorMap* d_tmap = nullptr;  // the reference image's TMA descriptor
@@ -260,7 +267,10 @@ int smvs_internal_prepare_job(smvs::JobParams* p, const smvs_options* o) {
   p->conf_blocks_x = (p->W + 31) / 32;
   // Threads per pixel: the requested value, raised until the block's cost
   // matrices fit in shared memory (maps do not depend on it).
-  const int tpp = smvs::FitThreadsPerPixel(p->R, smvs::ViewBucket(p->N), p->block_x, p->tpp > 0 ? p->tpp : 1);
+  // Jobs with a prior run the thread-per-pixel kernels, which alone carry the
+  // prior paths.
+  const int want = p->prior_mode != 0 ? 1 : (p->tpp > 0 ? p->tpp : 1);
+  const int tpp = smvs::FitThreadsPerPixel(p->R, smvs::ViewBucket(p->N), p->block_x, want);
   if (!tpp)
     return Fail(SMVS_EINVAL, "no launch shape with sweep_block_x=%d fits %d source views in shared memory",
                 p->block_x, p->N);
@@ -346,8 +356,18 @@ int smvs_options_check(const smvs_options* o) {
     return Fail(SMVS_EINVAL, "window (radius=%d, step=%d) not supported: use (3|5|7,1) or (3|4|5|7,2)",
                 o->window_radius, o->window_step);
   if (o->thk < 1 || o->thk > 4) return Fail(SMVS_EINVAL, "thk must be in 1..4 (mweights, kernel_functions.cu:22)");
-  if (o->has_prior_depth || o->propagate_depth)
-    return Fail(SMVS_EINVAL, "prior-depth and propagate-depth initialisation are not supported");
+  // patch_match_cuda.cu:946-947: the two prior paths share one set of buffers.
+  if (o->has_prior_depth && o->propagate_depth)
+    return Fail(SMVS_EINVAL, "has_prior_depth and propagate_depth exclude each other");
+  // The propagate-depth initialisation lives in the given-map branch of
+  // InitWorkspace (patch_match_cuda.cu:593-603), and its projections read the
+  // source depth maps that the geometric pass would use
+  // (patch_match_cuda.cu:318-377); the controller never combines them
+  // (patch_match_controller.cc:3611-3613).
+  if (o->propagate_depth && o->init_depth_random)
+    return Fail(SMVS_EINVAL, "propagate_depth needs init_depth_random == 0");
+  if (o->propagate_depth && o->geom_consistency)
+    return Fail(SMVS_EINVAL, "propagate_depth excludes geom_consistency");
   if (o->num_iterations > smvs::kMaxIterations)
     return Fail(SMVS_EINVAL, "num_iterations must be <= %d", smvs::kMaxIterations);
   if (o->image_storage < SMVS_STORE_U8 || o->image_storage > SMVS_STORE_F32)
@@ -370,6 +390,8 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
   if (opt->geom_consistency)
     for (int i = 0; i < prob->num_src; ++i)
       if (!prob->src[i].depth) return Fail(SMVS_EINVAL, "geom_consistency needs every source view's depth map");
+  if (opt->has_prior_depth && (!prob->ref.depth || !prob->ref.normal))
+    return Fail(SMVS_EINVAL, "has_prior_depth needs the reference view's depth and normal maps (ref.depth, ref.normal)");
   if (!opt->init_depth_random && (!prob->ref.depth || !prob->ref.normal) && opt->num_iterations >= 0) {
     // Run() with init_depth_random == 0 starts from the given maps
     // (patch_match_cuda.cu:593-601); RunFilter needs ref.depth only.
@@ -478,6 +500,10 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
     if (err != cudaSuccess) { delete e; return Fail(SMVS_ECUDA, "source texture: %s", cudaGetErrorString(err)); }
     e->textures.push_back(tex);
     p.src_tex[i] = tex;
+    e->src_w.push_back(v.width);
+    e->src_h.push_back(v.height);
+    e->src_depth.push_back(nullptr);
+    e->src_depth_pitch.push_back(0);
     if (v.depth) {
       float* dd = nullptr;
       size_t dpitch = 0;
@@ -490,6 +516,8 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
       if (err != cudaSuccess) { delete e; return Fail(SMVS_ECUDA, "depth texture: %s", cudaGetErrorString(err)); }
       e->textures.push_back(tex);
       p.dep_tex[i] = tex;
+      e->src_depth.back() = dd;
+      e->src_depth_pitch.back() = dpitch;
     }
   }
   e->has_src_depth = true;
@@ -508,6 +536,24 @@ int smvs_create(const smvs_options* opt, const smvs_problem* prob, void* stream,
     e->has_init = (prob->ref.normal != nullptr);
   }
   if (prob->ref_mask) TRY(StageIn(e, prob->ref_mask, WH, prob->memory, (void**)&e->d_mask));
+  // Prior maps (InitPriorDepthAndNormalInfo, patch_match_cuda.cu:715-746): the
+  // reference view's given depth and normal maps and its optional weights.
+  if (opt->has_prior_depth) {
+    p.prior_mode = 1;
+    p.prior_depth = e->d_init_depth;
+    p.prior_normal = e->d_init_normal;
+    if (prob->ref_prior_wgt) {
+      TRY(StageIn(e, prob->ref_prior_wgt, WH * sizeof(float), prob->memory, (void**)&e->d_prior_wgt));
+      p.prior_wgt = e->d_prior_wgt;
+    }
+  } else if (opt->propagate_depth) {
+    // The reference's sweep reads prior normal and weight maps that this mode
+    // never fills (0 x 0 buffers, patch_match_cuda.cu:588-591): here they read as 0.
+    TRY(e->Alloc((void**)&e->d_prior, WH * sizeof(float)));
+    TRY(e->Alloc((void**)&e->d_composite, (size_t)N * WH * sizeof(float)));
+    p.prior_mode = 2;
+    p.prior_depth = e->d_prior;
+  }
   if (opt->est_curvature && opt->geom_consistency) TRY(e->Alloc((void**)&e->d_curv, 2 * WH * sizeof(uint16_t)));
   TRY(e->Alloc(&e->d_batch, sizeof(smvs::JobParams) + 8 * sizeof(int)));
   TRY(e->Alloc((void**)&e->d_tmap, sizeof(CUtensorMap)));
@@ -560,6 +606,14 @@ int smvs_run(smvs_engine* e) {
     if (!e->has_init) return Fail(SMVS_EINVAL, "init_depth_random == 0 needs ref.depth and ref.normal");
     SMVS_CUDA(cudaMemcpyAsync(e->d_depth, e->d_init_depth, WH * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
     SMVS_CUDA(cudaMemcpyAsync(e->d_normal, e->d_init_normal, 3 * WH * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+  }
+  if (o.propagate_depth) {  // patch_match_cuda.cu:603-659
+    int st = Launch(e, SMVS_KERNEL_INIT, "propagate-depth init", [&] {
+      return smvs::LaunchPropagateInit(p, e->src_w.data(), e->src_h.data(),
+                                       e->src_depth.data(), e->src_depth_pitch.data(), e->d_composite,
+                                       e->d_prior, e->stream);
+    });
+    if (st) return st;
   }
   p.stage_key = smvs::StageKey(o.random_seed, smvs::kStageInit);
   int st = Launch(e, SMVS_KERNEL_INIT, "init", [&] {
@@ -636,6 +690,28 @@ int smvs_run(smvs_engine* e) {
   if (e->d_mask && (st = Launch(e, SMVS_KERNEL_MASK, "mask", [&] { return smvs::LaunchMask(p, e->d_mask, e->stream); })))
     return st;
   e->ran = true;
+  return SMVS_OK;
+}
+
+// Test hook: the propagate-depth initial maps alone (the given maps composited
+// with the projected source depths, before random hypotheses fill the rest).
+int smvs_test_propagate_init(smvs_engine* e, float* depth, float* normal, float* prior) {
+  if (!e || !depth || !normal || !prior) return Fail(SMVS_EINVAL, "null argument");
+  if (!e->opt.propagate_depth) return Fail(SMVS_EINVAL, "the engine was not created with propagate_depth");
+  cudaSetDevice(e->device);
+  const size_t WH = (size_t)e->W * e->H;
+  const smvs::JobParams& p = e->jp;
+  SMVS_CUDA(cudaMemcpyAsync(e->d_depth, e->d_init_depth, WH * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+  SMVS_CUDA(cudaMemcpyAsync(e->d_normal, e->d_init_normal, 3 * WH * sizeof(float), cudaMemcpyDeviceToDevice, e->stream));
+  int st = Launch(e, SMVS_KERNEL_INIT, "propagate-depth init", [&] {
+    return smvs::LaunchPropagateInit(p, e->src_w.data(), e->src_h.data(), e->src_depth.data(),
+                                     e->src_depth_pitch.data(), e->d_composite, e->d_prior, e->stream);
+  });
+  if (st) return st;
+  SMVS_CUDA(cudaMemcpyAsync(depth, e->d_depth, WH * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+  SMVS_CUDA(cudaMemcpyAsync(normal, e->d_normal, 3 * WH * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+  SMVS_CUDA(cudaMemcpyAsync(prior, e->d_prior, WH * sizeof(float), cudaMemcpyDeviceToHost, e->stream));
+  SMVS_CUDA(cudaStreamSynchronize(e->stream));
   return SMVS_OK;
 }
 

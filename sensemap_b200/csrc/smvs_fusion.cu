@@ -1883,6 +1883,164 @@ int CheckStatus(smvs_fusion* f) {
   return SMVS_OK;
 }
 
+// ---- clean-up passes after the image loop ----------------------------------
+// The fused cloud on the host (points, visibility offsets, image indices).
+struct HostCloud {
+  std::vector<smvs_fused_point> pts;
+  std::vector<uint64_t> off;
+  std::vector<uint32_t> vis;
+};
+
+int Download(smvs_fusion* f, HostCloud& c) {
+  c.pts.resize(f->num_points);
+  c.off.resize(f->num_points + 1);
+  c.vis.resize(f->num_vis);
+  if (f->num_points)
+    FU_CUDA(cudaMemcpyAsync(c.pts.data(), f->d_out_pts, f->num_points * sizeof(smvs_fused_point),
+                            cudaMemcpyDeviceToHost, f->stream));
+  FU_CUDA(cudaMemcpyAsync(c.off.data(), f->d_out_visoff, (f->num_points + 1) * sizeof(uint64_t),
+                          cudaMemcpyDeviceToHost, f->stream));
+  if (f->num_vis)
+    FU_CUDA(cudaMemcpyAsync(c.vis.data(), f->d_out_vis, f->num_vis * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                            f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  return SMVS_OK;
+}
+
+// Keeps the points with keep[i] (order preserved, as the reference's in-place
+// compaction loops do) and writes the cloud back to the device arrays, which
+// only shrink.
+int CompactUpload(smvs_fusion* f, HostCloud& c, const std::vector<uint8_t>& keep, size_t* removed) {
+  size_t j = 0, v = 0;
+  for (size_t i = 0; i < c.pts.size(); ++i) {
+    if (!keep[i]) continue;
+    const uint64_t b = c.off[i], e = c.off[i + 1];
+    c.pts[j] = c.pts[i];
+    c.off[j] = v;
+    for (uint64_t k = b; k < e; ++k) c.vis[v++] = c.vis[k];
+    ++j;
+  }
+  c.off[j] = v;
+  if (removed) *removed = c.pts.size() - j;
+  if (j) FU_CUDA(cudaMemcpyAsync(f->d_out_pts, c.pts.data(), j * sizeof(smvs_fused_point), cudaMemcpyHostToDevice,
+                                 f->stream));
+  FU_CUDA(cudaMemcpyAsync(f->d_out_visoff, c.off.data(), (j + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice,
+                          f->stream));
+  if (v) FU_CUDA(cudaMemcpyAsync(f->d_out_vis, c.vis.data(), v * sizeof(uint32_t), cudaMemcpyHostToDevice, f->stream));
+  FU_CUDA(cudaStreamSynchronize(f->stream));
+  f->num_points = j;
+  f->num_vis = v;
+  return SMVS_OK;
+}
+
+// Eigen 3.3's float evaluation of K * (R * X + T) (coefficient-based 3x3
+// products reduce as (p0 + p1) + p2), then proj / z rounded half away from
+// zero (std::round), as RemoveDuplicatePoints projects (fusion.cc:2216-2219).
+void ProjectPoint(const smvs_fusion_view& v, const smvs_fused_point& p, int* u, int* w) {
+  const float X[3] = {p.x, p.y, p.z};
+  float c[3], q[3];
+  for (int r = 0; r < 3; ++r) c[r] = ((v.R[3 * r] * X[0] + v.R[3 * r + 1] * X[1]) + v.R[3 * r + 2] * X[2]) + v.T[r];
+  for (int r = 0; r < 3; ++r) q[r] = (v.K[3 * r] * c[0] + v.K[3 * r + 1] * c[1]) + v.K[3 * r + 2] * c[2];
+  *u = (int)std::round(q[0] / q[2]);
+  *w = (int)std::round(q[1] / q[2]);
+}
+
+// Exact k-nearest-neighbour spacing on a uniform grid. Points are bucketed by
+// cell (counting sort); each query scans cubes of growing half-width r cells
+// around its own cell, keeping the K smallest squared distances (double, the
+// coordinate differences squared and summed x, y, z as CGAL's Euclidean
+// distance does), and stops once K are known and the K-th lies within r cell
+// widths (every point nearer than that is inside the scanned cube; a 1e-9
+// relative margin covers the rounding of the cell assignment) or the cube
+// covers the grid.
+constexpr int kMaxKnn = 64;
+
+struct KnnGrid {
+  double minx, miny, minz, h, inv_h;
+  int gx, gy, gz;
+};
+
+__device__ __forceinline__ int CellCoord(double v, double lo, double inv_h, int g) {
+  int c = (int)floor((v - lo) * inv_h);
+  return c < 0 ? 0 : (c >= g ? g - 1 : c);
+}
+
+__global__ void KnnCountKernel(const smvs_fused_point* __restrict__ pts, uint32_t n, KnnGrid g,
+                               uint32_t* __restrict__ cell_of, uint32_t* __restrict__ counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int cx = CellCoord((double)pts[i].x, g.minx, g.inv_h, g.gx);
+  const int cy = CellCoord((double)pts[i].y, g.miny, g.inv_h, g.gy);
+  const int cz = CellCoord((double)pts[i].z, g.minz, g.inv_h, g.gz);
+  const uint32_t cell = ((uint32_t)cz * g.gy + (uint32_t)cy) * g.gx + (uint32_t)cx;
+  cell_of[i] = cell;
+  atomicAdd(counts + cell, 1u);
+}
+
+__global__ void KnnScatterKernel(uint32_t n, const uint32_t* __restrict__ cell_of, const uint32_t* __restrict__ start,
+                                 uint32_t* __restrict__ cursor, uint32_t* __restrict__ sorted) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t c = cell_of[i];
+  sorted[start[c] + atomicAdd(cursor + c, 1u)] = i;
+}
+
+// ComputeAverageDistance's per-point spacing (patch_match_controller.cc:160-181):
+// the mean distance of the query's K = nb_neighbors + 1 nearest points (itself
+// included, at distance 0) over K - 1, accumulated nearest first in float with
+// each distance added in double.
+__global__ void KnnSpacingKernel(const smvs_fused_point* __restrict__ pts, uint32_t n, KnnGrid g,
+                                 const uint32_t* __restrict__ start, const uint32_t* __restrict__ sorted, int K,
+                                 float* __restrict__ spacing) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double qx = pts[i].x, qy = pts[i].y, qz = pts[i].z;
+  const int cx = CellCoord(qx, g.minx, g.inv_h, g.gx);
+  const int cy = CellCoord(qy, g.miny, g.inv_h, g.gy);
+  const int cz = CellCoord(qz, g.minz, g.inv_h, g.gz);
+  double best[kMaxKnn];
+  int cnt = 0;
+  const int rmax = max(g.gx, max(g.gy, g.gz));
+  for (int r = 0; r <= rmax; ++r) {
+    // Cells at Chebyshev distance exactly r from the query's cell.
+    for (int z = cz - r; z <= cz + r; ++z) {
+      if (z < 0 || z >= g.gz) continue;
+      for (int y = cy - r; y <= cy + r; ++y) {
+        if (y < 0 || y >= g.gy) continue;
+        // Inner rows of the shell hold only its two end cells.
+        const bool face = (z == cz - r || z == cz + r || y == cy - r || y == cy + r);
+        const int step = face ? 1 : 2 * r;
+        for (int x = cx - r; x <= cx + r; x += step) {
+          if (x < 0 || x >= g.gx) continue;
+          const uint32_t cell = ((uint32_t)z * g.gy + (uint32_t)y) * g.gx + (uint32_t)x;
+          for (uint32_t k = start[cell]; k < start[cell + 1]; ++k) {
+            const smvs_fused_point& p = pts[sorted[k]];
+            const double dx = qx - (double)p.x, dy = qy - (double)p.y, dz = qz - (double)p.z;
+            double d = dx * dx;
+            d += dy * dy;
+            d += dz * dz;
+            if (cnt < K) {
+              int m = cnt++;
+              while (m > 0 && best[m - 1] > d) { best[m] = best[m - 1]; --m; }
+              best[m] = d;
+            } else if (d < best[K - 1]) {
+              int m = K - 1;
+              while (m > 0 && best[m - 1] > d) { best[m] = best[m - 1]; --m; }
+              best[m] = d;
+            }
+          }
+        }
+      }
+    }
+    const double reach = (double)r * g.h * (1.0 - 1e-9);
+    if (cnt == K && best[K - 1] <= reach * reach) break;
+  }
+  float s = 0.0f;
+  for (int k = 0; k < cnt; ++k) s = (float)((double)s + sqrt(best[k]));
+  if (cnt > 1) s /= (float)(cnt - 1);
+  spacing[i] = s;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2257,6 +2415,165 @@ int smvs_test_fusion_waits(double limit_seconds, long long withhold_seed) {
   t_wait_limit_ns = (unsigned long long)(limit_seconds * 1e9);
   t_withhold = withhold_seed;
   return SMVS_OK;
+}
+
+int smvs_fusion_remove_duplicate_points(smvs_fusion* f, size_t* num_removed) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (!f->ran) return Fail(SMVS_ESTATE, "fusion: run first");
+  if (cudaSetDevice(f->device) != cudaSuccess) return Fail(SMVS_ECUDA, "fusion: cannot use GPU %d", f->device);
+  HostCloud c;
+  int st = Download(f, c);
+  if (st) return st;
+  // RemoveDuplicatePoints (fusion.cc:2184-2266): points in fusion order claim
+  // the pixel they project to in each of their images; a point meeting an
+  // occupant seen by more images is dropped (and looks no further), otherwise
+  // it takes the pixel and the occupant is dropped.
+  std::vector<std::vector<int64_t>> occ(f->num_views);
+  for (int v = 0; v < f->num_views; ++v)
+    occ[v].assign((size_t)f->views[v].width * (size_t)f->views[v].height, -1);
+  const size_t n = c.pts.size();
+  std::vector<uint8_t> removal(n, 0);
+  for (size_t i = 0; i < n; ++i) {
+    if (removal[i]) continue;
+    const uint64_t nvis = c.off[i + 1] - c.off[i];
+    for (uint64_t k = c.off[i]; k < c.off[i + 1]; ++k) {
+      const int img = (int)c.vis[k];
+      const smvs_fusion_view& v = f->views[img];
+      int u, w;
+      ProjectPoint(v, c.pts[i], &u, &w);
+      if (u < 0 || u >= v.width || w < 0 || w >= v.height) continue;
+      int64_t& o = occ[img][(size_t)w * v.width + u];
+      if (o == -1) {
+        o = (int64_t)i;
+        continue;
+      }
+      const uint64_t ovis = c.off[o + 1] - c.off[o];
+      if (ovis > nvis) {
+        removal[i] = 1;
+        break;
+      }
+      removal[o] = 1;
+      o = (int64_t)i;
+    }
+  }
+  std::vector<uint8_t> keep(n);
+  for (size_t i = 0; i < n; ++i) keep[i] = !removal[i];
+  return CompactUpload(f, c, keep, num_removed);
+}
+
+int smvs_fusion_remove_outliers(smvs_fusion* f, int nb_neighbors, double max_spacing_factor, size_t* num_removed) {
+  if (!f) return Fail(SMVS_EINVAL, "null fusion");
+  if (!f->ran) return Fail(SMVS_ESTATE, "fusion: run first");
+  if (nb_neighbors < 1 || nb_neighbors + 1 > kMaxKnn)
+    return Fail(SMVS_EINVAL, "fusion: nb_neighbors must be in 1..%d", kMaxKnn - 1);
+  if (!(max_spacing_factor > 0)) return Fail(SMVS_EINVAL, "fusion: max_spacing_factor must be > 0");
+  if (cudaSetDevice(f->device) != cudaSuccess) return Fail(SMVS_ECUDA, "fusion: cannot use GPU %d", f->device);
+  if (num_removed) *num_removed = 0;
+  const size_t n = f->num_points;
+  if (n == 0) return SMVS_OK;
+  if (n >= (1ull << 32) - 1) return Fail(SMVS_EINVAL, "fusion: too many points for the neighbour grid");
+  HostCloud c;
+  int st = Download(f, c);
+  if (st) return st;
+  // Grid: about one cell per point over the bounding box (cells of equal
+  // side, at least one per axis, at most 2^24 per axis).
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (const auto& p : c.pts) {
+    const double x[3] = {p.x, p.y, p.z};
+    for (int a = 0; a < 3; ++a) { lo[a] = std::min(lo[a], x[a]); hi[a] = std::max(hi[a], x[a]); }
+  }
+  if (!(std::isfinite(lo[0]) && std::isfinite(lo[1]) && std::isfinite(lo[2]) && std::isfinite(hi[0]) &&
+        std::isfinite(hi[1]) && std::isfinite(hi[2])))
+    return Fail(SMVS_EINVAL, "fusion: non-finite point coordinates");
+  const double ext[3] = {hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2]};
+  const double emax = std::max(ext[0], std::max(ext[1], ext[2]));
+  double vol = 1.0;
+  int flat = 0;
+  for (int a = 0; a < 3; ++a) {
+    if (ext[a] > emax * 1e-6) vol *= ext[a];
+    else ++flat;
+  }
+  double h = emax > 0 ? std::pow(vol / (double)n, 1.0 / (3 - std::min(flat, 2))) : 1.0;
+  if (!(h > 0)) h = 1.0;
+  KnnGrid g;
+  g.minx = lo[0]; g.miny = lo[1]; g.minz = lo[2];
+  int dims[3];
+  for (;;) {
+    for (int a = 0; a < 3; ++a) dims[a] = (int)std::min(16777216.0, std::floor(ext[a] / h) + 1.0);
+    if ((double)dims[0] * dims[1] * dims[2] <= 4.0 * (double)n + 64.0) break;
+    h *= 1.26;
+  }
+  g.h = h; g.inv_h = 1.0 / h;
+  g.gx = dims[0]; g.gy = dims[1]; g.gz = dims[2];
+  const size_t cells = (size_t)g.gx * g.gy * g.gz;
+  uint32_t *cell_of = nullptr, *counts = nullptr, *startv = nullptr, *cursor = nullptr, *sorted = nullptr;
+  float* spacing = nullptr;
+  auto release = [&] {
+    Free(f, cell_of); Free(f, counts); Free(f, startv); Free(f, cursor); Free(f, sorted); Free(f, spacing);
+  };
+  if ((st = Alloc(f, &cell_of, n)) || (st = Alloc(f, &counts, cells)) || (st = Alloc(f, &startv, cells + 1)) ||
+      (st = Alloc(f, &cursor, cells)) || (st = Alloc(f, &sorted, n)) || (st = Alloc(f, &spacing, n))) {
+    release();
+    return st;
+  }
+  const uint32_t nn = (uint32_t)n;
+  const int K = nb_neighbors + 1;
+  if (cudaMemsetAsync(counts, 0, cells * sizeof(uint32_t), f->stream) != cudaSuccess ||
+      cudaMemsetAsync(cursor, 0, cells * sizeof(uint32_t), f->stream) != cudaSuccess) {
+    release();
+    return Fail(SMVS_ECUDA, "fusion: clearing the neighbour grid failed");
+  }
+  KnnCountKernel<<<(nn + 255) / 256, 256, 0, f->stream>>>(f->d_out_pts, nn, g, cell_of, counts);
+  st = Scan(f, counts, cells, startv);
+  if (!st) {
+    KnnScatterKernel<<<(nn + 255) / 256, 256, 0, f->stream>>>(nn, cell_of, startv, cursor, sorted);
+    KnnSpacingKernel<<<(nn + 127) / 128, 128, 0, f->stream>>>(f->d_out_pts, nn, g, startv, sorted, K, spacing);
+    f->launches += 3;
+  }
+  std::vector<float> dists(n);
+  if (!st && (cudaGetLastError() != cudaSuccess ||
+              cudaMemcpyAsync(dists.data(), spacing, n * sizeof(float), cudaMemcpyDeviceToHost, f->stream) !=
+                  cudaSuccess ||
+              cudaStreamSynchronize(f->stream) != cudaSuccess))
+    st = Fail(SMVS_ECUDA, "fusion: neighbour spacing kernels failed");
+  release();
+  if (st) return st;
+  // ComputeAverageDistance's mean (patch_match_controller.cc:184-227): a float
+  // sum in point order.
+  float average = 0.0f;
+  for (size_t i = 0; i < n; ++i) average += dists[i];
+  average /= (float)n;
+  // RemoveOutliers (fusion.cc:2542-2611): blend each score with its spacing
+  // ratio, histogram the scores over 256 bins of [min, max], and drop points
+  // in a bin holding under 1 % of the points at or above the 90th cumulative
+  // percent.
+  if (average > 1e-6) {
+    for (size_t i = 0; i < n; ++i) {
+      const float factor = (float)((double)dists[i] / (max_spacing_factor * (double)average));
+      c.pts[i].score = (float)((double)c.pts[i].score * 0.6 + (double)factor * 0.4);
+    }
+  }
+  float smin = c.pts[0].score, smax = c.pts[0].score;
+  for (const auto& p : c.pts) { smin = std::min(smin, p.score); smax = std::max(smax, p.score); }
+  const float range = smax - smin;
+  // One score for every point (range 0) puts all points in bin 0: none is
+  // dropped (the reference divides 0 by 0 there).
+  auto bin = [&](float score) -> int {
+    if (!(range > 0)) return 0;
+    const float gray = (score - smin) / range;
+    return (int)(gray * 255);
+  };
+  std::vector<float> ratios(256, 0.0f), acc(256, 0.0f);
+  for (const auto& p : c.pts) ratios[bin(p.score)]++;
+  for (int k = 0; k < 256; ++k) ratios[k] /= (float)n;
+  float sum = 0.0f;
+  for (int k = 0; k < 256; ++k) { sum += ratios[k]; acc[k] = sum; }
+  std::vector<uint8_t> keep(n);
+  for (size_t i = 0; i < n; ++i) {
+    const int b = bin(c.pts[i].score);
+    keep[i] = !((double)ratios[b] < 0.01 && (double)acc[b] >= 0.9);
+  }
+  return CompactUpload(f, c, keep, num_removed);
 }
 
 void smvs_fusion_destroy(smvs_fusion* f) {

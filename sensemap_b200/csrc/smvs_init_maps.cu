@@ -27,12 +27,19 @@
 #include <cstdio>
 #include <cstring>
 
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "../../include/smvs.h"
 
 extern "C" void smvs_internal_set_error(const char* msg);
 cudaMemPool_t smvs_internal_device_pool(int device);
+
+namespace smvs {
+// smvs_delaunay.cpp
+int DelaunayTriangulate(const int32_t* xy, int n, std::vector<int32_t>& tris);
+}
 
 namespace {
 
@@ -376,6 +383,124 @@ __global__ void PointResolveKernel(Cam c, const PointRec* __restrict__ recs, siz
   }
 }
 
+// ---------------------------------------------------------------------------
+// Delaunay initial map: InitDepthMap's projection (:1236-1256, truncated pixel
+// positions), then InitDepthMapFromDelaunay (:398-474) over the triangulation
+// of those positions: each triangle's plane through its three back-projected
+// points is written, depth and camera-frame normal, to the pixels inside it.
+// ---------------------------------------------------------------------------
+__global__ void ProjectUvdKernel(Cam c, const float* __restrict__ xyz, size_t n, int2* __restrict__ uv,
+                                 float* __restrict__ z, uint32_t* __restrict__ range) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float X[3] = {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]};
+    float Y[3], Xc[3];
+    Apply3(c.Rf, X, c.Tf, Y);
+    Apply3(c.Kf, Y, (const float*)nullptr, Xc);
+    uv[i] = make_int2(-1, -1);
+    if (!(Xc[2] > 0)) continue;
+    const float qu = Xc[0] / Xc[2], qv = Xc[1] / Xc[2];
+    if (!(qu > -1.0f && qu < (float)c.W && qv > -1.0f && qv < (float)c.H)) continue;
+    uv[i] = make_int2((int)qu, (int)qv);
+    z[i] = Xc[2];
+    atomicMin(range, FKey(Xc[2]));
+    atomicMax(range + 1, FKey(Xc[2]));
+  }
+}
+
+struct DelaunayTri {
+  double x[3], y[3];  // vertex positions (pixels, as the reference's double CGAL points)
+  float n[3];         // unit normal (edge2 x edge1)
+  float np[3];        // normal / (normal . c0)
+  int u0, u1, v0, v1; // pixel box, clipped to the image
+  unsigned long long key;  // order-free owner key of shared pixels (0 = degenerate, skipped)
+};
+
+__device__ __forceinline__ float Dot3f(const float* a, const float* b) { return (a[0] * b[0] + a[1] * b[1]) + a[2] * b[2]; }
+
+// Per triangle: the plane of RasterDepthDataPlaneData (:230-247) from the
+// three points (u z, v z, z) mapped by K^-1 (float), as :435-447 composes it.
+__global__ void DelaunayPrepKernel(const int2* __restrict__ uv, const float* __restrict__ z,
+                                   const int32_t* __restrict__ vid, const int32_t* __restrict__ tris, int ntri,
+                                   const float* __restrict__ kinv, int W, int H, DelaunayTri* __restrict__ out) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntri) return;
+  DelaunayTri d;
+  float c[3][3];
+  int idx[3];
+  for (int k = 0; k < 3; ++k) {
+    idx[k] = tris[3 * t + k];
+    const int p = vid[idx[k]];
+    d.x[k] = (double)uv[p].x;
+    d.y[k] = (double)uv[p].y;
+    const double zz = (double)z[p];
+    const float q[3] = {(float)(d.x[k] * zz), (float)(d.y[k] * zz), (float)zz};
+    for (int r = 0; r < 3; ++r) c[k][r] = Dot3f(kinv + 3 * r, q);
+  }
+  const float e1[3] = {c[1][0] - c[0][0], c[1][1] - c[0][1], c[1][2] - c[0][2]};
+  const float e2[3] = {c[2][0] - c[0][0], c[2][1] - c[0][1], c[2][2] - c[0][2]};
+  float nn[3] = {e2[1] * e1[2] - e2[2] * e1[1], e2[2] * e1[0] - e2[0] * e1[2], e2[0] * e1[1] - e2[1] * e1[0]};
+  const float sq = Dot3f(nn, nn);
+  if (sq > 0.0f) {  // Eigen's normalized(): divide by the norm when it is not 0
+    const float nrm = sqrtf(sq);
+    nn[0] = nn[0] / nrm; nn[1] = nn[1] / nrm; nn[2] = nn[2] / nrm;
+  }
+  const float inv = 1.0f / Dot3f(nn, c[0]);
+  for (int r = 0; r < 3; ++r) { d.n[r] = nn[r]; d.np[r] = nn[r] * inv; }
+  const double umin = fmin(d.x[0], fmin(d.x[1], d.x[2])), umax = fmax(d.x[0], fmax(d.x[1], d.x[2]));
+  const double vmin = fmin(d.y[0], fmin(d.y[1], d.y[2])), vmax = fmax(d.y[0], fmax(d.y[1], d.y[2]));
+  d.u0 = max(0, (int)umin); d.u1 = min(W - 1, (int)umax);
+  d.v0 = max(0, (int)vmin); d.v1 = min(H - 1, (int)vmax);
+  // A pixel on an edge shared by two triangles is written by both in the
+  // reference, the later face in CGAL's face order last. The triangle with the
+  // largest sorted vertex triple writes it here, whatever the list order.
+  int a = idx[0], b = idx[1], e = idx[2];
+  if (a < b) { const int t2 = a; a = b; b = t2; }
+  if (b < e) { const int t2 = b; b = e; e = t2; }
+  if (a < b) { const int t2 = a; a = b; b = t2; }
+  d.key = ((unsigned long long)a << 42) | ((unsigned long long)b << 21) | (unsigned long long)e;
+  d.key += 1ull;
+  out[t] = d;
+}
+
+__device__ __forceinline__ bool InsideTri(const DelaunayTri& d, int u, int v) {
+  // :451-461 with Vector2d edges v1 = i1 - i0, v2 = i2 - i1, v3 = i0 - i2.
+  const double m1 = (d.x[1] - d.x[0]) * ((double)v - d.y[0]) - ((double)u - d.x[0]) * (d.y[1] - d.y[0]);
+  const double m2 = (d.x[2] - d.x[1]) * ((double)v - d.y[1]) - ((double)u - d.x[1]) * (d.y[2] - d.y[1]);
+  const double m3 = (d.x[0] - d.x[2]) * ((double)v - d.y[2]) - ((double)u - d.x[2]) * (d.y[0] - d.y[2]);
+  return m1 >= 0 && m2 >= 0 && m3 >= 0;
+}
+
+__global__ void DelaunayClaimKernel(const DelaunayTri* __restrict__ tri, int ntri, int W,
+                                    unsigned long long* __restrict__ owner) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntri) return;
+  const DelaunayTri d = tri[t];
+  for (int v = d.v0; v <= d.v1; ++v)
+    for (int u = d.u0; u <= d.u1; ++u)
+      if (InsideTri(d, u, v)) atomicMax(owner + (size_t)v * W + u, d.key);
+}
+
+__global__ void DelaunayWriteKernel(const DelaunayTri* __restrict__ tri, int ntri, int W, int H,
+                                    const unsigned long long* __restrict__ owner, const float* __restrict__ kinv,
+                                    float* __restrict__ depth, float* __restrict__ normal) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ntri) return;
+  const DelaunayTri d = tri[t];
+  const size_t wh = (size_t)W * H;
+  for (int v = d.v0; v <= d.v1; ++v)
+    for (int u = d.u0; u <= d.u1; ++u) {
+      const size_t p = (size_t)v * W + u;
+      if (owner[p] != d.key || !InsideTri(d, u, v)) continue;
+      const float q[3] = {(float)u, (float)v, 1.0f};
+      float xc[3];
+      for (int r = 0; r < 3; ++r) xc[r] = Dot3f(kinv + 3 * r, q);
+      depth[p] = 1.0f / Dot3f(d.np, xc);
+      normal[p] = d.n[0];
+      normal[wh + p] = d.n[1];
+      normal[2 * wh + p] = d.n[2];
+    }
+}
+
 __global__ void FillKernel(uint32_t* __restrict__ p, size_t n, uint32_t v) {
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
 }
@@ -512,6 +637,75 @@ int smvs_init_depth_from_sparse_points(const smvs_view* view, const float* xyz, 
   if (num_points) SparseSplatKernel<<<Grid(num_points), 256, 0, call.stream>>>(c, d_xyz, num_points, key, range);
   SparseResolveKernel<<<Grid(wh), 256, 0, call.stream>>>(key, wh, d_depth, d_normal);
   IM_CUDA(cudaGetLastError());
+  return Finish(&call, view, d_depth, d_normal, depth, normal, range, depth_range, true);
+}
+
+int smvs_init_depth_from_delaunay(const smvs_view* view, const float* xyz, size_t num_points, int memory,
+                                  float* depth, float* normal, float* depth_range, void* stream) {
+  int st = Check(view, memory, depth, normal);
+  if (st) return st;
+  if (num_points && !xyz) return Fail(SMVS_EINVAL, "init maps: null points");
+  if (num_points >= ((size_t)1 << 21)) return Fail(SMVS_EINVAL, "init maps: at most 2^21 - 1 points per view");
+  Call call;
+  if ((st = Begin(memory, stream, &call))) return st;
+  const size_t wh = (size_t)view->width * view->height;
+  const float* d_xyz;
+  float *d_depth, *d_normal, *d_z;
+  int2* d_uv;
+  uint32_t* range;
+  if ((st = call.In(xyz, num_points * 3, &d_xyz))) return st;
+  if ((st = Outputs(&call, view, depth, normal, &d_depth, &d_normal))) return st;
+  if ((st = call.Alloc(&d_uv, std::max<size_t>(num_points, 1) * sizeof(int2))) ||
+      (st = call.Alloc(&d_z, std::max<size_t>(num_points, 1) * sizeof(float))) || (st = call.Alloc(&range, 8)))
+    return st;
+  const Cam c = MakeCam(*view);
+  const uint32_t r0[2] = {FKey(FLT_MAX), FKey(FLT_EPSILON)};
+  IM_CUDA(cudaMemcpyAsync(range, r0, 8, cudaMemcpyHostToDevice, call.stream));
+  IM_CUDA(cudaMemsetAsync(d_depth, 0, wh * 4, call.stream));
+  IM_CUDA(cudaMemsetAsync(d_normal, 0, wh * 12, call.stream));
+  std::vector<int2> uv(num_points);
+  if (num_points) {
+    ProjectUvdKernel<<<Grid(num_points), 256, 0, call.stream>>>(c, d_xyz, num_points, d_uv, d_z, range);
+    IM_CUDA(cudaGetLastError());
+    IM_CUDA(cudaMemcpyAsync(uv.data(), d_uv, num_points * sizeof(int2), cudaMemcpyDeviceToHost, call.stream));
+    IM_CUDA(cudaStreamSynchronize(call.stream));
+  }
+  // The points that landed in the image, in input order, and the Delaunay
+  // triangulation of their pixel positions (host).
+  std::vector<int32_t> vid, xy, tris;
+  for (size_t i = 0; i < num_points; ++i)
+    if (uv[i].x >= 0) {
+      vid.push_back((int32_t)i);
+      xy.push_back(uv[i].x);
+      xy.push_back(uv[i].y);
+    }
+  if ((st = smvs::DelaunayTriangulate(xy.data(), (int)vid.size(), tris))) return st;
+  const int ntri = (int)(tris.size() / 3);
+  if (ntri > 0) {
+    float kinv[9];
+    for (int k = 0; k < 9; ++k) kinv[k] = (float)c.Kinv[k];
+    int32_t *d_vid, *d_tris;
+    float* d_kinv;
+    DelaunayTri* d_tri;
+    unsigned long long* owner;
+    if ((st = call.Alloc(&d_vid, vid.size() * 4)) || (st = call.Alloc(&d_tris, tris.size() * 4)) ||
+        (st = call.Alloc(&d_kinv, sizeof(kinv))) || (st = call.Alloc(&d_tri, (size_t)ntri * sizeof(DelaunayTri))) ||
+        (st = call.Alloc(&owner, wh * sizeof(unsigned long long))))
+      return st;
+    IM_CUDA(cudaMemcpyAsync(d_vid, vid.data(), vid.size() * 4, cudaMemcpyHostToDevice, call.stream));
+    IM_CUDA(cudaMemcpyAsync(d_tris, tris.data(), tris.size() * 4, cudaMemcpyHostToDevice, call.stream));
+    IM_CUDA(cudaMemcpyAsync(d_kinv, kinv, sizeof(kinv), cudaMemcpyHostToDevice, call.stream));
+    IM_CUDA(cudaMemsetAsync(owner, 0, wh * sizeof(unsigned long long), call.stream));
+    const int blocks = (ntri + 127) / 128;
+    DelaunayPrepKernel<<<blocks, 128, 0, call.stream>>>(d_uv, d_z, d_vid, d_tris, ntri, d_kinv, view->width,
+                                                         view->height, d_tri);
+    DelaunayClaimKernel<<<blocks, 128, 0, call.stream>>>(d_tri, ntri, view->width, owner);
+    DelaunayWriteKernel<<<blocks, 128, 0, call.stream>>>(d_tri, ntri, view->width, view->height, owner, d_kinv,
+                                                          d_depth, d_normal);
+    IM_CUDA(cudaGetLastError());
+    // The host vectors die at return: the uploads must be done first.
+    IM_CUDA(cudaStreamSynchronize(call.stream));
+  }
   return Finish(&call, view, d_depth, d_normal, depth, normal, range, depth_range, true);
 }
 

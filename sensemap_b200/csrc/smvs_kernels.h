@@ -47,6 +47,15 @@ struct alignas(16) JobParams {
   const float* ref_sqsum;  // W*H
   const float* grad;       // W*H
   const float* poses;      // N*43
+  // Prior maps of the sweep (SweepOptions::prior_depth_ncc / propagate_depth,
+  // kernel_functions.h:109-110). prior_mode 0: none; 1: has_prior_depth (the
+  // given depth and normal weight every cost, kernel_functions.cu:1470-1486);
+  // 2: propagate_depth (the projected median depth; normals and weights read
+  // as 0). A NULL normal or weight map reads as 0.
+  int prior_mode;
+  const float* prior_depth;   // W*H
+  const float* prior_normal;  // 3*W*H planar
+  const float* prior_wgt;     // W*H
   cudaTextureObject_t src_tex[SMVS_MAX_SRC];
   cudaTextureObject_t dep_tex[SMVS_MAX_SRC];
 };
@@ -121,6 +130,15 @@ cudaError_t LaunchConvertImage(const void* in, int in_format, size_t in_stride, 
                                int out_storage, size_t out_pitch, int normalise, cudaStream_t stream);
 cudaError_t LaunchPrepRef(const JobParams& p, float* ref_sum, float* ref_sqsum, float* grad, cudaStream_t stream);
 cudaError_t LaunchInit(const JobParams& p, int random_init, float opt_dmin, float opt_dmax, cudaStream_t stream);
+// Propagate-depth initial maps (InitWorkspace, patch_match_cuda.cu:603-659):
+// projects the depth map of every source with a map (src_depth[i], pitched
+// device memory of row pitch src_pitch[i]; NULL = none) into `composite`
+// (N*W*H floats of scratch), writes the median depths into p.depth where it is
+// <= 0 and the consistent medians into `prior` (W*H, cleared first), then fits
+// p.normal to p.depth. src_w/src_h: the sources' sizes (the projection grid is
+// the largest of them).
+cudaError_t LaunchPropagateInit(const JobParams& p, const int* src_w, const int* src_h, const float* const* src_depth,
+                                const size_t* src_pitch, float* composite, float* prior, cudaStream_t stream);
 // Batched checkerboard kernels: every job of `b` in one launch.
 cudaError_t LaunchInitConf(const Batch& b, cudaStream_t stream);
 cudaError_t LaunchSweep(const Batch& b, int colour, cudaStream_t stream);

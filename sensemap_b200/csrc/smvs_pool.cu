@@ -534,6 +534,8 @@ int smvs_pool_submit(smvs_pool* P, const smvs_options* o, int64_t ref_id, const 
   if (st) return st;
   if (o->median_filter || o->conf_filter || o->est_curvature)
     return Fail(SMVS_EINVAL, "pool jobs do not run the median/confidence filters or curvature; use smvs_create");
+  if (o->has_prior_depth || o->propagate_depth)
+    return Fail(SMVS_EINVAL, "pool jobs do not take prior or propagated depth maps; use smvs_create");
   if (n < 1 || n > SMVS_MAX_SRC) return Fail(SMVS_EINVAL, "num_src=%d outside 1..%d", n, SMVS_MAX_SRC);
   auto rv = P->views.find(ref_id);
   if (rv == P->views.end()) return Fail(SMVS_EINVAL, "reference view %lld is not resident", (long long)ref_id);

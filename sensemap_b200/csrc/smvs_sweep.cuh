@@ -273,19 +273,69 @@ struct PixRef {
   int ws;
 };
 
+// A pixel's prior (SweepOptions::prior_depth_ncc / propagate_depth): depth w,
+// normal xyz and weight, read where the reference reads them
+// (kernel_functions.cu:1533-1543, 2188-2200); a NULL map reads as 0.
+struct PriorInfo {
+  float x, y, z, w, wgt;
+};
+
+__device__ __forceinline__ PriorInfo LoadPrior(const JobParams& p, size_t pix) {
+  PriorInfo pi = {0.f, 0.f, 0.f, 0.f, 0.f};
+  if (p.prior_mode == 0) return pi;
+  const size_t WH = (size_t)p.W * p.H;
+  pi.w = p.prior_depth[pix];
+  if (p.prior_normal) {
+    pi.x = p.prior_normal[pix];
+    pi.y = p.prior_normal[WH + pix];
+    pi.z = p.prior_normal[2 * WH + pix];
+  }
+  if (p.prior_wgt) pi.wgt = p.prior_wgt[pix];
+  return pi;
+}
+
+// The factor ComputeMultiViewCostVector applies to every NCC cost of a
+// hypothesis (kernel_functions.cu:1470-1478): ComputeNCCWeightFromPrior
+// (:316-340), which lowers the cost of hypotheses near the prior depth and
+// normal, times 1 - 0.3 wgt for a weight strictly between 0 and 1. It is 1
+// unless the job has a prior depth and normal (mode 1) and the pixel's prior
+// depth is above FLT_EPSILON. The reference's mixed float/double arithmetic is
+// kept: the colour-variance term and the factors are double, the exponentials
+// of the depth and angle terms single precision.
+__device__ __forceinline__ float PriorWeight(const JobParams& p, const PriorInfo& pi, const float h[3], float hd,
+                                             float rvar) {
+  if (p.prior_mode != 1 || !(pi.w > FLT_EPSILON)) return 1.0f;
+  float regu = 1.0f;
+  const float sigma2 = (float)(0.5 - 0.4 * exp(-10000.0 * (double)fabsf(rvar)));
+  const float dd = hd - pi.w;
+  const float dd2 = fmaxf(dd * dd, 0.05f * 0.05f);
+  regu = (float)((double)regu * fmax(1.0 - 0.2 * (double)__expf(-dd2 / sigma2), 0.01));
+  const float pn = pi.x * pi.x + pi.y * pi.y + pi.z * pi.z;
+  if ((double)pn > 0.8 && (double)pn < 1.25) {
+    const float ct = pi.x * h[0] + pi.y * h[1] + pi.z * h[2];
+    const float dt2 = (1.0f - ct) * (1.0f - ct);
+    regu = (float)((double)regu * fmax(1.0 - 0.54 * (double)__expf(-dt2 / sigma2), 0.01));
+  }
+  if ((double)pi.wgt < 1.0 && (double)pi.wgt > 0.0) regu = (float)((double)regu * (1.0 - (double)pi.wgt * 0.3));
+  return regu;
+}
+
+// Cost of one hypothesis on source view v: the NCC cost times the prior
+// factor pw (1 without a prior), plus the weighted geometric term.
 template <int R, int S, int G>
 __device__ __forceinline__ float ViewCost(const JobParams& p, const float* poses, int v, int row, int col,
                                           float depth, const float n[3], const float np[3], const PixRef& pr,
-                                          const float* Kgeom, int lane, unsigned gmask) {
+                                          const float* Kgeom, int lane, unsigned gmask, float pw = 1.0f) {
   const float* pose = poses + v * SMVS_POSE_FLOATS;
   float cost = NccCost<R, S, G>(p.src_tex[v], pose, row, col, depth, n, p.refiK, p.W, p.H, pr.center, pr.rsum,
                                 pr.rvar, pr.win, pr.ws, p.sn, p.cn, lane, gmask);
+  if (pw != 1.0f) cost *= pw;  // keeps the no-prior arithmetic (and any contraction) unchanged
   if (p.geom)
     cost += p.geom_reg * GeomCost(pose, p.dep_tex[v], (float)row, (float)col, depth, np, Kgeom, p.geom_max);
   return cost;
 }
 
-// InitConfMapKernel, kernel_functions.cu:1497-1601 (no prior). One thread per
+// InitConfMapKernel, kernel_functions.cu:1497-1601. One thread per
 // pixel; the cost vector and its sort order live in shared memory
 // ([view][pixel], nb views per pixel).
 template <int R, int S>
@@ -320,10 +370,11 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   const float n[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
   const float depth = p.depth[pix];
   const unsigned gmask = GroupMask<1>();
+  const float pw = PriorWeight(p, LoadPrior(p, pix), n, depth, pr.rvar);
 #define C_(v) costs[(v) * kThreads + t]
 #define O_(v) order[(v) * kThreads + t]
   for (int v = 0; v < p.N; ++v) {
-    const float c = ViewCost<R, S, 1>(p, poses, v, row, col, depth, n, np, pr, p.refK, 0, gmask);
+    const float c = ViewCost<R, S, 1>(p, poses, v, row, col, depth, n, np, pr, p.refK, 0, gmask, pw);
     C_(v) = c;
     O_(v) = v;
     p.cost[(size_t)v * WH + pix] = c;
@@ -356,10 +407,9 @@ struct SweepSmem {
   float* PR;  // [nb][P]           view probabilities, then their CDF
 };
 
-// SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560 (no prior, no
-// propagate_depth): one checkerboard colour, G threads per pixel.
 // Threads-per-pixel 1: the thread-per-pixel form of SweepFromCheckerBoardOpt
-// (kernel_functions.cu:2136-2560) and LocalOptimization (:2736-2931). The
+// (kernel_functions.cu:2136-2560, with the prior and propagate-depth paths)
+// and LocalOptimization (:2736-2931). The
 // pixel's cost matrix M[kMaxHyp][NB], its hypotheses and view weights are
 // per-thread arrays (NB = the view bucket): the compiler keeps them in the
 // thread's local frame, which lives in the L1 next to the texture cache the
@@ -400,10 +450,13 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
   float depth = p.depth[pix];
   float normal[3] = {p.normal[pix], p.normal[WH + pix], p.normal[2 * WH + pix]};
   const float grad = p.grad[pix];
+  const PriorInfo pri = LoadPrior(p, pix);
+  // A prior depth narrows the random normal perturbation (:2201-2203, 2213-2214).
+  const float prf = (p.prior_mode == 1 && (double)pri.w > 1e-6) ? 0.1f : 1.0f;
   const float depth_min = p.depth_min;
   const float depth_max = (float)(1.2 * (double)p.depth_max);  // [quirk] :2213
-  const float a1 = fminf(p.rand_a1, (float)(180.0 * 0.0174532925199432));
-  const float a2 = fminf(p.rand_a2, (float)(90.0 * 0.0174532925199432));
+  const float a1 = fminf(p.rand_a1 * prf, (float)(180.0 * 0.0174532925199432));
+  const float a2 = fminf(p.rand_a2 * prf, (float)(90.0 * 0.0174532925199432));
   const float* iK = p.refiK;
   const float vd[3] = {iK[0] * col + iK[1], iK[2] * row + iK[3], 1.0f};
   const float ivl = rsqrtf(vd[0] * vd[0] + vd[1] * vd[1] + vd[2] * vd[2]);
@@ -450,7 +503,11 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
     for (int s = 0; s < 10; ++s) {
       const int nr = row + kDirSamples[k][2 * s], nc = col + kDirSamples[k][2 * s + 1];
       if (nr < 0 || nr >= H || nc < 0 || nc >= W) continue;
-      const float nconf = p.conf[(size_t)nr * W + nc];
+      float nconf = p.conf[(size_t)nr * W + nc];
+      if (p.prior_mode != 0 && p.prior_wgt) {  // PRIOR_WGT_PROGET, :2292-2304
+        const float pws = p.prior_wgt[(size_t)nr * W + nc];
+        if ((double)pws > 1e-6) nconf = (float)((double)nconf * (1.0 - 0.2 * (double)pws));
+      }
       if (best > nconf) { br = nr; bc = nc; best = nconf; }
     }
     if (best < FLT_MAX) {
@@ -477,8 +534,11 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
   // the propagated hypotheses 1..ns-1, phase 1 the refinement hypotheses 1..4.
   int h_end = ns;
   for (int phase = 0; phase < 2; ++phase) {
-    for (int h = 1; h < h_end; ++h)
-      for (int v = 0; v < N; ++v) M[h][v] = ViewCost<R, S, 1>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr, p.refK, 0, gmask);
+    for (int h = 1; h < h_end; ++h) {
+      const float pw = PriorWeight(p, pri, hyp[h], hyp[h][3], pr.rvar);
+      for (int v = 0; v < N; ++v)
+        M[h][v] = ViewCost<R, S, 1>(p, poses, v, row, col, hyp[h][3], hyp[h], vd, pr, p.refK, 0, gmask, pw);
+    }
     if (phase == 1) break;
 
     // ACMM view selection, :2364-2427.
@@ -528,7 +588,15 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
     }
     p.view_sel[pix] = sel;
     int mi = -1;
-    {
+    if (p.prior_mode == 1 && pri.w > 0.0f) {
+      // FindMinCostWithin (:661-671) over the band the prior allows
+      // (:2431-2437; [quirk] the lower end is min(0.95 w - 0.05, 0)).
+      const float lo = (float)fmin((double)(pri.w * 0.95f) - 0.05, 0.0);
+      const float hi = (float)((double)(pri.w * 1.05f) + 0.05);
+      float m = FLT_MAX;
+      for (int h = 0; h < ns; ++h)
+        if (costs[h] <= m && hyp[h][3] >= lo && hyp[h][3] <= hi) { m = costs[h]; mi = h; }
+    } else {
       float m = FLT_MAX;
       for (int h = 0; h < ns; ++h)
         if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
@@ -545,7 +613,10 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
     const float ndepth = r.Uniform() * (pd_max - pd_min) + pd_min;  // PerturbDepth :141-147
     PerturbNormalACMH(normal, nn, a1, a2, r);
     CorrectNormal(nn, vd, ivl);
-    const float rdepth = r.Uniform() * (depth_max - depth_min) + depth_min;
+    // With propagate_depth a pixel that has a prior depth gets no random
+    // depth hypothesis (:2467-2486).
+    const bool rand_depth = !(p.prior_mode == 2 && pri.w > 0.0f);
+    const float rdepth = rand_depth ? r.Uniform() * (depth_max - depth_min) + depth_min : 0.0f;
     float rn[3];
     RandomNormal(r, vd, rn);
     CorrectNormal(rn, vd, ivl);
@@ -554,10 +625,10 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
     hyp[2][0] = normal[0]; hyp[2][1] = normal[1]; hyp[2][2] = normal[2]; hyp[2][3] = ndepth;
     hyp[3][0] = rn[0]; hyp[3][1] = rn[1]; hyp[3][2] = rn[2]; hyp[3][3] = depth;
     hyp[4][0] = normal[0]; hyp[4][1] = normal[1]; hyp[4][2] = normal[2]; hyp[4][3] = rdepth;
-    h_end = 5;
+    h_end = rand_depth ? 5 : 4;
   }
   // :2488-2559: weighted refinement costs, argmin, write back.
-  for (int h = 0; h < 5; ++h) {
+  for (int h = 0; h < h_end; ++h) {
     float cs = 0.f;
     for (int v = 0; v < N; ++v) cs += vw[v] * M[h][v];
     costs[h] = cs;
@@ -565,7 +636,7 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
   int mi = -1;
   {
     float m = FLT_MAX;
-    for (int h = 0; h < 5; ++h)
+    for (int h = 0; h < h_end; ++h)
       if (costs[h] <= m) { m = costs[h]; mi = h; }
   }
   if (mi != -1) {
@@ -687,6 +758,9 @@ struct SweepOccupancy {
   static constexpr int kBlocks = G == 4 ? 3 : 2;
 };
 
+// SweepFromCheckerBoardOpt, kernel_functions.cu:2136-2560, G threads per
+// pixel, without the prior and propagate-depth paths: jobs with a prior run
+// the thread-per-pixel kernel (the launch shape never changes results).
 template <int R, int S, int G>
 __global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) SweepKernel(const Batch b, int colour) {
   extern __shared__ float smem[];

@@ -132,6 +132,26 @@ class StereoFusion:
         N.check(N.lib().smvs_fusion_run(self._handle()))
         self._points = None
 
+    def RemoveDuplicatePoints(self) -> int:
+        """StereoFusion::RemoveDuplicatePoints (fusion.cc:2184-2266), which the
+        reference's Run applies after the image loop when
+        Options::remove_duplicate_pnts (its default). Returns the points dropped."""
+        n = C.c_size_t()
+        N.check(N.lib().smvs_fusion_remove_duplicate_points(self._handle(), C.byref(n)))
+        self._points = None
+        return int(n.value)
+
+    def RemoveOutliers(self, nb_neighbors: int = 6, max_spacing_factor: float = 6.0) -> int:
+        """StereoFusion::RemoveOutliers (fusion.cc:2542-2611), applied by the
+        reference's Run when Options::outlier_removal (off by default); the
+        defaults are Options::nb_neighbors and max_spacing_factor. Returns the
+        points dropped; the remaining points' scores are updated."""
+        n = C.c_size_t()
+        N.check(N.lib().smvs_fusion_remove_outliers(self._handle(), int(nb_neighbors), float(max_spacing_factor),
+                                                     C.byref(n)))
+        self._points = None
+        return int(n.value)
+
     def _fetch(self):
         if self._points is None:
             npts, nvis = C.c_size_t(), C.c_size_t()

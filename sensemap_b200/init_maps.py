@@ -4,7 +4,8 @@ Mirrors the map builders PatchMatchController runs before a PatchMatch pass
 (src/controllers/patch_match_controller.cc): ``InitDepthMap`` (:1205-1307,
 sparse points the view observes, splatted by InitDepthMapFromSparsePoint
 :483-518), ``Model2Depth`` (:520-642, a triangle mesh) and ``Ply2Depth``
-(:643-750, oriented dense points). Each returns ``(depth, normal,
+(:643-750, oriented dense points), and the Delaunay variant of InitDepthMap
+(InitDepthMapFromDelaunay :398-474). Each returns ``(depth, normal,
 depth_range)``: depth H x W, normal 3 x H x W, and the (first, second) pair
 the reference returns. Inputs may be numpy arrays (host) or CUDA tensors
 (device; outputs are then CUDA tensors too).
@@ -68,6 +69,31 @@ def init_depth_from_sparse_points(width, height, K, R, T, xyz, stream=None):
         C.byref(_view(width, height, K, R, T)), p, int(keep[0].shape[0]), N.MEM_DEVICE if dev else N.MEM_HOST,
         dp, np_, rng, C.c_void_p(int(stream)) if stream is not None else None))
     return d, n, (rng[0], rng[1])
+
+
+def init_depth_from_delaunay(width, height, K, R, T, xyz, stream=None):
+    """InitDepthMap with init_from_delaunay: the points the view observes,
+    triangulated over their pixel positions (InitDepthMapFromDelaunay)."""
+    dev, keep, (p,) = _prep([np.asarray(xyz).reshape(-1, 3) if not _is_cuda_tensor(xyz) else xyz.reshape(-1, 3)],
+                            [np.float32])
+    d, n, dp, np_ = _outputs(dev, height, width)
+    rng = (C.c_float * 2)()
+    N.check(N.lib().smvs_init_depth_from_delaunay(
+        C.byref(_view(width, height, K, R, T)), p, int(keep[0].shape[0]), N.MEM_DEVICE if dev else N.MEM_HOST,
+        dp, np_, rng, C.c_void_p(int(stream)) if stream is not None else None))
+    return d, n, (rng[0], rng[1])
+
+
+def delaunay_triangles(xy) -> np.ndarray:
+    """The triangulation the Delaunay initial map uses: (m, 3) counter-clockwise
+    vertex indices into the (n, 2) integer positions `xy` (host)."""
+    xy = np.ascontiguousarray(xy, dtype=np.int32).reshape(-1, 2)
+    cap = 2 * len(xy) + 8
+    out = np.zeros((cap, 3), np.int32)
+    cnt = C.c_int()
+    N.check(N.lib().smvs_test_delaunay(xy.ctypes.data if len(xy) else None, len(xy), out.ctypes.data, cap,
+                                       C.byref(cnt)))
+    return out[:cnt.value].copy()
 
 
 def init_depth_from_mesh(width, height, K, R, T, vertices, faces, face_normals, stream=None):

@@ -107,6 +107,7 @@ class Problem:
     src_image_scales: Sequence[float] = field(default_factory=list)
     mask: Optional[object] = None  # H x W uint8 mask of the reference view
     src_image_extend_idxs: Sequence[int] = field(default_factory=list)  # cross-filter neighbours (:314)
+    prior_wgt: Optional[object] = None  # H x W prior weights of the reference view (prior_wgt_maps, :333)
 
 
 class DeviceBuffer:
@@ -207,6 +208,12 @@ def _problem_struct(problem: Problem):
         keep.append(o)
         memories.add(d)
         prob.ref_mask = p
+    if problem.prior_wgt is not None:
+        w = problem.prior_wgt if _is_cuda_tensor(problem.prior_wgt) else np.asarray(problem.prior_wgt, dtype=np.float32)
+        p, o, d = _addr(w)
+        keep.append(o)
+        memories.add(d)
+        prob.ref_prior_wgt = p
     if len(memories) > 1:
         raise N.SmvsError(N.SMVS_EINVAL, "all images and maps must live in the same memory (host or device)")
     prob.memory = N.MEM_DEVICE if memories == {True} else N.MEM_HOST

@@ -48,7 +48,7 @@ def test_defaults_match_reference():
 
 
 @pytest.mark.parametrize("field,value", [("window_radius", 6), ("window_step", 3), ("thk", 5), ("thk", 0),
-                                         ("depth_min", -1.0), ("has_prior_depth", True), ("image_storage", 7),
+                                         ("depth_min", -1.0), ("propagate_depth", True), ("image_storage", 7),
                                          ("num_samples", 0)])
 def test_options_check_rejects(field, value):
     o = PatchMatchOptions(depth_min=1.0, depth_max=10.0)
@@ -58,6 +58,24 @@ def test_options_check_rejects(field, value):
         o.check()
     assert ei.value.status == N.SMVS_EINVAL
     assert N.last_error()
+
+
+def test_prior_option_combinations():
+    """has_prior_depth alone is valid; propagate_depth needs given maps
+    (init_depth_random = 0) and no geometric pass, and excludes has_prior_depth
+    (patch_match_cuda.cu:946-947)."""
+    o = PatchMatchOptions(depth_min=1.0, depth_max=10.0, has_prior_depth=True)
+    o.check()
+    o = PatchMatchOptions(depth_min=1.0, depth_max=10.0, propagate_depth=True, geom_consistency=False,
+                          init_depth_random=False)
+    o.check()
+    for bad in (dict(has_prior_depth=True), dict(init_depth_random=True), dict(geom_consistency=True)):
+        q = PatchMatchOptions(depth_min=1.0, depth_max=10.0, propagate_depth=True, geom_consistency=False,
+                              init_depth_random=False)
+        for k, v in bad.items():
+            setattr(q, k, v)
+        with pytest.raises(N.SmvsError):
+            q.check()
 
 
 def test_mat_roundtrip(tmp_path):
