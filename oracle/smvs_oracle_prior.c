@@ -33,7 +33,9 @@ static void project_depth(const float* sdepth, int sw, int sh, int grid_w, int g
                          (double)texel(sdepth, sw, sh, col - 1, row) + (double)texel(sdepth, sw, sh, col, row);
       const float depth = (float)(sum * 0.25);
       if (depth < 1e-6f) continue;
-      const float c = (float)col * depth, r = (float)row * depth;
+      /* [quirk] kernel_functions.cu:803-804 stores the products back into the int
+       * pixel indices (col *= depth), truncating them toward zero. */
+      const float c = (float)(int)((float)col * depth), r = (float)(int)((float)row * depth);
       const float bx = iP[0] * c + iP[1] * r + iP[2] * depth + iP[3];
       const float by = iP[4] * c + iP[5] * r + iP[6] * depth + iP[7];
       const float bz = iP[8] * c + iP[9] * r + iP[10] * depth + iP[11];

@@ -43,7 +43,9 @@ __global__ void ProjectDepthKernel(const float* __restrict__ sdepth, size_t spit
   const float depth = (float)(sum * 0.25);
   if (depth < 1e-6f) return;
   const float* iP = pose + 31;  // P^-1, 3x4 row-major
-  const float c = (float)col * depth, r = (float)row * depth;
+  // [quirk] kernel_functions.cu:803-804 stores the products back into the int
+  // pixel indices (col *= depth), truncating them toward zero.
+  const float c = (float)(int)((float)col * depth), r = (float)(int)((float)row * depth);
   const float bx = iP[0] * c + iP[1] * r + iP[2] * depth + iP[3];
   const float by = iP[4] * c + iP[5] * r + iP[6] * depth + iP[7];
   const float bz = iP[8] * c + iP[9] * r + iP[10] * depth + iP[11];
