@@ -743,6 +743,12 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "serving": serving,
                 "clocks": clock_info, "autotune": tune, "accuracy": accuracy, "plain": plain,
                 "autotuned_window": autotuned, "reference_kernels": ref_k}
+        # The north star's second throughput unit: image megapixels x source
+        # views x iterations x passes per second (one depth map = 2 passes).
+        mpvi = args.width * args.height / 1e6 * (wl.V - 1) * ITERS * 2
+        line["mpix_views_iters_per_s"] = {"value": value * mpvi, "plain": plain["value"] * mpvi,
+                                          "autotuned_window": autotuned["value"] * mpvi,
+                                          "per_depth_map": mpvi}
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -132,6 +132,14 @@ void SetupTextures(const RefJob& j, Textures& t, bool with_images) {
   t.poses_tex = MakeArrayTexture(t.poses_dev->GetPtr(), cudaFilterModePoint, cudaReadModeElementType);
 }
 
+// Every pitched row cleared (the reference's GpuMat::FillWithScalar is a byte
+// cudaMemset of width * height * depth * sizeof(T) bytes from the start of a
+// pitched allocation, gpu_mat.h:240-243, which leaves the last rows of a map
+// whose pitch exceeds its row size uninitialised).
+void ClearMap(GpuMat<float>& m) {
+  CUDA_SAFE_CALL(cudaMemset2D(m.GetPtr(), m.GetPitch(), 0, m.GetWidth() * sizeof(float), m.GetHeight() * m.GetDepth()));
+}
+
 // The propagate-depth initial maps in the reference's order
 // (patch_match_cuda.cu:603-659): GenerateProjectDepthMaps per source with a
 // map, CompositeInitDepthMap, CompositeInitNormalMap. The reference launches
@@ -165,7 +173,9 @@ int PropagateInit(const RefJob& j, const Textures& t, GpuMatPRNG& rand_state, Gp
     if (cudaGetLastError() != cudaSuccess) return 20;
   }
   CUDA_SYNC_AND_CHECK();
-  prior_depth.FillWithScalar(0);
+  // The reference clears its prior map with FillWithScalar(0)
+  // (patch_match_cuda.cu:644-645); the driver clears all of it.
+  ClearMap(prior_depth);
   const dim3 g((j.W - 1) / b.x + 1, (j.H - 1) / b.y + 1);
   CompositeInitDepthMap<<<g, b>>>(rand_state, depth_map, prior_depth, composite, j.depth_min, j.depth_max);
   if (cudaGetLastError() != cudaSuccess) return 21;
@@ -206,10 +216,10 @@ extern "C" int ref_run(const RefJob* jp, RefOut* out) {
     prior_depth.CopyToDevice(j.init_depth, W * sizeof(float));
     prior_normal.CopyToDevice(j.init_normal, W * sizeof(float));
     if (j.prior_wgt) prior_wgt.CopyToDevice(j.prior_wgt, W * sizeof(float));
-    else prior_wgt.FillWithScalar(0);
+    else ClearMap(prior_wgt);
   } else if (j.prior_mode == 2) {
-    prior_normal.FillWithScalar(0);
-    prior_wgt.FillWithScalar(0);
+    ClearMap(prior_normal);
+    ClearMap(prior_wgt);
   }
   dim3 eb(THREADS_PER_BLOCK, THREADS_PER_BLOCK), eg((W - 1) / THREADS_PER_BLOCK + 1, (H - 1) / THREADS_PER_BLOCK + 1);
   // The reference launches InitDepthMap / InitNormalMap with 32x32 blocks

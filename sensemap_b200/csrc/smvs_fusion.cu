@@ -2428,7 +2428,9 @@ int smvs_fusion_remove_duplicate_points(smvs_fusion* f, size_t* num_removed) {
   // the pixel they project to in each of their images; a point meeting an
   // occupant seen by more images is dropped (and looks no further), otherwise
   // it takes the pixel and the occupant is dropped.
-  std::vector<std::vector<int64_t>> occ(f->num_views);
+  // Occupants as int32 like the reference's Mat<int> (fewer than 2^31 points:
+  // the views hold fewer than 2^31 pixels).
+  std::vector<std::vector<int32_t>> occ(f->num_views);
   for (int v = 0; v < f->num_views; ++v)
     occ[v].assign((size_t)f->views[v].width * (size_t)f->views[v].height, -1);
   const size_t n = c.pts.size();
@@ -2442,9 +2444,9 @@ int smvs_fusion_remove_duplicate_points(smvs_fusion* f, size_t* num_removed) {
       int u, w;
       ProjectPoint(v, c.pts[i], &u, &w);
       if (u < 0 || u >= v.width || w < 0 || w >= v.height) continue;
-      int64_t& o = occ[img][(size_t)w * v.width + u];
+      int32_t& o = occ[img][(size_t)w * v.width + u];
       if (o == -1) {
-        o = (int64_t)i;
+        o = (int32_t)i;
         continue;
       }
       const uint64_t ovis = c.off[o + 1] - c.off[o];
@@ -2453,7 +2455,7 @@ int smvs_fusion_remove_duplicate_points(smvs_fusion* f, size_t* num_removed) {
         break;
       }
       removal[o] = 1;
-      o = (int64_t)i;
+      o = (int32_t)i;
     }
   }
   std::vector<uint8_t> keep(n);
