@@ -27,12 +27,21 @@ pytestmark = pytest.mark.gpu
 needs_ref = pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
 
 
-def _propagate_problem(sc, drop=()):
+def _propagate_problem(sc, drop=(), crop=None):
+    """Propagate-depth problem: zero given maps for the reference, the sources'
+    exact depth maps (none for the views in `drop`); crop = (view, h, w) keeps
+    only the top-left h x w of that source (same K), a smaller source."""
     r = sc.ref_index
     H, W = sc.views[r].depth_gt.shape
     depths = [None if i in drop else v.depth_gt for i, v in enumerate(sc.views)]
     zero = (np.zeros((H, W), np.float32), np.zeros((3, H, W), np.float32))
-    return problem_from_scene(sc, depth_maps=depths, init=zero)
+    prob = problem_from_scene(sc, depth_maps=depths, init=zero)
+    if crop is not None:
+        k, h, w = crop
+        v = prob.images[k]
+        v.image = np.ascontiguousarray(np.asarray(v.image)[:h, :w])
+        v.depth = np.ascontiguousarray(np.asarray(v.depth)[:h, :w])
+    return prob
 
 
 def _engine_init(opt, prob):
@@ -53,10 +62,10 @@ def _engine(opt, prob):
                 "view_sel": pm.GetViewSelMap()}
 
 
-@pytest.mark.parametrize("seed,drop", [(41, ()), (42, (1,))])
-def test_propagate_init_bit_exact_with_oracle(seed, drop):
+@pytest.mark.parametrize("seed,drop,crop", [(41, (), None), (42, (1,), None), (48, (), (2, 90, 130))])
+def test_propagate_init_bit_exact_with_oracle(seed, drop, crop):
     sc = small_planes(seed=seed)
-    prob = _propagate_problem(sc, drop=drop)
+    prob = _propagate_problem(sc, drop=drop, crop=crop)
     opt = photometric_options(sc, iters=1, init_depth_random=False, propagate_depth=True)
     g = _engine_init(opt, prob)
     o = orc.propagate_init(prob)
