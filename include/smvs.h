@@ -322,6 +322,11 @@ int smvs_pool_submit(smvs_pool* pool, const smvs_options* opt, int64_t ref_view,
 int smvs_pool_step(smvs_pool* pool, smvs_pool_stats* stats);
 /* smvs_job_state; latency_s (may be NULL) = completion - submission for done jobs, else -1. */
 int smvs_pool_job_state(smvs_pool* pool, int64_t job_id, int* state, double* latency_s);
+/* Step the pool until job `job_id` is done or failed, or `timeout_s` seconds
+ * have passed (SMVS_ETIMEDOUT; the job keeps its place). *state (may be NULL)
+ * receives the job's last state. The smvs_wait(job, timeout) of the serving
+ * interface this library's pool provides; other jobs advance meanwhile. */
+int smvs_pool_wait(smvs_pool* pool, int64_t job_id, double timeout_s, int* state);
 /* Copy a done job's map (smvs_map_kind) to `out` (host or device). */
 int smvs_pool_get_map(smvs_pool* pool, int64_t job_id, int which, void* out);
 /* Store a done job's depth/normal as its reference view's resident maps. */

@@ -243,6 +243,7 @@ _SIGNATURES = {
                                    C.POINTER(C.c_int64)]),
     "smvs_pool_step": (C.c_int, [C.c_void_p, C.POINTER(smvs_pool_stats)]),
     "smvs_pool_job_state": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(C.c_int), C.POINTER(C.c_double)]),
+    "smvs_pool_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double, C.POINTER(C.c_int)]),
     "smvs_pool_get_map": (C.c_int, [C.c_void_p, C.c_int64, C.c_int, C.c_void_p]),
     "smvs_pool_keep_maps": (C.c_int, [C.c_void_p, C.c_int64]),
     "smvs_pool_release": (C.c_int, [C.c_void_p, C.c_int64]),

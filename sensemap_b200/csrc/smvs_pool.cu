@@ -930,6 +930,22 @@ int smvs_pool_job_state(smvs_pool* P, int64_t job_id, int* state, double* latenc
   return SMVS_OK;
 }
 
+int smvs_pool_wait(smvs_pool* P, int64_t job_id, double timeout_s, int* state) {
+  if (!P) return Fail(SMVS_EINVAL, "null pool");
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    int s = 0;
+    int st = smvs_pool_job_state(P, job_id, &s, nullptr);
+    if (st) return st;
+    if (state) *state = s;
+    if (s == kDone || s == kFailed) return SMVS_OK;
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el >= timeout_s)
+      return Fail(SMVS_ETIMEDOUT, "job %lld not done after %.3f s", (long long)job_id, timeout_s);
+    if ((st = smvs_pool_step(P, nullptr))) return st;
+  }
+}
+
 int smvs_pool_get_map(smvs_pool* P, int64_t job_id, int which, void* out) {
   if (!P || !out) return Fail(SMVS_EINVAL, "null argument");
   auto it = P->jobs.find(job_id);

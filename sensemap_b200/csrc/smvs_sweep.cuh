@@ -420,8 +420,18 @@ struct SweepSmem {
 // arithmetic is the same as the G-lane kernels (NccCost<R,S,1> sums the window
 // in the same canonical order), so maps are identical for every
 // threads-per-pixel value.
+// Resident blocks per SM the thread-per-pixel kernels ask the register
+// allocator for: at window step 2 with up to 16 views the launch is
+// latency-bound and a third block (80 registers, a few spills) is measured
+// 2-3 % faster (10 views); otherwise the allocator's own choice (128 registers,
+// two blocks) is kept (0 = no bound).
+template <int S, int NB>
+struct ThreadPixelBlocks {
+  static constexpr int kMin = (S == 2 && NB <= 16) ? 3 : 0;
+};
+
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colour) {
+__global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) SweepKernelL(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
@@ -648,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) SweepKernelL(const Batch b, int colo
 }
 
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads) LocalOptKernelL(const Batch b, int colour) {
+__global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) LocalOptKernelL(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;

@@ -96,6 +96,13 @@ class DepthMapPool:
         N.check(N.lib().smvs_pool_job_state(self._h, int(job), C.byref(st), C.byref(lat)))
         return st.value, lat.value
 
+    def wait(self, job: int, timeout_s: float) -> int:
+        """Step until the job is done or failed (smvs_pool_wait); raises
+        SmvsError(SMVS_ETIMEDOUT) after timeout_s seconds. Returns its state."""
+        st = C.c_int()
+        N.check(N.lib().smvs_pool_wait(self._h, int(job), float(timeout_s), C.byref(st)))
+        return st.value
+
     def run_until_done(self, jobs, max_steps: int = 100000) -> None:
         for _ in range(max_steps):
             if all(self.state(j)[0] == N.JOB_DONE for j in jobs):

@@ -72,6 +72,28 @@ def test_job_alone_equals_job_in_mix(scenes):
         assert_same(pool.maps(mixed), ref_maps)
 
 
+def test_wait_steps_until_done_or_times_out(scenes):
+    """smvs_pool_wait steps the pool for one job: with no time it reports
+    SMVS_ETIMEDOUT and the job keeps its place; given time it returns the job
+    done, with the maps of a job run to completion by explicit steps."""
+    sc = scenes[0]
+    opt = photometric_options(sc, iters=4, random_seed=6)
+    srcs = [i for i in range(1, len(sc.views))]
+    with DepthMapPool(max_active_jobs=2) as pool:
+        add_scene(pool, sc, 0)
+        job = pool.submit(opt, 0, srcs)
+        with pytest.raises(N.SmvsError) as ei:
+            pool.wait(job, 0.0)
+        assert ei.value.status == N.SMVS_ETIMEDOUT
+        assert pool.wait(job, 60.0) == N.JOB_DONE
+        waited = pool.maps(job)
+    with DepthMapPool(max_active_jobs=2) as pool:
+        add_scene(pool, sc, 0)
+        job = pool.submit(opt, 0, srcs)
+        pool.run_until_done([job])
+        assert_same(waited, pool.maps(job))
+
+
 def test_geometric_pass_through_pool_matches_engine(scenes):
     sc = scenes[0]
     n = len(sc.views)
