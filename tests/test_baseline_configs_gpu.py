@@ -19,7 +19,7 @@ import pytest
 
 import oracle.oracle as orc
 import oracle.ref_oracle as ref
-from sensemap_b200 import STORE_F32
+from sensemap_b200 import STORE_F16, STORE_F32
 from sensemap_b200 import synthetic as syn
 from sensemap_b200.patch_match import PatchMatchACMMCuda, PatchMatchOptions, Problem, View
 
@@ -138,6 +138,25 @@ def test_config2_both_passes_match_reference_kernels(config2):
     for name, (acc_g, acc_r, agree_d, agree_n) in out.items():
         assert abs(acc_g - acc_r) <= GT_GAP, name
         assert agree_d >= CFG2_DEPTH_AGREE and agree_n >= CFG2_NORMAL_AGREE, name
+
+
+def test_config2_precision_form_keeps_accuracy(config2):
+    """The precision form (FP16 source storage, FP32 accumulation) against the
+    plain FP32 path at config 2: view 0's photometric pass and its geometric
+    pass against the other views' photometric maps, each form from its own
+    maps; ground-truth accuracy within the north star's 0.5 points."""
+    sc = config2
+    V = len(sc.views)
+    gt = sc.views[0].depth_gt
+    acc = {}
+    for storage in (STORE_F32, STORE_F16):
+        photo = [_engine(_opts(sc, seed=r, image_storage=storage), _problem(sc, r)) for r in range(V)]
+        geo = _engine(_opts(sc, True, seed=1000, image_storage=storage),
+                      _problem(sc, 0, [(x["depth"], x["normal"]) for x in photo]))
+        acc[storage] = (syn.depth_accuracy(photo[0]["depth"], gt), syn.depth_accuracy(geo["depth"], gt))
+    print("config2 precision form (photometric, geometric) f32 / f16:", acc)
+    for k in range(2):
+        assert abs(acc[STORE_F16][k] - acc[STORE_F32][k]) <= GT_GAP
 
 
 def test_config2_photometric_band_matches_cpu_transcription(config2):
