@@ -265,12 +265,13 @@ class PoolWorkload:
     11 photometric jobs in one batch, then 11 geometric jobs in one batch."""
 
     def __init__(self, wl: Workload, block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 1,
-                 step: int = STEP):
+                 step: int = STEP, persistent: bool = False):
         self.wl = wl
         self.block_x = block_x
         self.ref_tile_tma = ref_tile_tma
         self.tpp = threads_per_pixel
         self.step = step
+        self.persistent = persistent
 
     def _run(self, pool, images, on_photo_done=None):
         from sensemap_b200.patch_match import View
@@ -300,7 +301,7 @@ class PoolWorkload:
         from sensemap_b200.pool import DepthMapPool
         return DepthMapPool(memory_budget_bytes=64 << 30, max_active_jobs=self.wl.V, image_storage=self.wl.storage,
                             sweep_block_x=self.block_x, stream=stream, ref_tile_tma=self.ref_tile_tma,
-                            threads_per_pixel=self.tpp)
+                            threads_per_pixel=self.tpp, persistent=self.persistent)
 
     def step_device(self, stream):
         pool = self.new_pool(stream)
@@ -550,7 +551,7 @@ def ncc_fp64_leg(scene, storage, tune, stream, samples=10000) -> dict:
     opt = make_options(scene, storage, False)
     dev_prob = Problem(0, list(range(1, V)), [View(v.image, v.K, v.R, v.T) for v in scene.views])
     with PatchMatchACMMCuda(opt, dev_prob, stream=stream) as pm:
-        pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"])
+        pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"], tune["persistent"])
         pm.Run()
         depth, normal, cost = pm.GetDepthMap(), pm.GetNormalMap(), pm.GetCostMap()
     rng = np.random.default_rng(11)
@@ -618,9 +619,11 @@ def main():
     from sensemap_b200.patch_match import PatchMatchACMMCuda, autotune
     tune = autotune(make_options(scene, storage, False), wl.problem(0, wl.views(dev_imgs)), stream=sptr, repeats=2)
     log(f"autotune: block_x={tune['sweep_block_x']} tpp={tune['threads_per_pixel']} tma={tune['ref_tile_tma']} "
-        f"({', '.join(f'{c['sweep_block_x']}/{c['threads_per_pixel']}: {c['ms_per_sweep']:.2f} ms' for c in tune['candidates'])})")
+        f"persistent={tune['persistent']} ({', '.join(f'{c['sweep_block_x']}/{c['threads_per_pixel']}'
+                                                      f'{'p' if c['persistent'] else ''}: {c['ms_per_sweep']:.2f} ms'
+                                                      for c in tune['candidates'])})")
     pw = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"],
-                      threads_per_pixel=tune["threads_per_pixel"])
+                      threads_per_pixel=tune["threads_per_pixel"], persistent=tune["persistent"])
 
     # Timed region: the batched form, device-resident inputs.
     clocks = ClockSampler(local)
@@ -638,7 +641,7 @@ def main():
     # Per-kernel device time (one profiled photometric pass of view 0).
     views = wl.views(dev_imgs)
     pm = PatchMatchACMMCuda(make_options(scene, storage, False), wl.problem(0, views), stream=sptr)
-    pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"])
+    pm.SetTuning(tune["sweep_block_x"], tune["ref_tile_tma"], tune["threads_per_pixel"], tune["persistent"])
     pm.SetProfiling(True)
     pm.Run()
     prof = pm.Profile()
@@ -696,7 +699,7 @@ def main():
     # The autotuner's window-step candidate: the batched form at S=2, accepted
     # when its ground-truth accuracy is within 0.5 points of the plain path's.
     pw2 = PoolWorkload(wl, block_x=tune["sweep_block_x"], ref_tile_tma=tune["ref_tile_tma"],
-                       threads_per_pixel=tune["threads_per_pixel"], step=2)
+                       threads_per_pixel=tune["threads_per_pixel"], step=2, persistent=tune["persistent"])
     s_steps = min(args.steps, 4)
     s_ms, s_launches, s_get, s_last, _ = timed_steps(pool_step_fn(pw2, sptr), s_steps, 1, stream, world)
     s_acc = accuracy_of(s_get, scene)
@@ -779,7 +782,8 @@ def run_serving(args, wl, sptr, tune) -> dict:
         specs.append(srv.JobSpec(o, r, [i for i in range(wl.V) if i != r]))
     slots = 8
     pool = DepthMapPool(memory_budget_bytes=32 << 30, max_active_jobs=slots, image_storage=wl.storage, stream=sptr,
-                        sweep_block_x=tune["sweep_block_x"], threads_per_pixel=tune["threads_per_pixel"])
+                        sweep_block_x=tune["sweep_block_x"], threads_per_pixel=tune["threads_per_pixel"],
+                        persistent=tune["persistent"])
     for i, v in enumerate(sc.views):
         pool.add_view(i, View(wl.dev[i], v.K, v.R, v.T))
     acc = []
@@ -1363,7 +1367,7 @@ def run_batched(args):
     def pool_pass(storage, step):
         pool = DepthMapPool(memory_budget_bytes=120 << 30, max_active_jobs=len(jobs), image_storage=storage,
                             sweep_block_x=tune["sweep_block_x"], threads_per_pixel=tune["threads_per_pixel"],
-                            stream=sptr)
+                            persistent=tune["persistent"], stream=sptr)
         for i, v in enumerate(views):
             pool.add_view(i, v)
         torch.cuda.synchronize()
@@ -1487,7 +1491,7 @@ def run_serving_aerial(args):
             arrivals = srv.poisson_arrivals(rate, jobs_per_rate, seed=int(rate * 100) + step)
             pool = DepthMapPool(memory_budget_bytes=120 << 30, max_active_jobs=16, image_storage=STORE_F16,
                                 sweep_block_x=tune["sweep_block_x"], threads_per_pixel=tune["threads_per_pixel"],
-                                stream=sptr)
+                                persistent=tune["persistent"], stream=sptr)
             acc = []
 
             def ensure(spec, pool=pool):

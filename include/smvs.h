@@ -243,6 +243,10 @@ typedef struct smvs_tuning {
                             the pixel's state in registers and local memory; 2, 4: in
                             shared memory, the smallest value >= this whose shared memory
                             fits the view count is used). Maps do not depend on it. */
+  int persistent;        /* threads_per_pixel 1: 1 = each checkerboard sweep launch is a
+                            persistent grid (resident blocks per SM x SMs) whose blocks loop
+                            over the tiles (the local optimisation keeps one block per tile);
+                            0 (default) = one block per tile. Maps do not depend on it. */
 } smvs_tuning;
 int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 /* The launch shape in use and whether the last smvs_run staged its reference
@@ -250,8 +254,9 @@ int smvs_set_tuning(smvs_engine* eng, const smvs_tuning* tuning);
 int smvs_get_tuning(const smvs_engine* eng, smvs_tuning* tuning);
 /* Launch-shape autotuner: on a scratch engine for (opt, prob), times one
  * iteration's checkerboard sweep for every launch shape (sweep_block_x 8, 16,
- * 32, 64 x threads_per_pixel 1, 2, 4, reference tiles by TMA where the image
- * qualifies), best of `repeats` (<= 0: 3), and writes the fastest to `best`. The
+ * 32, 64 x threads_per_pixel 1, 2, 4, with threads_per_pixel 1 both launch
+ * forms of `persistent`, reference tiles by TMA where the image qualifies),
+ * best of `repeats` (<= 0: 3), and writes the fastest to `best`. The
  * candidates and their ms per sweep launch go to tried/ms (up to `capacity`),
  * their number to num_tried. Maps do not depend on the choice. */
 int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* stream, int repeats, smvs_tuning* best,
@@ -283,6 +288,7 @@ typedef struct smvs_pool_options {
   int gpu_index;              /* -1 = current device */
   int ref_tile_tma;           /* stage reference tiles with TMA where a view qualifies (smvs_tuning) */
   int sweep_threads_per_pixel; /* threads per pixel of the checkerboard kernels (smvs_tuning) */
+  int sweep_persistent;        /* persistent checkerboard launches (smvs_tuning.persistent) */
 } smvs_pool_options;
 
 typedef struct smvs_pool_stats {

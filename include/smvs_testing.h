@@ -54,6 +54,13 @@ int smvs_test_fusion_waits(double limit_seconds, long long withhold_seed);
  * smvs_synchronize or getter returns SMVS_ETIMEDOUT. */
 int smvs_test_tile_waits(smvs_engine* eng, int polls, int skip_copy);
 
+/* Persistent launches (smvs_tuning.persistent, smvs_pool_options.
+ * sweep_persistent) of engines and pools in this process that start a run or
+ * build a batch after this call use at most max_blocks blocks (0 restores the
+ * resident count), so that small images still have each block loop over many
+ * tiles. Maps do not change. */
+int smvs_test_persistent_grid(int max_blocks);
+
 /* The propagate-depth initial maps of an engine created with propagate_depth:
  * the given reference maps with the projected source depths composited in
  * (depth W*H, normal 3*W*H planar) and the prior depth (W*H), before random

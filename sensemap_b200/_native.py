@@ -84,13 +84,14 @@ class smvs_problem(C.Structure):
 
 
 class smvs_tuning(C.Structure):
-    _fields_ = [("sweep_block_x", C.c_int), ("ref_tile_tma", C.c_int), ("threads_per_pixel", C.c_int)]
+    _fields_ = [("sweep_block_x", C.c_int), ("ref_tile_tma", C.c_int), ("threads_per_pixel", C.c_int),
+                ("persistent", C.c_int)]
 
 
 class smvs_pool_options(C.Structure):
     _fields_ = [("memory_budget_bytes", C.c_size_t), ("max_active_jobs", C.c_int), ("image_storage", C.c_int),
                 ("sweep_block_x", C.c_int), ("use_graphs", C.c_int), ("gpu_index", C.c_int),
-                ("ref_tile_tma", C.c_int), ("sweep_threads_per_pixel", C.c_int)]
+                ("ref_tile_tma", C.c_int), ("sweep_threads_per_pixel", C.c_int), ("sweep_persistent", C.c_int)]
 
 
 class smvs_pool_stats(C.Structure):
@@ -258,6 +259,7 @@ _SIGNATURES = {
     "smvs_test_take_cuda_error": (C.c_int, []),
     "smvs_test_fusion_waits": (C.c_int, [C.c_double, C.c_longlong]),
     "smvs_test_tile_waits": (C.c_int, [C.c_void_p, C.c_int, C.c_int]),
+    "smvs_test_persistent_grid": (C.c_int, [C.c_int]),
     "smvs_test_propagate_init": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
     "smvs_test_delaunay": (C.c_int, [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "smvs_pyramid_level_size": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),

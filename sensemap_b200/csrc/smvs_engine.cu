@@ -165,6 +165,7 @@ struct smvs_engine {
   CUtensorMap* d_tmap = nullptr;  // the reference image's TMA descriptor
   int* d_status = nullptr;        // bounded waits of the kernels that gave up
   bool use_tma = true;
+  int persistent = 0;             // thread-per-pixel kernels as a persistent grid (smvs_tuning)
   bool tma_active = false;        // the last run staged reference tiles with TMA
   int tpp_used = 0;               // threads per pixel of the last run
   int tma_polls = 0;              // TMA tile wait bound (0 = default; a test hook shortens it)
@@ -620,7 +621,7 @@ int smvs_run(smvs_engine* e) {
     return smvs::LaunchInit(p, o.init_depth_random, (float)o.depth_min, (float)o.depth_max, e->stream);
   });
   if (st) return st;
-  smvs::Batch b;
+  smvs::Batch b{};
   if ((st = smvs_internal_prepare_job(&p, &o))) return st;
   if ((st = UploadRefMap(e, &p))) return st;
   e->tma_active = p.tma_box_w > 0;
@@ -653,6 +654,8 @@ int smvs_run(smvs_engine* e) {
     b.status = e->d_status;
     b.tma_polls = e->tma_polls;
     b.tma_skip_copy = e->tma_skip_copy;
+    b.persistent = e->persistent;
+    b.grid_cap = smvs::PersistentGridCap();
   }
   if ((st = Launch(e, SMVS_KERNEL_INIT_CONF, "init conf", [&] { return smvs::LaunchInitConf(b, e->stream); }))) return st;
   int* iters = const_cast<int*>(b.iters);
@@ -795,6 +798,7 @@ int smvs_set_tuning(smvs_engine* e, const smvs_tuning* t) {
   e->jp.block_x = bx;
   e->jp.tpp = tpp;
   e->use_tma = t->ref_tile_tma != 0;
+  e->persistent = t->persistent != 0;
   return SMVS_OK;
 }
 
@@ -803,6 +807,7 @@ int smvs_get_tuning(const smvs_engine* e, smvs_tuning* t) {
   t->sweep_block_x = e->jp.block_x;
   t->ref_tile_tma = e->tma_active ? 1 : 0;
   t->threads_per_pixel = e->tpp_used > 0 ? e->tpp_used : e->jp.tpp;
+  t->persistent = t->threads_per_pixel == 1 ? e->persistent : 0;  // only the thread-per-pixel kernels loop
   return SMVS_OK;
 }
 
@@ -830,6 +835,12 @@ int smvs_get_profile(smvs_engine* e, int kind, int* count, double* total_ms) {
 }
 void smvs_destroy(smvs_engine* e) { delete e; }
 
+int smvs_test_persistent_grid(int max_blocks) {
+  if (max_blocks < 0) return Fail(SMVS_EINVAL, "persistent grid: bad arguments");
+  smvs::SetPersistentGridCap(max_blocks);
+  return SMVS_OK;
+}
+
 int smvs_test_tile_waits(smvs_engine* e, int polls, int skip_copy) {
   if (!e || polls < 0) return Fail(SMVS_EINVAL, "tile waits: bad arguments");
   e->tma_polls = polls;
@@ -838,10 +849,11 @@ int smvs_test_tile_waits(smvs_engine* e, int polls, int skip_copy) {
 }
 
 // Launch-shape autotuner: times the checkerboard sweep of one iteration of
-// `prob` for every candidate launch shape (threads per block in x, reference
-// tiles by TMA or by plain loads) on a scratch engine, best of `repeats`, and
-// returns the fastest. Results do not depend on the launch shape, so the
-// choice only affects speed.
+// `prob` for every candidate launch shape (pixels per block row x threads per
+// pixel, and for one thread per pixel one block per tile or a persistent grid;
+// reference tiles by TMA where the image qualifies) on a scratch engine, best
+// of `repeats`, and returns the fastest. Results do not depend on the launch
+// shape, so the choice only affects speed.
 int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* stream, int repeats, smvs_tuning* best,
                   smvs_tuning* tried, double* ms, int capacity, int* num_tried) {
   if (!opt || !prob || !best) return Fail(SMVS_EINVAL, "null argument");
@@ -856,9 +868,10 @@ int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* strea
   int n = 0;
   std::vector<smvs_tuning> seen;
   for (int k = 0; k < 4 && st == SMVS_OK; ++k)
-    for (int j = 0; j < 3 && st == SMVS_OK; ++j) {
-      if (!smvs::ValidSweepShape(xs[k], ts[j])) continue;
-      smvs_tuning t{xs[k], 1, ts[j]};
+    for (int j = 0; j < 3 * 2 && st == SMVS_OK; ++j) {
+      const int tpp = ts[j / 2], pers = j % 2;
+      if (!smvs::ValidSweepShape(xs[k], tpp) || (pers && tpp != 1)) continue;
+      smvs_tuning t{xs[k], 1, tpp, pers};
       if ((st = smvs_set_tuning(e, &t))) break;
       double t_best = 0;
       for (int r = 0; r < (repeats > 0 ? repeats : 3) && st == SMVS_OK; ++r) {
@@ -876,7 +889,8 @@ int smvs_autotune(const smvs_options* opt, const smvs_problem* prob, void* strea
       smvs_get_tuning(e, &used);
       bool dup = false;  // threads_per_pixel raised to fit: the same shape as an earlier candidate
       for (const auto& u : seen)
-        dup = dup || (u.sweep_block_x == used.sweep_block_x && u.threads_per_pixel == used.threads_per_pixel);
+        dup = dup || (u.sweep_block_x == used.sweep_block_x && u.threads_per_pixel == used.threads_per_pixel &&
+                      u.persistent == used.persistent);
       if (dup) continue;
       seen.push_back(used);
       if (tried && ms && n < capacity) {

@@ -1,6 +1,7 @@
 // smvs_kernels.cu — per-pixel kernels (image conversion, reference moments,
 // initialisation, mask, geometric-consistency filter) and the dispatch over
 // the window-templated PatchMatch kernels of smvs_sweep.cuh.
+#include <atomic>
 #include <mutex>
 
 #include <cuda_fp16.h>
@@ -369,6 +370,10 @@ cudaError_t LaunchAdvance(int* iters, int num_jobs, cudaStream_t stream) {
 }
 
 int ViewBucket(int N) { return (N + 3) & ~3; }
+
+static std::atomic<int> g_persistent_grid_cap{0};
+int PersistentGridCap() { return g_persistent_grid_cap.load(std::memory_order_relaxed); }
+void SetPersistentGridCap(int max_blocks) { g_persistent_grid_cap.store(max_blocks, std::memory_order_relaxed); }
 
 int FitThreadsPerPixel(int R, int nb, int bx, int tpp) {
   for (int t = tpp; t <= 4; t *= 2)

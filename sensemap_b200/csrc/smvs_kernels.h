@@ -78,6 +78,8 @@ struct Batch {
   int* status;                  // set to 1 when a bounded wait of a kernel gave up
   int tma_polls;                // mbarrier polls before a TMA tile wait gives up (0 = the default bound)
   int tma_skip_copy;            // test hook: arm the tile barrier but issue no copy (its waits run out)
+  int persistent;               // tpp == 1: a persistent grid strides over the tiles (0: one block per tile)
+  int grid_cap;                 // test hook: at most this many persistent blocks (0 = the resident count)
 };
 
 // Checkerboard blocks: 256 threads, tpp threads per pixel, bx pixels per
@@ -151,6 +153,10 @@ int ViewBucket(int N);
 // The smallest tpp >= `tpp` whose sweep block fits in shared memory for nb
 // views (results do not depend on it); 0 if none does.
 int FitThreadsPerPixel(int R, int nb, int bx, int tpp);
+// Test hook: at most this many blocks in persistent launches built from now on
+// (0 = the resident count).
+int PersistentGridCap();
+void SetPersistentGridCap(int max_blocks);
 // Opt every checkerboard kernel into large dynamic shared memory on the
 // current device. Called once per device by the engine and the pool before
 // any launch (and before any stream capture).

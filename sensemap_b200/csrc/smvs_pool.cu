@@ -695,7 +695,7 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
   for (auto& kv : by_key) {
     const auto& list = kv.second;
     const int n = (int)list.size();
-    smvs::Batch b;
+    smvs::Batch b{};
     b.R = std::get<0>(kv.first);
     b.S = std::get<1>(kv.first);
     b.NB = std::get<2>(kv.first);
@@ -703,6 +703,8 @@ int BuildGroups(smvs_pool* P, const std::vector<int64_t>& ids, std::vector<smvs:
     b.tpp = std::get<4>(kv.first);
     b.tma_polls = 0;
     b.tma_skip_copy = 0;
+    b.persistent = P->opt.sweep_persistent != 0;
+    b.grid_cap = smvs::PersistentGridCap();
     const int by = smvs::SweepRows(b.block_x, b.tpp);
     int tot = 0, ctot = 0;
     for (int k = 0; k < n; ++k) {

@@ -88,20 +88,28 @@ __device__ __forceinline__ bool MbarWait(uint32_t bar, uint32_t parity, uint32_t
 // The block's reference tile as one TMA load: box (RefTileW x RefTileH) of
 // `map` at column x (a multiple of 4) and row y into `tile` (128-byte aligned
 // shared memory); rows and columns outside the image read as zero (the
-// border of the reference's texture). Every thread waits on the mbarrier with
-// a bounded wait (`polls`). Returns false after setting *status if the copy
-// did not land; the caller then leaves the block's pixels unchanged.
+// border of the reference's texture). `uses` counts the block's earlier
+// loads (block-uniform): the first one initialises the mbarrier, and load k
+// completes the barrier's phase k, so a persistent block reuses one barrier
+// for all its tiles. Every thread waits with a bounded wait (`polls`). Returns
+// false after setting *status if the copy did not land; the caller then leaves
+// the block's pixels unchanged and the block stops.
 __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile, int x, int y, uint32_t bytes,
-                                             uint64_t* mbar, int* status, uint32_t polls, bool skip_copy) {
+                                             uint64_t* mbar, uint32_t& uses, int* status, uint32_t polls,
+                                             bool skip_copy) {
   const uint32_t bar = SmemAddr(mbar);
   const bool leader = threadIdx.x == 0 && threadIdx.y == 0;
-  if (leader) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (uses == 0) {
+    if (leader) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
   }
-  __syncthreads();
   if (leader) {
+    // The block's reads of the previous tile (ordered before this point by the
+    // barrier that ended it) come before the copy that overwrites it.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
     if (!skip_copy)
       asm volatile(
@@ -109,12 +117,14 @@ __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile
           ::"r"(SmemAddr(tile)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
           : "memory");
   }
-  const bool landed = MbarWait(bar, 0, polls);
+  const uint32_t parity = uses & 1u;
+  ++uses;
+  const bool landed = MbarWait(bar, parity, polls);
   if (!__syncthreads_or(!landed)) return true;  // block-uniform outcome
   if (leader) atomicExch(status, 1);
   // Let a late copy land before the block's shared memory is released (no
   // copy is in flight when the test hook skipped it).
-  if (!skip_copy) MbarWait(bar, 0, kTmaWaitPolls);
+  if (!skip_copy) MbarWait(bar, parity, kTmaWaitPolls);
   return false;
 }
 
@@ -123,7 +133,7 @@ __device__ __forceinline__ bool TmaStageTile(const CUtensorMap* map, float* tile
 // RefTileW floats starting at (row0 - R, col0 - R - RefTileShift(R)).
 template <int R>
 __device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobParams& p, float* tile, int row0,
-                                             int col0, int rows, float* poses, uint64_t* mbar) {
+                                             int col0, int rows, float* poses, uint64_t* mbar, uint32_t& tma_uses) {
   const int bx = b.block_x;
   const int tw = RefTileW(bx, R), th = rows + 2 * R;
   const int x0 = col0 - R - RefTileShift(R), y0 = row0 - R;
@@ -134,18 +144,17 @@ __device__ __forceinline__ bool StageRefTile(const Batch& b, int job, const JobP
   }
   const int tid = threadIdx.y * blockDim.x + threadIdx.x;
   for (int i = tid; i < p.N * SMVS_POSE_FLOATS; i += blockDim.x * blockDim.y) poses[i] = __ldg(p.poses + i);
-  return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, b.status,
+  return TmaStageTile(b.ref_maps + job, tile, x0, y0, (uint32_t)(tw * th * sizeof(float)), mbar, tma_uses, b.status,
                       b.tma_polls > 0 ? (uint32_t)b.tma_polls : kTmaWaitPolls, b.tma_skip_copy != 0);
 }
 
-// Batched launches: find this block's job (binary search over the block
+// Batched launches: find the job of tile `bid` (binary search over the tile
 // prefix sums), read its iteration counter and stage its parameters in
 // shared memory. Every thread of the block returns the same values.
-__device__ __forceinline__ void DecodeBlock(const Batch& b, const int* prefix, JobParams& sp, int& job, int& blk,
-                                            int& iter) {
+__device__ __forceinline__ void DecodeBlock(const Batch& b, const int* prefix, int bid, JobParams& sp, int& job,
+                                            int& blk, int& iter) {
   __shared__ int s_job, s_blk, s_iter;
   if (threadIdx.x == 0 && threadIdx.y == 0) {
-    const int bid = blockIdx.x;
     int lo = 0, hi = b.num_jobs - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -343,7 +352,7 @@ __global__ void __launch_bounds__(kThreads) InitConfKernel(const Batch b) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   int job, blk, iter;
-  DecodeBlock(b, b.conf_block_start, sp, job, blk, iter);
+  DecodeBlock(b, b.conf_block_start, blockIdx.x, sp, job, blk, iter);
   const JobParams& p = sp;
   const int kBX = blockDim.x, kBY = blockDim.y;
   const int tw = kBX + 2 * R, th = kBY + 2 * R;
@@ -431,14 +440,12 @@ struct ThreadPixelBlocks {
 };
 
 template <int R, int S, int NB>
-__global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) SweepKernelL(const Batch b, int colour) {
-  extern __shared__ float smem[];
-  __shared__ JobParams sp;
-  __shared__ uint64_t mbar;
+__device__ __forceinline__ bool SweepTileL(const Batch& b, int colour, int bid, float* smem, JobParams& sp,
+                                           uint64_t* mbar, uint32_t& tma_uses) {
   int job, blk, iter;
-  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  DecodeBlock(b, b.block_start, bid, sp, job, blk, iter);
   const JobParams& p = sp;
-  if (iter >= p.num_iterations) return;  // finished job of the batch (block-uniform)
+  if (iter >= p.num_iterations) return true;  // finished job of the batch (block-uniform)
   const float th_mc = p.th_tab[iter];
   const uint64_t skey = StageKey(p.seed, StageSweep(iter, colour));
   const int kBX = b.block_x, kBY = kThreads / b.block_x;
@@ -446,12 +453,12 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Swee
   float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
   float* poses = tile + tw * th;
   const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, &mbar)) return;  // block-uniform
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, mbar, tma_uses)) return false;  // block-uniform
   __syncthreads();
   const int tx = threadIdx.x % kBX, ty = threadIdx.x / kBX;
   const int row = row0 + ty;
   const int col = col0 + 2 * tx + ((row + colour) & 1);
-  if (col >= p.W || row >= p.H) return;
+  if (col >= p.W || row >= p.H) return true;
   const int W = p.W, H = p.H, N = p.N;
   const size_t WH = (size_t)W * H;
   const size_t pix = (size_t)row * W + col;
@@ -566,7 +573,7 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Swee
       probs[v] = pv;
       if ((int)n1 >= p.num_good && (int)n2 <= p.num_bad) flags |= (1u << v);
     }
-    if (flags == 0) return;
+    if (flags == 0) return true;
     for (int v = 0; v < N; ++v)
       if (!((flags >> v) & 1u)) probs[v] = 0.f;
     {
@@ -587,7 +594,7 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Swee
     }
     float wn = 0.f;
     for (int v = 0; v < N; ++v) wn += vw[v];
-    if (wn <= 1e-5f) return;
+    if (wn <= 1e-5f) return true;
     const float iwn = 1.0f / wn;
     uint32_t sel = 0;
     for (int v = 0; v < N; ++v) { vw[v] *= iwn; if (vw[v] > 0) sel |= (1u << v); }
@@ -611,7 +618,7 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Swee
       for (int h = 0; h < ns; ++h)
         if (costs[h] <= m) { m = costs[h]; mi = h; }  // FindMinCost :648-659 ('<=')
     }
-    if (mi < 0) return;
+    if (mi < 0) return true;
     depth = hyp[mi][3];
     normal[0] = hyp[mi][0]; normal[1] = hyp[mi][1]; normal[2] = hyp[mi][2];
     if (mi != 0)
@@ -655,15 +662,35 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Swee
     p.normal[pix] = hyp[mi][0]; p.normal[WH + pix] = hyp[mi][1]; p.normal[2 * WH + pix] = hyp[mi][2];
     for (int v = 0; v < N; ++v) p.cost[(size_t)v * WH + pix] = M[mi][v];
   }
+  return true;
 }
 
+// One block per checkerboard tile, or a persistent grid (resident blocks per
+// SM x SMs) whose blocks stride over the tiles: a tile's pixels read only
+// the other colour's state, so the tile order never changes results. The
+// per-pixel arithmetic is the same code in both launch forms.
+template <int R, int S, int NB>
+__global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) SweepKernelL(const Batch b, int colour) {
+  extern __shared__ float smem[];
+  __shared__ JobParams sp;
+  __shared__ uint64_t mbar;
+  uint32_t tma_uses = 0;
+  for (int t = blockIdx.x; t < b.total_blocks; t += gridDim.x) {
+    if (!SweepTileL<R, S, NB>(b, colour, t, smem, sp, &mbar, tma_uses)) return;
+    __syncthreads();  // the tile's shared memory is free for the next tile
+  }
+}
+
+// One block per checkerboard tile. (This kernel is kept out of the
+// persistent form: restructured as a tile loop its code generation rounds a
+// few normals differently in the last bit from LocalOptKernel<R, S, G>.)
 template <int R, int S, int NB>
 __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) LocalOptKernelL(const Batch b, int colour) {
   extern __shared__ float smem[];
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
   int job, blk, iter;
-  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  DecodeBlock(b, b.block_start, blockIdx.x, sp, job, blk, iter);
   const JobParams& p = sp;
   // Iterations > 2 only (patch_match_cuda.cu:861-880); block-uniform.
   if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
@@ -673,7 +700,8 @@ __global__ void __launch_bounds__(kThreads, ThreadPixelBlocks<S, NB>::kMin) Loca
   float* tile = Align128(smem);  // a TMA destination starts on a 128-byte boundary
   float* poses = tile + tw * th;
   const int col0 = (blk % p.blocks_x) * 2 * kBX, row0 = (blk / p.blocks_x) * kBY;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, &mbar)) return;  // block-uniform
+  uint32_t tma_uses = 0;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, kBY, poses, &mbar, tma_uses)) return;  // block-uniform
   __syncthreads();
   const int tx = threadIdx.x % kBX, ty = threadIdx.x / kBX;
   const int row = row0 + ty;
@@ -777,7 +805,7 @@ __global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) SweepKer
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
   int job, blk, iter;
-  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  DecodeBlock(b, b.block_start, blockIdx.x, sp, job, blk, iter);
   const JobParams& p = sp;
   if (iter >= p.num_iterations) return;  // finished job of the batch (block-uniform)
   const float th_mc = p.th_tab[iter];
@@ -793,7 +821,8 @@ __global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) SweepKer
   sm.VW = sm.HY + kMaxHyp * 4 * P;
   sm.PR = sm.VW + nb * P;
   const int col0 = (blk % p.blocks_x) * 2 * bx, row0 = (blk / p.blocks_x) * rows;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar)) return;  // block-uniform
+  uint32_t tma_uses = 0;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar, tma_uses)) return;  // block-uniform
   __syncthreads();
   const int g = threadIdx.x / G, lane = threadIdx.x % G;
   const int row = row0 + g / bx;
@@ -1017,7 +1046,7 @@ __global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) LocalOpt
   __shared__ JobParams sp;
   __shared__ uint64_t mbar;
   int job, blk, iter;
-  DecodeBlock(b, b.block_start, sp, job, blk, iter);
+  DecodeBlock(b, b.block_start, blockIdx.x, sp, job, blk, iter);
   const JobParams& p = sp;
   // Iterations > 2 only (patch_match_cuda.cu:861-880); block-uniform.
   if (iter >= p.num_iterations || !p.local_opt || iter <= 2) return;
@@ -1029,7 +1058,8 @@ __global__ void __launch_bounds__(kThreads, SweepOccupancy<G>::kBlocks) LocalOpt
   float* poses = tile + tw * th;
   float* Ms = poses + nb * SMVS_POSE_FLOATS;  // [5][nb][P]
   const int col0 = (blk % p.blocks_x) * 2 * bx, row0 = (blk / p.blocks_x) * rows;
-  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar)) return;  // block-uniform
+  uint32_t tma_uses = 0;
+  if (!StageRefTile<R>(b, job, p, tile, row0, col0, rows, poses, &mbar, tma_uses)) return;  // block-uniform
   __syncthreads();
   const int g = threadIdx.x / G, lane = threadIdx.x % G;
   const int row = row0 + g / bx;
@@ -1132,14 +1162,36 @@ cudaError_t LaunchSweepT(const Batch& b, int colour, bool local, cudaStream_t st
   return cudaGetLastError();
 }
 
+// Grid of a thread-per-pixel launch: one block per tile, or with b.persistent
+// the blocks that fit on the device at once (occupancy x SMs), capped at the
+// tile count (and at b.grid_cap when set).
+template <typename Kernel>
+cudaError_t TilesGrid(Kernel k, const Batch& b, size_t smem, int* grid) {
+  *grid = b.total_blocks;
+  if (!b.persistent) return cudaSuccess;
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kThreads, smem);
+  if (e != cudaSuccess) return e;
+  const long long resident = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  if (resident < *grid) *grid = (int)resident;
+  if (b.grid_cap > 0 && b.grid_cap < *grid) *grid = b.grid_cap;
+  return cudaSuccess;
+}
+
 template <int R, int S, int NB>
 cudaError_t LaunchSweepL(const Batch& b, int colour, bool local, cudaStream_t stream) {
   if (b.total_blocks <= 0) return cudaSuccess;
   const size_t smem = SweepKernelSmem(R, b.NB, b.block_x, 1);
-  if (local)
+  if (local) {
     LocalOptKernelL<R, S, NB><<<b.total_blocks, kThreads, smem, stream>>>(b, colour);
-  else
-    SweepKernelL<R, S, NB><<<b.total_blocks, kThreads, smem, stream>>>(b, colour);
+    return cudaGetLastError();
+  }
+  int grid = 0;
+  const cudaError_t e = TilesGrid(SweepKernelL<R, S, NB>, b, smem, &grid);
+  if (e != cudaSuccess) return e;
+  SweepKernelL<R, S, NB><<<grid, kThreads, smem, stream>>>(b, colour);
   return cudaGetLastError();
 }
 

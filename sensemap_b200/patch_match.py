@@ -292,9 +292,10 @@ class PatchMatchACMMCuda:
     def LaunchCount(self) -> int:
         return int(N.lib().smvs_launch_count(self._h))
 
-    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 1) -> None:
+    def SetTuning(self, sweep_block_x: int = 32, ref_tile_tma: bool = True, threads_per_pixel: int = 1,
+                  persistent: bool = False) -> None:
         t = N.smvs_tuning(sweep_block_x=sweep_block_x, ref_tile_tma=int(ref_tile_tma),
-                          threads_per_pixel=int(threads_per_pixel))
+                          threads_per_pixel=int(threads_per_pixel), persistent=int(persistent))
         N.check(N.lib().smvs_set_tuning(self._h, C.byref(t)))
 
     def Tuning(self) -> dict:
@@ -302,7 +303,7 @@ class PatchMatchACMMCuda:
         t = N.smvs_tuning()
         N.check(N.lib().smvs_get_tuning(self._h, C.byref(t)))
         return {"sweep_block_x": t.sweep_block_x, "ref_tile_tma": bool(t.ref_tile_tma),
-                "threads_per_pixel": t.threads_per_pixel}
+                "threads_per_pixel": t.threads_per_pixel, "persistent": bool(t.persistent)}
 
     def SetProfiling(self, enable: bool = True) -> None:
         N.check(N.lib().smvs_set_profiling(self._h, int(enable)))
@@ -348,7 +349,8 @@ def autotune(options: PatchMatchOptions, problem: Problem, stream=None, repeats:
     N.check(N.lib().smvs_autotune(C.byref(options.to_c()), C.byref(prob), stream_ptr, int(repeats), C.byref(best),
                                   tried, ms, cap, C.byref(n)))
     return {"sweep_block_x": best.sweep_block_x, "ref_tile_tma": bool(best.ref_tile_tma),
-            "threads_per_pixel": best.threads_per_pixel,
+            "threads_per_pixel": best.threads_per_pixel, "persistent": bool(best.persistent),
             "candidates": [{"sweep_block_x": tried[i].sweep_block_x, "ref_tile_tma": bool(tried[i].ref_tile_tma),
-                            "threads_per_pixel": tried[i].threads_per_pixel, "ms_per_sweep": ms[i]}
+                            "threads_per_pixel": tried[i].threads_per_pixel, "persistent": bool(tried[i].persistent),
+                            "ms_per_sweep": ms[i]}
                            for i in range(min(n.value, cap))]}

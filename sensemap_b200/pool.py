@@ -19,7 +19,7 @@ from .patch_match import PatchMatchOptions, View, _addr, _is_cuda_tensor
 class DepthMapPool:
     def __init__(self, memory_budget_bytes: int = 16 << 30, max_active_jobs: int = 64, image_storage: int = N.STORE_U8,
                  sweep_block_x: int = 32, use_graphs: bool = True, gpu_index: int = -1, stream=None,
-                 ref_tile_tma: bool = True, threads_per_pixel: int = 1):
+                 ref_tile_tma: bool = True, threads_per_pixel: int = 1, persistent: bool = False):
         o = N.smvs_pool_options()
         N.check(N.lib().smvs_pool_options_default(C.byref(o)))
         o.memory_budget_bytes = int(memory_budget_bytes)
@@ -30,6 +30,7 @@ class DepthMapPool:
         o.gpu_index = int(gpu_index)
         o.ref_tile_tma = int(ref_tile_tma)
         o.sweep_threads_per_pixel = int(threads_per_pixel)
+        o.sweep_persistent = int(persistent)
         h = C.c_void_p()
         N.check(N.lib().smvs_pool_create(C.byref(o), C.c_void_p(int(stream)) if stream is not None else None,
                                          C.byref(h)))

@@ -35,20 +35,28 @@ def add_scene(pool, scene, base):
         pool.add_view(base + i, View(v.image, v.K, v.R, v.T))
 
 
-def test_batched_jobs_match_single_engine(scenes):
+@pytest.mark.parametrize("persistent,cap", [(False, 0), (True, 0), (True, 5)])
+def test_batched_jobs_match_single_engine(scenes, persistent, cap):
+    """Persistent launches too: with a cap of 5 blocks each block loops over
+    the tiles of every job of the batch (jobs of two image sizes, 4 and 5
+    iterations, so the batch changes while they run)."""
     jobs = []
-    with DepthMapPool(max_active_jobs=8) as pool:
-        for si, sc in enumerate(scenes):
-            add_scene(pool, sc, 100 * si)
-            for r in (0, 1):
-                opt = photometric_options(sc, iters=5, random_seed=10 * si + r)
-                srcs = [100 * si + i for i in range(len(sc.views)) if i != r]
-                jobs.append((pool.submit(opt, 100 * si + r, srcs), sc, r, opt))
-        pool.run_until_done([j[0] for j in jobs])
-        st = pool.stats()
-        assert st["graphs_built"] >= 1 and st["done"] == len(jobs)
-        for jid, sc, r, opt in jobs:
-            assert_same(pool.maps(jid), engine_maps(opt, problem_from_scene(sc, ref=r)))
+    N.check(N.lib().smvs_test_persistent_grid(cap))
+    try:
+        with DepthMapPool(max_active_jobs=8, persistent=persistent) as pool:
+            for si, sc in enumerate(scenes):
+                add_scene(pool, sc, 100 * si)
+                for r in (0, 1):
+                    opt = photometric_options(sc, iters=4 + r, random_seed=10 * si + r)
+                    srcs = [100 * si + i for i in range(len(sc.views)) if i != r]
+                    jobs.append((pool.submit(opt, 100 * si + r, srcs), sc, r, opt))
+            pool.run_until_done([j[0] for j in jobs])
+            st = pool.stats()
+            assert st["graphs_built"] >= 1 and st["done"] == len(jobs)
+            for jid, sc, r, opt in jobs:
+                assert_same(pool.maps(jid), engine_maps(opt, problem_from_scene(sc, ref=r)))
+    finally:
+        N.check(N.lib().smvs_test_persistent_grid(0))
 
 
 def test_job_alone_equals_job_in_mix(scenes):

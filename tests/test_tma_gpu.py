@@ -86,3 +86,26 @@ def test_autotune_picks_a_candidate_and_maps_do_not_change():
     a = _run(scene, res["ref_tile_tma"], res["sweep_block_x"], iters=3, tpp=res["threads_per_pixel"])
     b = _run(scene, False, 32, iters=3)
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+@pytest.mark.parametrize("tma,block_x,cap", [(True, 32, 0), (True, 32, 7), (False, 32, 7), (True, 8, 5),
+                                             (True, 64, 3)])
+def test_persistent_launch_does_not_change_maps(tma, block_x, cap):
+    """Thread-per-pixel kernels as a persistent grid: with a cap of a few blocks
+    each block loops over many tiles (one TMA barrier, one phase per tile)."""
+    from sensemap_b200 import _native as N
+    scene = small_planes(seed=6, w=200, h=120)
+    opt = photometric_options(scene, iters=4)
+    pm = PatchMatchACMMCuda(opt, problem_from_scene(scene))
+    pm.SetTuning(block_x, ref_tile_tma=tma, threads_per_pixel=1, persistent=True)
+    N.check(N.lib().smvs_test_persistent_grid(cap))
+    try:
+        pm.Run()
+        a = (pm.GetDepthMap(), pm.GetNormalMap(), pm.GetCostMap(), pm.GetViewSelMap(), pm.Tuning())
+    finally:
+        N.check(N.lib().smvs_test_persistent_grid(0))
+        pm.close()
+    b = _run(scene, True, 32, iters=4, tpp=2)
+    assert a[4]["persistent"] and a[4]["threads_per_pixel"] == 1 and a[4]["ref_tile_tma"] == tma
+    for x, y in zip(a[:4], b[:4]):
+        assert np.array_equal(x, y)
