@@ -273,16 +273,18 @@ class PoolWorkload:
         self.step = step
         self.persistent = persistent
 
-    def _run(self, pool, images, on_photo_done=None):
+    def _run(self, pool, images, on_photo_done=None, base=0):
+        """Both passes of every view; view ids base .. base + V - 1 (a fresh base
+        makes the pool upload the images again)."""
         from sensemap_b200.patch_match import View
         wl, sc = self.wl, self.wl.scene
         for i, v in enumerate(sc.views):
-            pool.add_view(i, View(images[i], v.K, v.R, v.T))
+            pool.add_view(base + i, View(images[i], v.K, v.R, v.T))
         opt_p = make_options(sc, wl.storage, False, self.step)
         photo = []
         for r in range(wl.V):
             opt_p.random_seed = r
-            photo.append(pool.submit(opt_p, r, [i for i in range(wl.V) if i != r]))
+            photo.append(pool.submit(opt_p, base + r, [base + i for i in range(wl.V) if i != r]))
         pool.run_until_done(photo)
         for j in photo:
             if on_photo_done is not None:
@@ -293,7 +295,7 @@ class PoolWorkload:
         geo = []
         for r in range(wl.V):
             opt_g.random_seed = 1000 + r
-            geo.append(pool.submit(opt_g, r, [i for i in range(wl.V) if i != r]))
+            geo.append(pool.submit(opt_g, base + r, [base + i for i in range(wl.V) if i != r]))
         pool.run_until_done(geo)
         return geo
 
@@ -311,18 +313,44 @@ class PoolWorkload:
     def step_host(self, stream):
         """Host images in; every job's depth, normal and confidence maps back to
         host, for the photometric and the geometric pass (what ProcessProblem
-        reads back and writes, patch_match_controller.cc:4679-4720)."""
+        reads back and writes, patch_match_controller.cc:4679-4720). One pool
+        serves every host step, as a long-running process keeps it: each step
+        adds the pinned host images under fresh view ids (so they are uploaded
+        again) and reads the maps back into pinned host buffers allocated on the
+        first call and reused."""
+        import torch
         import sensemap_b200._native as NN
         kinds = (NN.MAP_DEPTH, NN.MAP_NORMAL, NN.MAP_CONF)
-        pool = self.new_pool(stream)
-        out = []
-        geo = self._run(pool, self.wl.host, on_photo_done=lambda j: out.extend(pool.get_map(j, k) for k in kinds))
-        out += [pool.get_map(j, k) for j in geo for k in kinds]
+        wl = self.wl
+        if getattr(self, "_host_pool", None) is None:
+            self._host_pool = self.new_pool(stream)
+            self._host_steps = 0
+            H, W = wl.scene.views[0].image.shape
+            shapes = {NN.MAP_DEPTH: (H, W), NN.MAP_NORMAL: (3, H, W), NN.MAP_CONF: (H, W)}
+            self._host_out = [torch.empty(shapes[k], dtype=torch.float32).pin_memory()
+                              for _ in range(2 * wl.V) for k in kinds]
+        pool, out = self._host_pool, self._host_out
+        slot = iter(range(len(out)))
+        reads = []
+
+        def read(j):
+            for k in kinds:
+                reads.append(pool.get_map(j, k, out=out[next(slot)]))
+        base = 1000 * self._host_steps
+        self._host_steps += 1
+        geo = self._run(pool, wl.host, on_photo_done=read, base=base)
+        for j in geo:
+            read(j)
+            pool.release(j)
         st = pool.stats()
-        pool.close()
-        h2d = sum(int(t.numel()) * 4 for t in self.wl.host)
-        d2h = sum(o.nbytes for o in out)
-        return out, h2d, d2h, st["launches"]
+        h2d = sum(int(t.numel()) * 4 for t in wl.host)
+        d2h = sum(int(o.numel()) * 4 for o in reads)
+        return reads, h2d, d2h, st["launches"]
+
+    def close_host_pool(self):
+        if getattr(self, "_host_pool", None) is not None:
+            self._host_pool.close()
+            self._host_pool = None
 
 
 def storage_code(name):
@@ -670,7 +698,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         # End to end through host buffers (pinned inputs; depth, normal and
-        # confidence maps of both passes back to host).
+        # confidence maps of both passes back to pinned host buffers).
         host_step = wl.step_host if args.mode == "engine" else (lambda: pw.step_host(sptr))
         host_step()
         torch.cuda.synchronize()
@@ -678,12 +706,17 @@ def main():
         e2e_steps = min(args.steps, 3)
         t = time.perf_counter()
         h2d = d2h = 0
+        step_s = []
         for _ in range(e2e_steps):
+            t_step = time.perf_counter()
             _, h2d, d2h, _ = host_step()
+            step_s.append(time.perf_counter() - t_step)
         torch.cuda.synchronize()
         el = max_over_ranks(time.perf_counter() - t, world)
         e2e = {"value": e2e_steps * wl.V * world / el, "unit": "depth maps/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "steps": e2e_steps}
+               "d2h_bytes_per_step": d2h, "steps": e2e_steps, "step_s": [round(x, 3) for x in step_s]}
+        log(f"e2e {e2e['value']:.3f} depth maps/s, host steps {', '.join(f'{x:.2f}' for x in step_s)} s")
+        pw.close_host_pool()
 
     # The plain path: FP32 storage, one engine per reference view and pass.
     plain_wl = Workload(scene, STORE_F32, dev_imgs, host_imgs)

@@ -111,13 +111,26 @@ class DepthMapPool:
             self.step()
         raise RuntimeError("jobs did not finish")
 
-    def get_map(self, job: int, which: int) -> np.ndarray:
+    def get_map(self, job: int, which: int, out=None):
+        """A done job's map (smvs_pool_get_map). `out`, if given, receives it: a
+        contiguous numpy array or torch tensor (pinned host memory copies at
+        full DMA rate; a CUDA tensor gets a device copy) of the map's size."""
         H, W, Nn = self._jobs[job]
         shape, dtype = {N.MAP_DEPTH: ((H, W), np.float32), N.MAP_NORMAL: ((3, H, W), np.float32),
                         N.MAP_CONF: ((H, W), np.float32), N.MAP_COST: ((Nn, H, W), np.float32),
                         N.MAP_VIEW_SEL: ((H, W), np.uint32)}[which]
-        out = np.empty(shape, dtype)
-        N.check(N.lib().smvs_pool_get_map(self._h, int(job), int(which), out.ctypes.data))
+        if out is None:
+            out = np.empty(shape, dtype)
+        nbytes = int(np.prod(shape)) * 4
+        if isinstance(out, np.ndarray):
+            if not out.flags.c_contiguous or not out.flags.writeable or out.nbytes != nbytes:
+                raise ValueError(f"out must be a writable contiguous array of {nbytes} bytes")
+            ptr = out.ctypes.data
+        else:  # torch tensor
+            if not out.is_contiguous() or out.numel() * out.element_size() != nbytes:
+                raise ValueError(f"out must be a contiguous tensor of {nbytes} bytes")
+            ptr = out.data_ptr()
+        N.check(N.lib().smvs_pool_get_map(self._h, int(job), int(which), C.c_void_p(ptr)))
         return out
 
     def maps(self, job: int) -> dict:

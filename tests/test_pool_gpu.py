@@ -156,3 +156,23 @@ def test_ring_of_uneven_views_batched():
         pool.run_until_done([j[0] for j in results])
         for jid, r, srcs, opt in results:
             assert_same(pool.maps(jid), engine_maps(opt, problem_from_scene(sc, ref=r, src=srcs)))
+
+
+def test_get_map_into_caller_buffers(scenes):
+    """Maps read into a pinned host tensor, a CUDA tensor and a numpy array
+    equal the getter's own array; a buffer of the wrong size is rejected."""
+    import torch
+    sc = scenes[0]
+    with DepthMapPool(max_active_jobs=2) as pool:
+        add_scene(pool, sc, 0)
+        job = pool.submit(photometric_options(sc, iters=2, random_seed=8), 0, [1, 2, 3, 4])
+        pool.run_until_done([job])
+        want = pool.get_map(job, N.MAP_NORMAL)
+        pinned = pool.get_map(job, N.MAP_NORMAL, out=torch.empty(want.shape, dtype=torch.float32).pin_memory())
+        cuda = pool.get_map(job, N.MAP_NORMAL, out=torch.empty(want.shape, dtype=torch.float32, device="cuda"))
+        arr = pool.get_map(job, N.MAP_NORMAL, out=np.empty(want.shape, np.float32))
+        np.testing.assert_array_equal(pinned.numpy(), want)
+        np.testing.assert_array_equal(cuda.cpu().numpy(), want)
+        np.testing.assert_array_equal(arr, want)
+        with pytest.raises(ValueError):
+            pool.get_map(job, N.MAP_NORMAL, out=np.empty(want.shape[1:], np.float32))
