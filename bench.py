@@ -400,7 +400,59 @@ def cpu_band(scene, maps, rows: int) -> dict:
 
 
 def cpu_baseline(scene, maps, rows: int) -> dict:
-    return cpu_band(scene, maps, rows)
+    out = cpu_band(scene, maps, rows)
+    out["config1_full"] = config1_full_leg()
+    return out
+
+
+def config1_full_leg(seed: int = 0) -> dict:
+    """A full depth map, measured and not extrapolated: the small planes
+    configuration (640x480, 1 reference + 4 source views, f = 500, window
+    radius 5 step 1, 6 iterations, photometric only, FP32 sources) through the
+    oracle on every host thread and through the engine (device-resident
+    images, smvs_create + Run timed with CUDA events, best of 3 after a
+    warm-up), with both maps' ground-truth accuracy and their agreement."""
+    import torch
+    import oracle.oracle as orc
+    from sensemap_b200 import STORE_F32
+    from sensemap_b200 import synthetic as syn
+    from sensemap_b200.patch_match import PatchMatchACMMCuda, PatchMatchOptions, Problem, View
+    sc = syn.planes_scene(seed=seed, width=640, height=480, focal=500.0, num_src=4)
+    opt = PatchMatchOptions(depth_min=sc.depth_min, depth_max=sc.depth_max, window_radius=5, window_step=1,
+                            sigma_spatial=5, num_iterations=6, geom_consistency=False, init_depth_random=True,
+                            image_storage=STORE_F32, random_seed=seed)
+    host = Problem(sc.ref_index, sc.src_indices, [View(v.image, v.K, v.R, v.T) for v in sc.views])
+    t = time.perf_counter()
+    cpu_maps = orc.run(opt, host)
+    cpu_s = time.perf_counter() - t
+    dev = Problem(sc.ref_index, sc.src_indices,
+                  [View(torch.from_numpy(v.image).cuda(), v.K, v.R, v.T) for v in sc.views])
+    stream = torch.cuda.Stream()  # the engine's launching stream (a non-default one, as in the other legs)
+    gpu_ms = []
+    for rep in range(4):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        pm = PatchMatchACMMCuda(opt, dev, stream=stream.cuda_stream)
+        pm.Run()
+        e1.record(stream)
+        pm.Synchronize()
+        e1.synchronize()
+        depth = pm.GetDepthMap()
+        pm.close()
+        if rep:
+            gpu_ms.append(e0.elapsed_time(e1))
+    gt = sc.views[sc.ref_index].depth_gt
+    m = gt > 0
+    agree = float(np.mean(np.abs(depth[m] - cpu_maps["depth"][m]) <= 0.01 * np.abs(cpu_maps["depth"][m])))
+    gpu_s = min(gpu_ms) / 1000.0
+    return {"what": "planes scene 640x480, 1 + 4 views, R=5, S=1, 6 iterations, photometric, FP32 sources; one "
+                    "full depth map, no extrapolation",
+            "cpu_s": cpu_s, "cpu_depth_maps_per_s": 1.0 / cpu_s, "cpu_cores": orc.num_threads(),
+            "gpu_s": gpu_s, "gpu_depth_maps_per_s": 1.0 / gpu_s, "gpu_over_cpu": cpu_s / gpu_s,
+            "gpu_within_1pct_gt": syn.depth_accuracy(depth, gt),
+            "cpu_within_1pct_gt": syn.depth_accuracy(cpu_maps["depth"], gt),
+            "gpu_cpu_depth_agreement": agree}
 
 
 def run_reference(args):
