@@ -841,10 +841,6 @@ int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
   // 3. One iteration of every active job.
   if (!P->active.empty()) {
     if (P->batch_dirty) {
-      if (P->graph) {
-        cudaGraphExecDestroy(P->graph);
-        P->graph = nullptr;
-      }
       int st = BuildGroups(P, P->active, P->groups);
       if (st) return st;
       if ((st = Upload(P, (int)P->active.size()))) return st;
@@ -855,10 +851,27 @@ int smvs_pool_step(smvs_pool* P, smvs_pool_stats* stats) {
         cudaError_t ce = cudaStreamEndCapture(P->stream, &g);
         if (est) { if (g) cudaGraphDestroy(g); return est; }
         if (ce != cudaSuccess) return Fail(SMVS_ECUDA, "graph capture: %s", cudaGetErrorString(ce));
-        ce = cudaGraphInstantiate(&P->graph, g, 0);
+        // A batch that changed only in its parameters (the same groups, so the
+        // same launch sequence) updates the executable graph in place; launches
+        // already enqueued keep the parameters they were enqueued with. A
+        // changed launch sequence instantiates a new one.
+        if (P->graph) {
+          cudaGraphExecUpdateResultInfo info;
+          if (cudaGraphExecUpdate(P->graph, g, &info) != cudaSuccess) {
+            (void)cudaGetLastError();  // the refused update, not an earlier error
+            cudaGraphExecDestroy(P->graph);
+            P->graph = nullptr;
+          }
+        }
+        if (!P->graph) {
+          ce = cudaGraphInstantiate(&P->graph, g, 0);
+          if (ce != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return Fail(SMVS_ECUDA, "graph instantiate: %s", cudaGetErrorString(ce));
+          }
+          P->graphs_built++;
+        }
         cudaGraphDestroy(g);
-        if (ce != cudaSuccess) return Fail(SMVS_ECUDA, "graph instantiate: %s", cudaGetErrorString(ce));
-        P->graphs_built++;
       }
       P->batch_dirty = false;
     }
