@@ -458,9 +458,11 @@ int64_t smvs_cross_filter_launch_count(smvs_cross_filter* cf);
 int smvs_cross_filter_dedup_levels(smvs_cross_filter* cf);
 int smvs_cross_filter_synchronize(smvs_cross_filter* cf);
 void smvs_cross_filter_destroy(smvs_cross_filter* cf);
-/* Cross filters allocate from a per-device stream-ordered pool that keeps
- * freed blocks for the next filter; this returns them to the device
- * (synchronises the device). gpu_index -1 = current device. */
+/* Cross filters, depth-map pools (views, kept maps, job state), fusion and
+ * the initial-map builders allocate from a per-device stream-ordered memory
+ * pool that keeps freed memory reserved for the next call; this returns the
+ * free part of it to the device (synchronises the device). gpu_index -1 =
+ * current device. */
 int smvs_cross_filter_release_cache(int gpu_index);
 
 /* ---- initial depth/normal maps from the model ---------------------------- */

@@ -21,6 +21,8 @@
 #include "smvs_device.cuh"
 #include "smvs_kernels.h"
 
+cudaMemPool_t smvs_internal_device_pool(int device);
+
 namespace {
 
 thread_local std::string g_last_error;
@@ -179,14 +181,25 @@ struct smvs_engine {
   struct Timed { int kind; cudaEvent_t start, stop; };
   std::vector<Timed> timed;
 
+  // Memory the library's per-device memory pool keeps in reserve (freed by
+  // pools, filters and fusion) is returned to the device before an allocation
+  // here reports that the device is full.
+  static bool ReleaseReserve() {
+    (void)cudaGetLastError();
+    int dev = 0;
+    cudaMemPool_t pool = cudaGetDevice(&dev) == cudaSuccess ? smvs_internal_device_pool(dev) : nullptr;
+    return pool && cudaDeviceSynchronize() == cudaSuccess && cudaMemPoolTrimTo(pool, 0) == cudaSuccess;
+  }
   int Alloc(void** p, size_t bytes) {
     cudaError_t e = cudaMalloc(p, bytes);
+    if (e == cudaErrorMemoryAllocation && ReleaseReserve()) e = cudaMalloc(p, bytes);
     if (e != cudaSuccess) return Fail(SMVS_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
     allocations.push_back(*p);
     return SMVS_OK;
   }
   int AllocPitch(void** p, size_t* pitch, size_t wbytes, int h) {
     cudaError_t e = cudaMallocPitch(p, pitch, wbytes, (size_t)h);
+    if (e == cudaErrorMemoryAllocation && ReleaseReserve()) e = cudaMallocPitch(p, pitch, wbytes, (size_t)h);
     if (e != cudaSuccess) return Fail(SMVS_ENOMEM, "cudaMallocPitch failed: %s", cudaGetErrorString(e));
     allocations.push_back(*p);
     return SMVS_OK;
