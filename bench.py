@@ -560,7 +560,7 @@ def engine_step_fn(wl, stream):
     return step
 
 
-def reference_kernels_leg(scene, ours_view0, repeats=2) -> dict:
+def reference_kernels_leg(scene, ours_view0, repeats=3) -> dict:
     """Baseline leg: the reference's own PatchMatch kernels (compiled from its
     sources into the checker library) on this GPU for view 0 of the bench scene:
     their launch order, launch shapes, 8-bit layered source texture and a device
