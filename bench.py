@@ -306,9 +306,29 @@ class PoolWorkload:
                             threads_per_pixel=self.tpp, persistent=self.persistent)
 
     def step_device(self, stream):
-        pool = self.new_pool(stream)
-        geo = self._run(pool, self.wl.dev)
-        return pool, geo
+        """Device-resident images in. One pool serves every device step, as a
+        long-running process keeps it (and as step_host does): each step adds
+        the images under fresh view ids, so they are converted again, releases
+        the previous step's jobs and runs both passes of every view. Returns
+        the pool, this step's geometric jobs and the kernels it launched."""
+        if getattr(self, "_dev_pool", None) is None:
+            self._dev_pool = self.new_pool(stream)
+            self._dev_steps = 0
+            self._dev_prev = []
+        pool = self._dev_pool
+        for j in self._dev_prev:
+            pool.release(j)
+        before = pool.stats()["launches"]
+        base = 1000 * self._dev_steps
+        self._dev_steps += 1
+        geo = self._run(pool, self.wl.dev, base=base)
+        self._dev_prev = geo
+        return pool, geo, pool.stats()["launches"] - before
+
+    def close_device_pool(self):
+        if getattr(self, "_dev_pool", None) is not None:
+            self._dev_pool.close()
+            self._dev_pool = None
 
     def step_host(self, stream):
         """Host images in; every job's depth, normal and confidence maps back to
@@ -545,9 +565,9 @@ def accuracy_of(getter, scene):
 def pool_step_fn(pw, stream):
     import sensemap_b200._native as NN
 
-    def step():
-        pool, geo = pw.step_device(stream)
-        return [pool], pool.stats()["launches"], \
+    def step():  # the pool outlives the step (PoolWorkload.close_device_pool)
+        pool, geo, launches = pw.step_device(stream)
+        return [], launches, \
             (lambda i: (pool.get_map(geo[i], NN.MAP_DEPTH), pool.get_map(geo[i], NN.MAP_NORMAL)))
     return step
 
@@ -716,6 +736,7 @@ def main():
     ours_view0 = getter(0)
     for o in last:
         o.close()
+    pw.close_device_pool()
     log(f"value {value:.3f} depth maps/s, accuracy {acc['within_1pct_gt']:.4f}")
 
     # Per-kernel device time (one profiled photometric pass of view 0).
@@ -790,6 +811,7 @@ def main():
     s_acc = accuracy_of(s_get, scene)
     for o in s_last:
         o.close()
+    pw2.close_device_pool()
     s_value = s_steps * wl.V * world / (s_ms / 1000.0)
     gap = 100.0 * (plain["within_1pct_gt"] - s_acc["within_1pct_gt"])
     autotuned = {"window_step": 2 if gap <= 0.5 else STEP, "candidate": {"window_step": 2, "value": s_value,
