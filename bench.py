@@ -853,7 +853,7 @@ def main():
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "serving": serving,
                 "clocks": clock_info, "autotune": tune, "accuracy": accuracy, "plain": plain,
                 "autotuned_window": autotuned, "reference_kernels": ref_k}
-        # The north star's second throughput unit: image megapixels x source
+        # The metric's second throughput unit: image megapixels x source
         # views x iterations x passes per second (one depth map = 2 passes).
         mpvi = args.width * args.height / 1e6 * (wl.V - 1) * ITERS * 2
         line["mpix_views_iters_per_s"] = {"value": value * mpvi, "plain": plain["value"] * mpvi,
@@ -1358,7 +1358,7 @@ def large_scene(seed=0, width=6000, height=4000, focal=6000.0, altitude=100.0):
 
 
 def run_large(args):
-    """Config 5: one 24 MP reference view with 20 source views of the aerial
+    """The large single view: one 24 MP reference view with 20 source views of the aerial
     scene, coarse-to-fine over 3 pyramid levels (photometric + geometric
     passes of every view at the coarsest level, then geometric passes of the
     reference at each finer level), FP16 storage against plain FP32: seconds,
@@ -1437,7 +1437,7 @@ def _job_options(dmin, dmax, storage, step=STEP, seed=0):
 
 
 def run_batched(args):
-    """Config 3: a 200-camera ring (radius 20 m, heights 2-6 m) around the
+    """The batched ring: a 200-camera ring (radius 20 m, heights 2-6 m) around the
     heightfield; 64 reference views of three sizes (800x600, 1600x1200,
     3000x2000) with 5-20 nearest ring cameras as sources, one photometric pass
     each: the whole set in one batched pool (every view resident once, one
@@ -1539,7 +1539,7 @@ SERVE_METRIC = "p50/p99 depth-map job latency (s) at Poisson arrival rates, 400-
 
 
 def run_serving_aerial(args):
-    """Config 4: an aerial survey of 400 cameras (20 x 20 stations at 100 m,
+    """Aerial serving: an aerial survey of 400 cameras (20 x 20 stations at 100 m,
     80 % overlap, nadir and 45-degree obliques) over terrain with buildings,
     2000x1500 images kept in pinned host memory (8-bit); depth-map jobs (one
     photometric pass of a reference with its 8-16 nearest cameras of similar

@@ -439,8 +439,8 @@ def dense_points(scene: Scene, view: int, step: int = 3, seed: int = 0, duplicat
 
 def ring_model(num_cameras: int = 40, num_points: int = 3000, radius: float = 20.0, width: int = 1600,
                height: int = 1200, focal: float = 1200.0, seed: int = 0, drop: float = 0.2):
-    """Stand-in for a sparse SfM model around a ring of cameras (config 3's
-    200-camera ring, radius 20 m, heights 2-6 m): cameras look at the scene
+    """Stand-in for a sparse SfM model around a ring of cameras (like the batched
+    workload's 200-camera ring, radius 20 m, heights 2-6 m): cameras look at the scene
     centre; points lie on a seeded terrain inside the ring; a point's track is
     the cameras it projects into, each observation dropped with probability
     `drop`. Returns (Rs, Ts, K, points n x 3 float32, tracks, is_rig)."""

@@ -1,8 +1,8 @@
-"""Parity at the benchmark configurations, against both oracles.
+"""Parity on the benchmark scenes, against both oracles.
 
-Config 1: the planes scene at 640x480, 1 reference + 4 source views (f = 500,
+The planes scene at 640x480, 1 reference + 4 source views (f = 500,
 30-degree arc, 0.3 m baseline), window radius 5 step 1, 6 iterations,
-photometric only, FP32. Config 2: the heightfield scene at 1600x1200 with 10
+photometric only, FP32. The heightfield scene at 1600x1200 with 10
 source views (gain 0.8-1.2, noise sigma 2), photometric then geometric pass.
 
 The oracles are the reference's own kernels (oracle/_ref, run on this GPU) and
@@ -10,7 +10,7 @@ the CPU transcription of the reference kernel logic. Their random number
 generators differ from the engine's (cuRAND XORWOW vs a counter-based
 generator), so maps are compared statistically:
 * ground-truth accuracy (fraction of pixels within 1 % of the analytic depth)
-  must agree within 0.5 points, the north star's tolerance;
+  must agree within 0.5 points, the tolerance the benchmark metric states;
 * the fraction of pixels whose depth is within 1 % and normal within 10 degrees
   of the oracle's map is stated in each test and must be reached.
 """
@@ -27,10 +27,10 @@ pytestmark = pytest.mark.gpu
 
 GT_GAP = 0.005  # 0.5 points of the within-1 % fraction
 # Agreement with an oracle's map: fraction of pixels within 1 % depth / 10
-# degrees normal. The planes scene of config 1 has large weakly textured areas
+# degrees normal. The 640x480 planes scene has large weakly textured areas
 # where both solvers settle on different normals of equal cost.
-CFG1_DEPTH_AGREE, CFG1_NORMAL_AGREE = 0.95, 0.80
-CFG2_DEPTH_AGREE, CFG2_NORMAL_AGREE = 0.97, 0.90
+PLANES_DEPTH_AGREE, PLANES_NORMAL_AGREE = 0.95, 0.80
+HEIGHTFIELD_DEPTH_AGREE, HEIGHTFIELD_NORMAL_AGREE = 0.97, 0.90
 
 
 def _engine(opt, prob):
@@ -64,13 +64,13 @@ def _problem(scene, ref_idx, maps=None):
 
 
 @pytest.fixture(scope="module", params=[0, 1])
-def config1(request):
+def planes_640x480(request):
     return syn.planes_scene(seed=request.param, width=640, height=480, focal=500.0, num_src=4)
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
-def test_config1_matches_reference_kernels(config1):
-    sc = config1
+def test_planes_640x480_matches_reference_kernels(planes_640x480):
+    sc = planes_640x480
     prob = _problem(sc, sc.ref_index)
     opt = _opts(sc)
     poses = orc.run(_opts(sc, num_iterations=0), prob)["poses"]
@@ -80,14 +80,14 @@ def test_config1_matches_reference_kernels(config1):
     m = gt > 0
     acc_g, acc_r = syn.depth_accuracy(g["depth"], gt), syn.depth_accuracy(r["depth"], gt)
     agree_d, agree_n = _agreement(g, r, m)
-    print(f"config1 vs reference kernels: GT {acc_g:.4f} vs {acc_r:.4f}; agreement depth {agree_d:.4f} "
+    print(f"planes_640x480 vs reference kernels: GT {acc_g:.4f} vs {acc_r:.4f}; agreement depth {agree_d:.4f} "
           f"normal {agree_n:.4f}")
     assert abs(acc_g - acc_r) <= GT_GAP
-    assert agree_d >= CFG1_DEPTH_AGREE and agree_n >= CFG1_NORMAL_AGREE
+    assert agree_d >= PLANES_DEPTH_AGREE and agree_n >= PLANES_NORMAL_AGREE
 
 
-def test_config1_matches_cpu_transcription(config1):
-    sc = config1
+def test_planes_640x480_matches_cpu_transcription(planes_640x480):
+    sc = planes_640x480
     prob = _problem(sc, sc.ref_index)
     opt = _opts(sc)
     o = orc.run(opt, prob)
@@ -96,25 +96,25 @@ def test_config1_matches_cpu_transcription(config1):
     m = gt > 0
     acc_g, acc_o = syn.depth_accuracy(g["depth"], gt), syn.depth_accuracy(o["depth"], gt)
     agree_d, agree_n = _agreement(g, o, m)
-    print(f"config1 vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
+    print(f"planes_640x480 vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
           f"normal {agree_n:.4f}")
     assert abs(acc_g - acc_o) <= GT_GAP
-    assert agree_d >= CFG1_DEPTH_AGREE and agree_n >= CFG1_NORMAL_AGREE
+    assert agree_d >= PLANES_DEPTH_AGREE and agree_n >= PLANES_NORMAL_AGREE
 
 
 @pytest.fixture(scope="module")
-def config2():
+def heightfield_1600x1200():
     import torch
     return syn.heightfield_scene(seed=0, width=1600, height=1200, num_src=10,
                                  device="cuda" if torch.cuda.is_available() else "cpu")
 
 
 @pytest.mark.skipif(not ref.available(), reason="oracle/_ref not built")
-def test_config2_both_passes_match_reference_kernels(config2):
+def test_heightfield_1600x1200_both_passes_match_reference_kernels(heightfield_1600x1200):
     """Photometric maps of every view, then view 0's geometric pass against the
     others' photometric maps, by the engine and by the reference kernels, each
     from its own maps."""
-    sc = config2
+    sc = heightfield_1600x1200
     V = len(sc.views)
     fviews = [orc.FilterView(v.K, v.R, v.T, v.depth_gt, v.normal_gt) for v in sc.views]
     ours, theirs = [], []
@@ -134,18 +134,18 @@ def test_config2_both_passes_match_reference_kernels(config2):
     for name, a, b in (("photometric", ours[0], theirs[0]), ("geometric", g, res)):
         acc_g, acc_r = syn.depth_accuracy(a["depth"], gt), syn.depth_accuracy(b["depth"], gt)
         out[name] = (acc_g, acc_r) + _agreement(a, b, m)
-    print("config2 vs reference kernels (GT ours, GT reference, agreement depth, normal):", out)
+    print("heightfield_1600x1200 vs reference kernels (GT ours, GT reference, agreement depth, normal):", out)
     for name, (acc_g, acc_r, agree_d, agree_n) in out.items():
         assert abs(acc_g - acc_r) <= GT_GAP, name
-        assert agree_d >= CFG2_DEPTH_AGREE and agree_n >= CFG2_NORMAL_AGREE, name
+        assert agree_d >= HEIGHTFIELD_DEPTH_AGREE and agree_n >= HEIGHTFIELD_NORMAL_AGREE, name
 
 
-def test_config2_precision_form_keeps_accuracy(config2):
+def test_heightfield_1600x1200_precision_form_keeps_accuracy(heightfield_1600x1200):
     """The precision form (FP16 source storage, FP32 accumulation) against the
-    plain FP32 path at config 2: view 0's photometric pass and its geometric
+    plain FP32 path on the 1600x1200 heightfield scene: view 0's photometric pass and its geometric
     pass against the other views' photometric maps, each form from its own
-    maps; ground-truth accuracy within the north star's 0.5 points."""
-    sc = config2
+    maps; ground-truth accuracy within the metric's 0.5 points."""
+    sc = heightfield_1600x1200
     V = len(sc.views)
     gt = sc.views[0].depth_gt
     acc = {}
@@ -154,16 +154,16 @@ def test_config2_precision_form_keeps_accuracy(config2):
         geo = _engine(_opts(sc, True, seed=1000, image_storage=storage),
                       _problem(sc, 0, [(x["depth"], x["normal"]) for x in photo]))
         acc[storage] = (syn.depth_accuracy(photo[0]["depth"], gt), syn.depth_accuracy(geo["depth"], gt))
-    print("config2 precision form (photometric, geometric) f32 / f16:", acc)
+    print("heightfield_1600x1200 precision form (photometric, geometric) f32 / f16:", acc)
     for k in range(2):
         assert abs(acc[STORE_F16][k] - acc[STORE_F32][k]) <= GT_GAP
 
 
-def test_config2_photometric_band_matches_cpu_transcription(config2):
+def test_heightfield_1600x1200_photometric_band_matches_cpu_transcription(heightfield_1600x1200):
     """The CPU transcription on a 64-row band of view 0 (its sweeps read rows
     outside the band that it does not update, so only the band's 16 central
     rows are compared) against the engine's full photometric map."""
-    sc = config2
+    sc = heightfield_1600x1200
     prob = _problem(sc, 0)
     opt = _opts(sc)
     Hh = sc.views[0].image.shape[0]
@@ -177,7 +177,7 @@ def test_config2_photometric_band_matches_cpu_transcription(config2):
     acc_g = float(np.mean(np.abs(g["depth"][m] - gt[m]) <= 0.01 * gt[m]))
     acc_o = float(np.mean(np.abs(o["depth"][m] - gt[m]) <= 0.01 * gt[m]))
     agree_d, agree_n = _agreement(g, o, m)
-    print(f"config2 band vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
+    print(f"heightfield_1600x1200 band vs CPU transcription: GT {acc_g:.4f} vs {acc_o:.4f}; agreement depth {agree_d:.4f} "
           f"normal {agree_n:.4f}")
     assert abs(acc_g - acc_o) <= GT_GAP
-    assert agree_d >= CFG2_DEPTH_AGREE and agree_n >= CFG2_NORMAL_AGREE
+    assert agree_d >= HEIGHTFIELD_DEPTH_AGREE and agree_n >= HEIGHTFIELD_NORMAL_AGREE
