@@ -32,7 +32,8 @@ def serve(pool, specs, arrivals, on_done=None, time_fn=time.perf_counter, before
     """Run `specs[i]` arriving at `arrivals[i]` seconds; returns latency stats.
     `on_done(i, job_id)` is called for each finished job (e.g. to read maps);
     `before_submit(spec)` before a job is submitted (e.g. to make its views
-    resident)."""
+    resident). A job that fails raises RuntimeError (the other jobs stay in the
+    pool)."""
     t0 = time_fn()
     pending = 0
     i = 0
@@ -61,6 +62,8 @@ def serve(pool, specs, arrivals, on_done=None, time_fn=time.perf_counter, before
                 latency[k] = now - arrivals[k]
                 if on_done is not None:
                     on_done(k, jid)
+            elif st == N.JOB_FAILED:
+                raise RuntimeError(f"serving: job {jid} (request {live[jid]}) failed")
     total = time_fn() - t0
     return {"jobs": len(specs), "wall_s": total, "throughput_jobs_s": len(specs) / total,
             "p50_s": float(np.percentile(latency, 50)), "p99_s": float(np.percentile(latency, 99)),
