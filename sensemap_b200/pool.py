@@ -105,8 +105,12 @@ class DepthMapPool:
         return st.value
 
     def run_until_done(self, jobs, max_steps: int = 100000) -> None:
+        """Step until every job in `jobs` is done; a failed job raises at once."""
         for _ in range(max_steps):
-            if all(self.state(j)[0] == N.JOB_DONE for j in jobs):
+            states = [self.state(j)[0] for j in jobs]
+            if any(st == N.JOB_FAILED for st in states):
+                raise RuntimeError(f"job {jobs[states.index(N.JOB_FAILED)]} failed")
+            if all(st == N.JOB_DONE for st in states):
                 return
             self.step()
         raise RuntimeError("jobs did not finish")

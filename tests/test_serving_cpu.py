@@ -72,3 +72,26 @@ def test_serve_raises_on_a_failed_job():
     specs = [JobSpec(None, r, [r + 1]) for r in range(3)]
     with pytest.raises(RuntimeError, match="failed"):
         serve(FakePool(iters=2, fail={2}), specs, np.zeros(3), time_fn=FakeClock())
+
+
+def test_pool_run_until_done_raises_on_a_failed_job():
+    """DepthMapPool.run_until_done with its native calls replaced: it steps until
+    every job is done and stops at once when one fails."""
+    from sensemap_b200.pool import DepthMapPool
+    pool = object.__new__(DepthMapPool)  # no native pool behind it
+    states = {1: N.JOB_ACTIVE, 2: N.JOB_ACTIVE}
+    steps = [0]
+
+    def step():
+        steps[0] += 1
+        if steps[0] == 2:
+            states[1], states[2] = N.JOB_DONE, N.JOB_FAILED
+
+    pool.state = lambda j: (states[j], 0.0)
+    pool.step = step
+    with pytest.raises(RuntimeError, match="job 2 failed"):
+        pool.run_until_done([1, 2])
+    assert steps[0] == 2
+    states[2] = N.JOB_DONE
+    pool.run_until_done([1, 2])  # both done: returns without stepping
+    assert steps[0] == 2
