@@ -943,12 +943,27 @@ def run_single(args, wl, sptr):
     from sensemap_b200.patch_match import PatchMatchACMMCuda
     views = wl.views(wl.dev)
     opt = make_options(wl.scene, wl.storage, False, step=args.single_step)
+    per_kernel = {}
     for i in range(args.warmup + args.steps):
         with PatchMatchACMMCuda(opt, wl.problem(0, views), stream=sptr) as pm:
+            pm.SetProfiling(i >= args.warmup)
             pm.Run()
             pm.Synchronize()
+            if i >= args.warmup:
+                for k, (n, ms) in pm.Profile().items():
+                    per_kernel.setdefault(k, []).append(ms / max(n, 1))
+                depth = pm.GetDepthMap()
     torch.cuda.synchronize()
     log("single-pass profiling run done")
+    if per_kernel:
+        # Per-kernel device time of the pass (CUDA events around each launch),
+        # the best step's average launch, and the map's ground-truth accuracy.
+        from sensemap_b200 import synthetic as syn
+        print(json.dumps({"single_pass": {
+            "workload": f"photometric pass of view 0, {args.width}x{args.height}, N={args.views - 1}, R={RADIUS}, "
+                        f"S={args.single_step}, {ITERS} iterations, {args.storage} storage, default launch shape",
+            "ms_per_launch": {k: round(min(v), 3) for k, v in per_kernel.items()},
+            "within_1pct_gt": syn.depth_accuracy(depth, wl.scene.views[0].depth_gt)}}), flush=True)
 
 
 # ---------------------------------------------------------------------------
